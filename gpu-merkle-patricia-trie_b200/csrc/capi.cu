@@ -1,0 +1,319 @@
+// capi.cu -- the C ABI (include/gmpt.h and the reference's include/libgmpt.h)
+// over gmpt::Trie.  No exceptions or exits cross the boundary.
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gmpt.h"
+#include "../../include/libgmpt.h"
+#include "trie.h"
+
+struct gmpt_trie {
+  gmpt::Trie *t;
+};
+
+namespace {
+
+thread_local int g_last = 0;
+thread_local std::string g_msg;
+
+int record(int rc, const std::string &msg) {
+  g_last = rc;
+  g_msg = rc ? msg : std::string();
+  return rc;
+}
+
+int record_trie(int rc, gmpt::Trie *t) { return record(rc, rc ? t->error() : std::string()); }
+
+int env_device() {
+  const char *s = std::getenv("GMPT_DEVICE");
+  return s ? std::atoi(s) : 0;
+}
+
+int env_mode() {
+  const char *s = std::getenv("GMPT_ENCODE_MODE");
+  return (s && (std::strcmp(s, "geth") == 0 || std::strcmp(s, "1") == 0)) ? GMPT_MODE_GETH : GMPT_MODE_REF;
+}
+
+gmpt::BatchIn host_batch(const uint8_t *k, const int *ki, const uint8_t *v, const int64_t *vi,
+                         const uint8_t *const *hps, int n) {
+  gmpt::BatchIn b;
+  b.keys_hexs = k;
+  b.keys_indexs = ki;
+  b.values = v;
+  b.values_indexs = vi;
+  b.values_hps = reinterpret_cast<const uint64_t *>(hps);
+  b.n = n;
+  b.device = false;
+  return b;
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+int gmpt_version(void) { return 1; }
+
+gmpt_trie *gmpt_create(int device, int encode_mode) {
+  gmpt_trie *h = new (std::nothrow) gmpt_trie{nullptr};
+  if (!h) {
+    record(GMPT_E_CAPACITY, "out of host memory");
+    return nullptr;
+  }
+  h->t = new (std::nothrow) gmpt::Trie(device, encode_mode);
+  if (!h->t || !h->t->error().empty()) {
+    record(GMPT_E_CUDA, h->t ? h->t->error() : "out of host memory");
+    delete h->t;
+    delete h;
+    return nullptr;
+  }
+  record(0, "");
+  return h;
+}
+
+void gmpt_destroy(gmpt_trie *t) {
+  if (!t) return;
+  delete t->t;
+  delete t;
+}
+
+int gmpt_reset(gmpt_trie *t) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->reset(), t->t);
+}
+
+int gmpt_puts_2phase(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                     const uint8_t *values_bytes, const int64_t *values_indexs,
+                     const uint8_t *const *values_hps, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->put_2phase(host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n)),
+                     t->t);
+}
+
+int gmpt_puts_latching(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                       const uint8_t *values_bytes, const int64_t *values_indexs,
+                       const uint8_t *const *values_hps, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(
+      t->t->put_latching(host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n)), t->t);
+}
+
+static gmpt::BatchIn device_batch(const uint8_t *k, const int *ki, const uint8_t *v, const int64_t *vi,
+                                  const uint64_t *hps, int n, int64_t kb, int64_t vb) {
+  gmpt::BatchIn b;
+  b.keys_hexs = k;
+  b.keys_indexs = ki;
+  b.values = v;
+  b.values_indexs = vi;
+  b.values_hps = hps;
+  b.n = n;
+  b.keys_bytes = kb;
+  b.values_bytes = vb;
+  b.device = true;
+  return b;
+}
+
+int gmpt_puts_2phase_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                            const uint8_t *d_values_bytes, const int64_t *d_values_indexs,
+                            const uint64_t *d_values_hps, int n, int64_t keys_bytes, int64_t values_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->put_2phase(device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs,
+                                                   d_values_hps, n, keys_bytes, values_bytes)),
+                     t->t);
+}
+
+int gmpt_puts_latching_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                              const uint8_t *d_values_bytes, const int64_t *d_values_indexs,
+                              const uint64_t *d_values_hps, int n, int64_t keys_bytes, int64_t values_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->put_latching(device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs,
+                                                     d_values_hps, n, keys_bytes, values_bytes)),
+                     t->t);
+}
+
+int gmpt_hash_onepass(gmpt_trie *t) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->hash(), t->t);
+}
+
+int gmpt_pending_targets(gmpt_trie *t, const uint32_t **d_targets, int *n) {
+  if (!t || !d_targets || !n) return record(GMPT_E_ARG, "null argument");
+  *d_targets = t->t->pending_dirty(n);
+  return record(0, "");
+}
+
+int gmpt_get_root_hash(gmpt_trie *t, uint8_t out[32], int *size) {
+  if (!t || !out || !size) return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->root(out, size), t->t);
+}
+
+int gmpt_gets_parallel(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int n,
+                       const uint8_t **values_hps, int *values_sizes) {
+  if (!t || (n > 0 && (!keys_hexs || !keys_indexs || !values_hps || !values_sizes)))
+    return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->gets(keys_hexs, keys_indexs, n, false, reinterpret_cast<uint64_t *>(values_hps),
+                                values_sizes),
+                     t->t);
+}
+
+int gmpt_get_values(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int n, uint8_t *out,
+                    int64_t out_cap, int64_t *out_indexs, int64_t *out_len) {
+  if (!t || !out_len || (n > 0 && (!keys_hexs || !keys_indexs || !out_indexs)))
+    return record(GMPT_E_ARG, "null argument");
+  std::vector<uint8_t> vals;
+  std::vector<int64_t> offs;
+  int rc = t->t->get_values(keys_hexs, keys_indexs, n, vals, offs);
+  if (rc) return record_trie(rc, t->t);
+  *out_len = (int64_t)vals.size();
+  if ((int64_t)vals.size() > out_cap || (!out && !vals.empty())) return record(GMPT_E_ARG, "output buffer too small");
+  if (!vals.empty()) std::memcpy(out, vals.data(), vals.size());
+  std::memcpy(out_indexs, offs.data(), sizeof(int64_t) * offs.size());
+  return record(0, "");
+}
+
+int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out) {
+  if (!t || !out) return record(GMPT_E_ARG, "null argument");
+  static_assert(sizeof(gmpt_stats) == sizeof(gmpt::TrieStats), "stats layout");
+  std::memcpy(out, &t->t->stats(), sizeof(gmpt_stats));
+  return record(0, "");
+}
+
+int gmpt_set_timing(gmpt_trie *t, int on) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  t->t->set_timing(on != 0);
+  return record(0, "");
+}
+
+void *gmpt_stream(gmpt_trie *t) { return t ? static_cast<void *>(t->t->stream()) : nullptr; }
+
+int gmpt_last_error(void) { return g_last; }
+const char *gmpt_last_error_message(void) { return g_msg.c_str(); }
+void gmpt_free_buffer(void *p) { std::free(p); }
+
+// ---------------------------------------------------------------------------
+// reference ABI (lib/libgmpt.cu)
+
+static std::mutex g_tries_mu;
+static gmpt_trie *g_tries[3] = {nullptr, nullptr, nullptr};
+
+static const uint8_t *insert_hash_root(gmpt_trie *t, bool two_phase, const uint8_t *keys_hexs,
+                                       int *keys_hexs_indexs, const uint8_t *values_bytes,
+                                       int64_t *values_bytes_indexs, const uint8_t **values_hps, int n) {
+  if (!t) {
+    record(GMPT_E_ARG, "null trie");
+    return nullptr;
+  }
+  int rc = two_phase ? gmpt_puts_2phase(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs,
+                                        values_hps, n)
+                     : gmpt_puts_latching(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs,
+                                          values_hps, n);
+  if (rc) return nullptr;
+  if (gmpt_hash_onepass(t)) return nullptr;
+  uint8_t root[32];
+  int size = 0;
+  if (gmpt_get_root_hash(t, root, &size)) return nullptr;
+  if (size == 0) return nullptr;
+  uint8_t *out = static_cast<uint8_t *>(std::malloc(32));
+  if (!out) {
+    record(GMPT_E_CAPACITY, "out of host memory");
+    return nullptr;
+  }
+  std::memset(out, 0, 32);
+  std::memcpy(out, root, (size_t)size);
+  return out;
+}
+
+int preprocess() {
+  std::lock_guard<std::mutex> g(g_tries_mu);
+  for (auto &t : g_tries) {
+    gmpt_destroy(t);
+    t = nullptr;
+  }
+  int dev = env_device(), mode = env_mode();
+  for (auto &t : g_tries) {
+    t = gmpt_create(dev, mode);
+    if (!t) return 0;
+  }
+  return 1;
+}
+
+static gmpt_trie *global_trie(TrieType tt) {
+  std::lock_guard<std::mutex> g(g_tries_mu);
+  int i = (int)tt;
+  if (i < 0 || i > 2) return nullptr;
+  return g_tries[i];
+}
+
+const uint8_t *build_mpt_2phase(enum TrieType trie_type, const uint8_t *keys_hexs, int *keys_hexs_indexs,
+                                const uint8_t *values_bytes, int64_t *values_bytes_indexs,
+                                const uint8_t **values_hps, int insert_num) {
+  return insert_hash_root(global_trie(trie_type), true, keys_hexs, keys_hexs_indexs, values_bytes,
+                          values_bytes_indexs, values_hps, insert_num);
+}
+
+const uint8_t *build_mpt_olc(enum TrieType trie_type, const uint8_t *keys_hexs, int *keys_hexs_indexs,
+                             const uint8_t *values_bytes, int64_t *values_bytes_indexs,
+                             const uint8_t **values_hps, int insert_num) {
+  return insert_hash_root(global_trie(trie_type), false, keys_hexs, keys_hexs_indexs, values_bytes,
+                          values_bytes_indexs, values_hps, insert_num);
+}
+
+struct nodeset get_all_nodes(enum TrieType trie_type, const uint8_t *keys_hexs, int *keys_hexs_indexs, int num) {
+  struct nodeset ns {};
+  gmpt_trie *t = global_trie(trie_type);
+  if (!t) {
+    record(GMPT_E_ARG, "trie not initialised (call preprocess)");
+    return ns;
+  }
+  std::vector<uint8_t> hashs, encs;
+  std::vector<unsigned long long> idx;
+  int rc = t->t->flush_nodes(keys_hexs, keys_hexs_indexs, num, hashs, encs, idx);
+  if (rc) {
+    record_trie(rc, t->t);
+    return ns;
+  }
+  uint8_t *h = static_cast<uint8_t *>(std::malloc(hashs.size() + 1));
+  uint8_t *e = static_cast<uint8_t *>(std::malloc(encs.size() + 1));
+  unsigned long long *ix = static_cast<unsigned long long *>(std::malloc(sizeof(unsigned long long) * idx.size() + 8));
+  if (!h || !e || !ix) {
+    std::free(h);
+    std::free(e);
+    std::free(ix);
+    record(GMPT_E_CAPACITY, "out of host memory");
+    return ns;
+  }
+  if (!hashs.empty()) std::memcpy(h, hashs.data(), hashs.size());
+  if (!encs.empty()) std::memcpy(e, encs.data(), encs.size());
+  if (!idx.empty()) std::memcpy(ix, idx.data(), sizeof(unsigned long long) * idx.size());
+  ns.hashs = h;
+  ns.encs = e;
+  ns.encs_indexs = ix;
+  ns.num = hashs.size() / 32;
+  record(0, "");
+  return ns;
+}
+
+void *init_mpt() { return gmpt_create(env_device(), env_mode()); }
+
+const uint8_t *insert_mpt_2phase(void *mpt, const uint8_t *keys_hexs, int *keys_hexs_indexs,
+                                 const uint8_t *values_bytes, int64_t *values_bytes_indexs,
+                                 const uint8_t **values_hps, int insert_num) {
+  return insert_hash_root(static_cast<gmpt_trie *>(mpt), true, keys_hexs, keys_hexs_indexs, values_bytes,
+                          values_bytes_indexs, values_hps, insert_num);
+}
+
+const uint8_t *insert_mpt_olc(void *mpt, const uint8_t *keys_hexs, int *keys_hexs_indexs,
+                              const uint8_t *values_bytes, int64_t *values_bytes_indexs,
+                              const uint8_t **values_hps, int insert_num) {
+  return insert_hash_root(static_cast<gmpt_trie *>(mpt), false, keys_hexs, keys_hexs_indexs, values_bytes,
+                          values_bytes_indexs, values_hps, insert_num);
+}
+
+void free_mpt(void *mpt) { gmpt_destroy(static_cast<gmpt_trie *>(mpt)); }
+
+}  // extern "C"
+#pragma GCC visibility pop

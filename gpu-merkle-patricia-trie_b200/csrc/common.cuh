@@ -1,0 +1,152 @@
+// common.cuh -- shared device definitions for the B200 MPT path.
+//
+// Trie storage (HBM, structure of arrays, 32-bit node references):
+//   ref = kind(2 bits) | index(30 bits); kind 0 = null, 1 = full (branch),
+//   2 = short (extension / leaf), 3 = value.
+// The reference links 56..240-byte AoS nodes by 64-bit pointers
+// (mpt/node.cuh:340-589); here a branch is 17 x 4-byte child refs plus
+// separate hash / depth / epoch arrays, so the walk touches 68 bytes per
+// branch and the hash stage reads only what it encodes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gmpt {
+
+enum : uint32_t { KIND_NULL = 0, KIND_FULL = 1, KIND_SHORT = 2, KIND_VALUE = 3 };
+
+__host__ __device__ __forceinline__ uint32_t ref_kind(uint32_t r) { return r >> 30; }
+__host__ __device__ __forceinline__ uint32_t ref_idx(uint32_t r) { return r & 0x3FFFFFFFu; }
+__host__ __device__ __forceinline__ uint32_t make_ref(uint32_t k, uint32_t i) { return (k << 30) | i; }
+
+constexpr uint32_t kMaxNodes = 0x3FFFFFFFu;  // per node kind
+constexpr int kMaxKeyNibbles = 1024;          // longest accepted hex key
+constexpr uint16_t kLcpInf = 0xFFFF;
+
+// Device error word bits (read back by the host after each call).
+enum : uint32_t {
+  ERR_BAD_KEY = 1u << 0,       // nibble > 16, terminator not last, or prefix key
+  ERR_CAPACITY = 1u << 1,      // a node pool ran out (host bound violated)
+  ERR_RETRY_LIMIT = 1u << 2,   // LockNU insert exceeded its retry budget
+  ERR_KEY_TOO_LONG = 1u << 3,
+  ERR_INTERNAL = 1u << 4,
+};
+
+// Where a new subtree gets linked: a branch child slot, or the root word.
+// slot = (full index << 5) | child, or kSlotRoot.
+constexpr uint64_t kSlotRoot = ~0ull;
+
+struct Counters {
+  uint32_t n_full, n_short, n_value, pad0;
+  uint32_t n_dirty, n_items, n_groups, error;
+  uint64_t key_used, val_used;
+  uint32_t n_pseudo, retries_max, hashed, pad2;
+  unsigned long long enc_bytes, keccak_blocks;  // last hash pass
+};
+
+// Everything a kernel needs to reach the trie; passed by value.
+struct TrieView {
+  // branch (full) nodes
+  uint32_t *full_child;   // [cap_full * 17]
+  uint32_t *full_epoch;   // dirty marker
+  uint16_t *full_depth;   // nibble depth of the node's path
+  uint8_t *full_hash;     // [cap_full * 32]
+  uint8_t *full_hlen;
+  // short nodes
+  uint64_t *short_key;    // nibble offset into the key arena
+  uint32_t *short_klen;
+  uint32_t *short_child;
+  uint32_t *short_epoch;
+  uint16_t *short_depth;
+  uint8_t *short_dead;
+  uint8_t *short_hash;    // [cap_short * 32]
+  uint8_t *short_hlen;
+  uint32_t *short_claim;  // split claim: the batch epoch that claimed it
+  uint32_t *short_pseudo; // pseudo item created by that claim
+  // value nodes -> value records
+  unsigned long long *value_vid;
+  uint64_t *rec_off;      // byte offset into the value arena
+  uint32_t *rec_len;
+  uint64_t *rec_hp;       // caller's host pointer (echoed by gets)
+  // arenas
+  const uint8_t *keys;    // nibble arena (one byte per nibble, 16 = term.)
+  const uint8_t *vals;    // value byte arena
+  uint32_t *root;         // root ref word
+  Counters *ctr;
+  uint32_t cap_full, cap_short, cap_value;
+  uint32_t epoch;         // put batch number (split claims)
+  uint32_t gen;           // hash generation (dirty marks)
+  int geth_mode;          // 1 = embed <32 B children, hash the root always
+};
+
+// ---------------------------------------------------------------------------
+// small device helpers
+
+__device__ __forceinline__ void set_error(Counters *c, uint32_t bits) { atomicOr(&c->error, bits); }
+
+// Warp-aggregated allocation of n (0..7) slots among the currently converged
+// lanes: one atomicAdd per warp instead of one per thread.  Returns the first
+// slot of this lane's run.
+__device__ __forceinline__ uint32_t warp_alloc(uint32_t *counter, uint32_t n) {
+  unsigned mask = __activemask();
+  unsigned lane = threadIdx.x & 31;
+  unsigned lt = (1u << lane) - 1u;
+  unsigned b0 = __ballot_sync(mask, n & 1u);
+  unsigned b1 = __ballot_sync(mask, n & 2u);
+  unsigned b2 = __ballot_sync(mask, n & 4u);
+  uint32_t total = __popc(b0) + 2u * __popc(b1) + 4u * __popc(b2);
+  uint32_t before = __popc(b0 & lt) + 2u * __popc(b1 & lt) + 4u * __popc(b2 & lt);
+  int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader && total) base = atomicAdd(counter, total);
+  base = __shfl_sync(mask, base, leader);
+  return base + before;
+}
+
+// Unaligned 8-byte little-endian load from a byte array padded by >= 8 bytes.
+__device__ __forceinline__ uint64_t load_u64_unaligned(const uint8_t *p) {
+  uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint64_t *q = reinterpret_cast<const uint64_t *>(a & ~uintptr_t(7));
+  uint32_t sh = (uint32_t)(a & 7) * 8;
+  uint64_t lo = __ldg(q);
+  if (sh == 0) return lo;
+  uint64_t hi = __ldg(q + 1);
+  return (lo >> sh) | (hi << (64 - sh));
+}
+
+// Same, through the coherent path (data written earlier in this kernel).
+__device__ __forceinline__ uint64_t load_u64_unaligned_cg(const uint8_t *p) {
+  uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint64_t *q = reinterpret_cast<const uint64_t *>(a & ~uintptr_t(7));
+  uint32_t sh = (uint32_t)(a & 7) * 8;
+  uint64_t lo = q[0];
+  if (sh == 0) return lo;
+  uint64_t hi = q[1];
+  return (lo >> sh) | (hi << (64 - sh));
+}
+
+// 8 nibble bytes (little-endian in a u64, each 0..16) -> 32-bit big-endian
+// nibble chunk, terminator mapped to 0 (byte & 15).
+__device__ __forceinline__ uint32_t pack_nibbles8(uint64_t x) {
+  x &= 0x0F0F0F0F0F0F0F0Full;
+  uint64_t be = __byte_perm((uint32_t)(x >> 32), 0, 0x0123) |
+                ((uint64_t)__byte_perm((uint32_t)x, 0, 0x0123) << 32);
+  be = (be | (be >> 4)) & 0x00FF00FF00FF00FFull;
+  be = (be | (be >> 8)) & 0x0000FFFF0000FFFFull;
+  be = (be | (be >> 16)) & 0x00000000FFFFFFFFull;
+  return (uint32_t)be;
+}
+
+// Number of equal leading nibbles of a[0..n) and b[0..n).
+__device__ __forceinline__ int match_nibbles(const uint8_t *a, const uint8_t *b, int n) {
+  int m = 0;
+  while (m + 8 <= n) {
+    uint64_t x = load_u64_unaligned(a + m) ^ load_u64_unaligned(b + m);
+    if (x) return m + (__ffsll((long long)x) - 1) / 8;
+    m += 8;
+  }
+  while (m < n && a[m] == b[m]) ++m;
+  return m;
+}
+
+}  // namespace gmpt

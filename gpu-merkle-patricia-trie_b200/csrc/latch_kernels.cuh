@@ -1,0 +1,182 @@
+// latch_kernels.cuh -- LockNU: concurrent per-key insert on the live trie.
+//
+// The reference's LockNU (puts_latching_v2, gpu_mpt_kernels.cuh:1573-1605 ->
+// put_olc_v2 :971-1228) runs one warp per key with only lane 0 working and
+// optimistic lock coupling (version word read-lock / validate / upgrade CAS,
+// node.cuh:360-396) with an unbounded restart loop.  Here one thread inserts
+// one key and nodes are never modified after they are published, except a
+// branch's child slots and a value node's record id:
+//   * an empty slot is filled with a CAS from null to a new leaf;
+//   * a short node that must be split is replaced as a whole: the new upper
+//     extension / branch / remainder / own leaf are built privately and
+//     swung into the parent slot with one CAS (the old node is marked dead);
+//   * an existing key takes max(record id), i.e. the last batch position of
+//     the key wins, whatever order the threads run in.
+// A failed CAS re-reads the same slot; the number of failures per key is
+// bounded and exceeding it raises ERR_RETRY_LIMIT instead of spinning.
+#pragma once
+#include "common.cuh"
+#include "trie_kernels.cuh"
+
+namespace gmpt {
+
+__device__ __forceinline__ uint32_t load_slot(const uint32_t *p) {
+  return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+__device__ __forceinline__ uint32_t alloc_short(const TrieView &tv) {
+  uint32_t s = atomicAdd(&tv.ctr->n_short, 1u);
+  if (s >= tv.cap_short) {
+    set_error(tv.ctr, ERR_CAPACITY);
+    return 0xFFFFFFFFu;
+  }
+  return s;
+}
+
+__device__ __forceinline__ uint32_t alloc_full(const TrieView &tv) {
+  uint32_t f = atomicAdd(&tv.ctr->n_full, 1u);
+  if (f >= tv.cap_full) {
+    set_error(tv.ctr, ERR_CAPACITY);
+    return 0xFFFFFFFFu;
+  }
+  return f;
+}
+
+__device__ __forceinline__ void init_short(const TrieView &tv, uint32_t s, uint64_t key_off, uint32_t klen,
+                                           uint32_t child, uint32_t depth, uint32_t gen) {
+  tv.short_key[s] = key_off;
+  tv.short_klen[s] = klen;
+  tv.short_child[s] = child;
+  tv.short_depth[s] = (uint16_t)depth;
+  tv.short_epoch[s] = gen;
+  tv.short_dead[s] = 0;
+  tv.short_claim[s] = 0;
+  tv.short_hlen[s] = 0;
+}
+
+__global__ void k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff, const uint32_t *klen, int n,
+                               uint64_t vid_base, uint32_t retry_limit) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t gen = tv.gen;
+  const uint64_t ko = koff[i];
+  const uint8_t *kb = tv.keys + ko;
+  const uint32_t len = klen[i];
+  const unsigned long long vid = vid_base + (unsigned long long)i;
+  uint32_t vnode = 0xFFFFFFFFu, leaf = 0xFFFFFFFFu, br = 0xFFFFFFFFu, up = 0xFFFFFFFFu, left = 0xFFFFFFFFu;
+  uint32_t *sp = tv.root;
+  uint32_t x = 0;
+  uint32_t fails = 0;
+  for (uint32_t guard = 0; guard < len + 2 + retry_limit; ++guard) {
+    uint32_t ref = load_slot(sp);
+    uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
+    if (kind == KIND_NULL) {
+      if (vnode == 0xFFFFFFFFu) {
+        vnode = atomicAdd(&tv.ctr->n_value, 1u);
+        if (vnode >= tv.cap_value) {
+          set_error(tv.ctr, ERR_CAPACITY);
+          return;
+        }
+        tv.value_vid[vnode] = vid;
+      }
+      uint32_t vref = make_ref(KIND_VALUE, vnode);
+      uint32_t nref = vref;
+      if (x < len) {
+        if (leaf == 0xFFFFFFFFu && (leaf = alloc_short(tv)) == 0xFFFFFFFFu) return;
+        init_short(tv, leaf, ko + x, len - x, vref, x, gen);
+        nref = make_ref(KIND_SHORT, leaf);
+      }
+      __threadfence();
+      if (atomicCAS(sp, 0u, nref) == 0u) {
+        if (x < len) dirty_push(tv.ctr, dl, nref, x);
+        return;
+      }
+      if (++fails > retry_limit) break;
+      continue;
+    }
+    if (kind == KIND_FULL) {
+      mark_full(tv, dl, idx, gen);
+      if (x >= len) break;
+      uint32_t c = kb[x];
+      sp = tv.full_child + (size_t)idx * 17 + c;
+      ++x;
+      continue;
+    }
+    if (kind == KIND_VALUE) {
+      if (x != len) break;
+      atomicMax(&tv.value_vid[idx], vid);
+      return;
+    }
+    // short node
+    const uint64_t sko = __ldcg(tv.short_key + idx);
+    const uint32_t sl = __ldcg(tv.short_klen + idx);
+    const uint32_t schild = __ldcg(tv.short_child + idx);
+    const uint8_t *sk = tv.keys + sko;
+    uint32_t lim = min(sl, len - x);
+    uint32_t mm = (uint32_t)match_nibbles(sk, kb + x, (int)lim);
+    if (mm == sl) {
+      mark_short(tv, dl, idx, gen);
+      sp = tv.short_child + idx;
+      x += sl;
+      continue;
+    }
+    if (mm == len - x) break;  // key is a prefix of a stored key
+    // split: [up(key[0..mm))] -> br{ sk[mm]: left/rest, kb[x+mm]: own leaf }
+    if (br == 0xFFFFFFFFu && (br = alloc_full(tv)) == 0xFFFFFFFFu) return;
+    uint32_t bd = x + mm;
+    uint32_t *ch = tv.full_child + (size_t)br * 17;
+#pragma unroll
+    for (int c = 0; c < 17; ++c) ch[c] = 0;
+    tv.full_depth[br] = (uint16_t)bd;
+    tv.full_epoch[br] = gen;
+    tv.full_hlen[br] = 0;
+    // the old node's remainder
+    uint32_t rest = schild;
+    bool use_left = sl - mm - 1 > 0;
+    if (use_left) {
+      if (left == 0xFFFFFFFFu && (left = alloc_short(tv)) == 0xFFFFFFFFu) return;
+      init_short(tv, left, sko + mm + 1, sl - mm - 1, schild, bd + 1, gen);
+      rest = make_ref(KIND_SHORT, left);
+    }
+    ch[sk[mm]] = rest;
+    // this key's leaf
+    if (vnode == 0xFFFFFFFFu) {
+      vnode = atomicAdd(&tv.ctr->n_value, 1u);
+      if (vnode >= tv.cap_value) {
+        set_error(tv.ctr, ERR_CAPACITY);
+        return;
+      }
+      tv.value_vid[vnode] = vid;
+    }
+    uint32_t own = make_ref(KIND_VALUE, vnode);
+    bool use_leaf = bd + 1 < len;
+    if (use_leaf) {
+      if (leaf == 0xFFFFFFFFu && (leaf = alloc_short(tv)) == 0xFFFFFFFFu) return;
+      init_short(tv, leaf, ko + bd + 1, len - bd - 1, own, bd + 1, gen);
+      own = make_ref(KIND_SHORT, leaf);
+    }
+    ch[kb[bd]] = own;
+    uint32_t top = make_ref(KIND_FULL, br);
+    if (mm > 0) {
+      if (up == 0xFFFFFFFFu && (up = alloc_short(tv)) == 0xFFFFFFFFu) return;
+      init_short(tv, up, sko, mm, top, x, gen);
+      top = make_ref(KIND_SHORT, up);
+    }
+    __threadfence();
+    if (atomicCAS(sp, ref, top) == ref) {
+      tv.short_dead[idx] = 1;
+      dirty_push(tv.ctr, dl, make_ref(KIND_FULL, br), bd);
+      if (use_left) dirty_push(tv.ctr, dl, make_ref(KIND_SHORT, left), bd + 1);
+      if (use_leaf) dirty_push(tv.ctr, dl, make_ref(KIND_SHORT, leaf), bd + 1);
+      if (mm > 0) dirty_push(tv.ctr, dl, make_ref(KIND_SHORT, up), x);
+      return;
+    }
+    if (++fails > retry_limit) break;
+  }
+  if (fails > retry_limit)
+    set_error(tv.ctr, ERR_RETRY_LIMIT);
+  else
+    set_error(tv.ctr, ERR_BAD_KEY);
+}
+
+}  // namespace gmpt

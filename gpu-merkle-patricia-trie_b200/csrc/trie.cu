@@ -1,0 +1,814 @@
+// trie.cu -- host orchestration of the B200 MPT update path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "trie.h"
+#include "trie_kernels.cuh"
+#include "latch_kernels.cuh"
+#include "export_kernels.cuh"
+
+namespace gmpt {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kHashThreads = 128;
+constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);
+
+inline unsigned blocks_for(int64_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+template <typename T>
+cudaError_t grow_array(T *&p, size_t old_n, size_t new_n, cudaStream_t st) {
+  T *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, new_n * sizeof(T) + 64);
+  if (e != cudaSuccess) return e;
+  if (p && old_n) {
+    e = cudaMemcpyAsync(q, p, old_n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+  }
+  if (p) cudaFree(p);
+  p = q;
+  return cudaSuccess;
+}
+
+template <typename T>
+T *wsp(DevBlock &b, size_t n, cudaError_t &e) {
+  if (e != cudaSuccess) return nullptr;
+  e = b.ensure(n * sizeof(T) + 64);
+  return b.as<T>();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+Trie::Trie(int device, int geth_mode) : dev_(device), geth_(geth_mode ? 1 : 0) {
+  cudaError_t e = cudaSetDevice(dev_);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&root_, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&ctr_, sizeof(Counters));
+  if (e == cudaSuccess) e = cudaMallocHost(&h_ctr_, sizeof(Counters));
+  if (e == cudaSuccess) e = cudaMallocHost(&h_small_, 256);
+  if (e == cudaSuccess) e = cudaMemset(root_, 0, 64);
+  if (e == cudaSuccess) e = cudaMemset(ctr_, 0, sizeof(Counters));
+  if (e != cudaSuccess) {
+    err_ = std::string("trie init: ") + cudaGetErrorString(e);
+    return;
+  }
+  tv_.root = root_;
+  tv_.ctr = ctr_;
+  tv_.geth_mode = geth_;
+  ensure_capacity(1024, 1024, 1024, 1024, 4096, 4096);
+}
+
+Trie::~Trie() {
+  cudaSetDevice(dev_);
+  if (st_) cudaStreamSynchronize(st_);
+  void *ptrs[] = {tv_.full_child, tv_.full_epoch, tv_.full_depth, tv_.full_hash, tv_.full_hlen,
+                  tv_.short_key, tv_.short_klen, tv_.short_child, tv_.short_epoch, tv_.short_depth,
+                  tv_.short_dead, tv_.short_hash, tv_.short_hlen, tv_.short_claim, tv_.short_pseudo,
+                  tv_.value_vid, tv_.rec_off, tv_.rec_len, tv_.rec_hp, (void *)tv_.keys, (void *)tv_.vals,
+                  root_, ctr_, dirty_ref_, dirty_depth_};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  DevBlock *blocks[] = {&ws_.koff, &ws_.klen, &ws_.ki, &ws_.vi, &ws_.hp, &ws_.kin, &ws_.order, &ws_.eqprev,
+                        &ws_.flags, &ws_.pos, &ws_.act, &ws_.skey, &ws_.sval, &ws_.uord, &ws_.w_status,
+                        &ws_.w_code, &ws_.w_d0, &ws_.w_slot, &ws_.w_short, &ws_.w_after, &ws_.p_short,
+                        &ws_.p_d0, &ws_.p_slot, &ws_.p_amin, &ws_.p_max, &ws_.it_key, &ws_.it_id,
+                        &ws_.it_base, &ws_.it_len, &ws_.it_ref, &ws_.it_d0, &ws_.it_slot, &ws_.sb_base,
+                        &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
+                        &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
+                        &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.misc};
+  for (DevBlock *b : blocks) b->release();
+  for (int k = 0; k < 2; ++k) {
+    ws_.s_start[k].release();
+    ws_.s_end[k].release();
+    ws_.s_depth[k].release();
+    ws_.s_slot[k].release();
+    ws_.s_D[k].release();
+    ws_.s_branch[k].release();
+  }
+  sorter_.release();
+  scan_ws_.release();
+  if (h_ctr_) cudaFreeHost(h_ctr_);
+  if (h_small_) cudaFreeHost(h_small_);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+int Trie::fail(int code, const std::string &msg) {
+  err_ = msg;
+  return code;
+}
+
+int Trie::check_cuda(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return OK;
+  return fail(E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int Trie::sync_counters() {
+  cudaError_t e = cudaMemcpyAsync(h_ctr_, ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  if (e != cudaSuccess) return check_cuda(e, "sync counters");
+  n_full_ = h_ctr_->n_full;
+  n_short_ = h_ctr_->n_short;
+  n_value_ = h_ctr_->n_value;
+  uint32_t err = h_ctr_->error;
+  if (err) {
+    cudaMemsetAsync(&ctr_->error, 0, 4, st_);
+    if (err & ERR_CAPACITY) return fail(E_CAPACITY, "node pool capacity exceeded");
+    if (err & ERR_RETRY_LIMIT) return fail(E_RETRY_LIMIT, "insert retry limit exceeded");
+    if (err & ERR_KEY_TOO_LONG) return fail(E_BAD_KEY, "key longer than the supported maximum");
+    if (err & ERR_BAD_KEY)
+      return fail(E_BAD_KEY, "malformed key: nibble > 16, terminator not last, or a key that is a prefix of another");
+    return fail(E_INTERNAL, "internal consistency check failed");
+  }
+  return OK;
+}
+
+uint64_t Trie::read_u64(const void *dptr) {
+  cudaMemcpyAsync(h_small_, dptr, 8, cudaMemcpyDeviceToHost, st_);
+  cudaStreamSynchronize(st_);
+  return h_small_[0];
+}
+
+int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
+                          uint64_t add_key_bytes, uint64_t add_val_bytes) {
+  cudaError_t e = cudaSuccess;
+  auto grow_to = [](uint64_t need, uint64_t cap) {
+    uint64_t c = cap ? cap : 1024;
+    while (c < need) c = c + c / 2 + 1024;
+    return c;
+  };
+  uint64_t need_full = (uint64_t)n_full_ + add_full;
+  if (need_full > kMaxNodes) return fail(E_CAPACITY, "branch node count exceeds 2^30");
+  if (need_full > cap_full_) {
+    uint64_t nc = std::min<uint64_t>(grow_to(need_full, cap_full_), kMaxNodes);
+    size_t o = n_full_;
+    if (e == cudaSuccess) e = grow_array(tv_.full_child, o * 17, nc * 17, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_epoch, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_depth, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_hash, o * 32, nc * 32, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_hlen, o, nc, st_);
+    if (e != cudaSuccess) return check_cuda(e, "grow branch pool");
+    cap_full_ = (uint32_t)nc;
+  }
+  uint64_t need_short = (uint64_t)n_short_ + add_short;
+  if (need_short > kMaxNodes) return fail(E_CAPACITY, "short node count exceeds 2^30");
+  if (need_short > cap_short_) {
+    uint64_t nc = std::min<uint64_t>(grow_to(need_short, cap_short_), kMaxNodes);
+    size_t o = n_short_;
+    if (e == cudaSuccess) e = grow_array(tv_.short_key, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_klen, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_child, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_epoch, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_depth, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_dead, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_hash, o * 32, nc * 32, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_hlen, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_claim, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_pseudo, o, nc, st_);
+    if (e != cudaSuccess) return check_cuda(e, "grow short pool");
+    cap_short_ = (uint32_t)nc;
+  }
+  uint64_t need_value = (uint64_t)n_value_ + add_value;
+  if (need_value > kMaxNodes) return fail(E_CAPACITY, "value node count exceeds 2^30");
+  if (need_value > cap_value_) {
+    uint64_t nc = std::min<uint64_t>(grow_to(need_value, cap_value_), kMaxNodes);
+    if ((e = grow_array(tv_.value_vid, n_value_, nc, st_)) != cudaSuccess) return check_cuda(e, "grow values");
+    cap_value_ = (uint32_t)nc;
+  }
+  uint64_t need_rec = n_rec_ + add_rec;
+  if (need_rec > cap_rec_) {
+    uint64_t nc = grow_to(need_rec, cap_rec_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_off, n_rec_, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_len, n_rec_, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_hp, n_rec_, nc, st_);
+    if (e != cudaSuccess) return check_cuda(e, "grow value records");
+    cap_rec_ = nc;
+  }
+  uint64_t need_keys = key_used_ + add_key_bytes + 64;
+  if (need_keys > cap_keys_) {
+    uint64_t nc = grow_to(need_keys, cap_keys_);
+    uint8_t *p = const_cast<uint8_t *>(tv_.keys);
+    if ((e = grow_array(p, key_used_, nc + 64, st_)) != cudaSuccess) return check_cuda(e, "grow key arena");
+    tv_.keys = p;
+    cap_keys_ = nc;
+  }
+  uint64_t need_vals = val_used_ + add_val_bytes + 64;
+  if (need_vals > cap_vals_) {
+    uint64_t nc = grow_to(need_vals, cap_vals_);
+    uint8_t *p = const_cast<uint8_t *>(tv_.vals);
+    if ((e = grow_array(p, val_used_, nc + 64, st_)) != cudaSuccess) return check_cuda(e, "grow value arena");
+    tv_.vals = p;
+    cap_vals_ = nc;
+  }
+  // every node is pushed to the dirty list at most once per hash generation
+  uint64_t need_dirty = (uint64_t)cap_full_ + cap_short_;
+  if (need_dirty > cap_dirty_) {
+    uint64_t nc = need_dirty;
+    uint32_t nd = 0;
+    if (cap_dirty_) {
+      cudaMemcpyAsync(h_small_, &ctr_->n_dirty, 4, cudaMemcpyDeviceToHost, st_);
+      cudaStreamSynchronize(st_);
+      nd = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+    }
+    if (e == cudaSuccess) e = grow_array(dirty_ref_, nd, nc, st_);
+    if (e == cudaSuccess) e = grow_array(dirty_depth_, nd, nc, st_);
+    if (e != cudaSuccess) return check_cuda(e, "grow dirty list");
+    cap_dirty_ = nc;
+  }
+  tv_.cap_full = cap_full_;
+  tv_.cap_short = cap_short_;
+  tv_.cap_value = cap_value_;
+  stats_.device_bytes = (uint64_t)cap_full_ * (68 + 4 + 2 + 32 + 1) + (uint64_t)cap_short_ * (8 + 4 + 4 + 4 + 2 + 1 + 32 + 1 + 8) +
+                        (uint64_t)cap_value_ * 8 + cap_rec_ * 20 + cap_keys_ + cap_vals_ + cap_dirty_ * 6;
+  return OK;
+}
+
+// Copy the batch into the arenas and build per-key records.
+int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
+                uint32_t *maxlen) {
+  const int n = b.n;
+  cudaError_t e = cudaSuccess;
+  int64_t kbytes = b.keys_bytes, vbytes = b.values_bytes;
+  if (kbytes < 0 || vbytes < 0) {
+    if (b.device) return fail(E_ARG, "device batches must give keys_bytes and values_bytes");
+    kbytes = (int64_t)b.keys_indexs[2 * n - 1] + 1;
+    vbytes = (int64_t)b.values_indexs[2 * n - 1] + 1;
+  }
+  int rc = ensure_capacity(2ull * n, 4ull * n, (uint64_t)n, (uint64_t)n, (uint64_t)kbytes, (uint64_t)vbytes);
+  if (rc) return rc;
+  key_base = key_used_;
+  vid_base = n_rec_;
+  uint64_t val_base = val_used_;
+  cudaMemcpyKind kind = b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  uint8_t *karena = const_cast<uint8_t *>(tv_.keys);
+  uint8_t *varena = const_cast<uint8_t *>(tv_.vals);
+  int *ki = wsp<int>(ws_.ki, 2 * (size_t)n, e);
+  int64_t *vi = wsp<int64_t>(ws_.vi, 2 * (size_t)n, e);
+  uint64_t *hp = b.values_hps ? wsp<uint64_t>(ws_.hp, (size_t)n, e) : nullptr;
+  *koff = wsp<uint64_t>(ws_.koff, (size_t)n, e);
+  *klen = wsp<uint32_t>(ws_.klen, (size_t)n, e);
+  uint32_t *d_max = wsp<uint32_t>(ws_.misc, 16, e);
+  if (e != cudaSuccess) return check_cuda(e, "stage alloc");
+  e = cudaMemcpyAsync(karena + key_base, b.keys_hexs, (size_t)kbytes, kind, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(varena + val_base, b.values, (size_t)vbytes, kind, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ki, b.keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vi, b.values_indexs, sizeof(int64_t) * 2 * (size_t)n, kind, st_);
+  if (e == cudaSuccess && hp) e = cudaMemcpyAsync(hp, b.values_hps, sizeof(uint64_t) * (size_t)n, kind, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(karena + key_base + kbytes, 0, 64, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
+  if (e != cudaSuccess) return check_cuda(e, "stage copy");
+  k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
+                                                *koff, *klen, d_max);
+  e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  if (e != cudaSuccess) return check_cuda(e, "stage");
+  *maxlen = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  // keys are 8-aligned in the arena so chunk loads start aligned more often
+  key_used_ += ((uint64_t)kbytes + 7) & ~7ull;
+  val_used_ += (uint64_t)vbytes;
+  n_rec_ += (uint64_t)n;
+  stats_.key_bytes = key_used_;
+  stats_.value_bytes = val_used_;
+  stats_.n_records = n_rec_;
+  return OK;
+}
+
+// Lexicographic order of the batch (terminator before nibble 0) with the last
+// occurrence of every key kept: uord[0..m) are batch indices.
+int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, uint32_t **uord_out,
+                      int *m_out) {
+  cudaError_t e = cudaSuccess;
+  uint32_t *order = wsp<uint32_t>(ws_.order, (size_t)n, e);
+  uint8_t *eqprev = wsp<uint8_t>(ws_.eqprev, (size_t)n + 1, e);
+  unsigned long long *flags = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
+  uint32_t *act = wsp<uint32_t>(ws_.act, (size_t)n, e);
+  uint64_t *skey = wsp<uint64_t>(ws_.skey, (size_t)n, e);
+  uint32_t *sval = wsp<uint32_t>(ws_.sval, (size_t)n, e);
+  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)n, e);
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+  if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
+  if (e != cudaSuccess) return check_cuda(e, "sort alloc");
+  k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
+  int nchunks = (int)((maxlen + 7) / 8);
+  stats_.sort_passes = 0;
+  for (int c = 0; c <= nchunks; ++c) {
+    int cc = (c == nchunks) ? -1 : c;  // final pass: key length
+    k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
+    e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+    if (e != cudaSuccess) return check_cuda(e, "sort flags");
+    int K = (int)(h_small_[0] & 0xFFFFFFFFu);
+    if (K == 0) break;
+    k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval);
+    int passes = 0;
+    if ((e = sorter_.sort(skey, sval, K, st_, &passes)) != cudaSuccess) return check_cuda(e, "radix sort");
+    stats_.sort_passes += passes;
+    k_sort_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act, skey, sval, K, order, eqprev);
+  }
+  k_keep_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
+  e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
+  if (e == cudaSuccess) k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, order, n, uord);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  if (e != cudaSuccess) return check_cuda(e, "unique");
+  *m_out = (int)(h_small_[0] & 0xFFFFFFFFu);
+  *uord_out = uord;
+  return OK;
+}
+
+// Level-synchronous construction over the T sorted items in ws_.sb_*.
+int Trie::build_levels(int T) {
+  cudaError_t e = cudaSuccess;
+  SortedItems si{ws_.sb_base.as<uint64_t>(), ws_.sb_len.as<uint32_t>(), ws_.sb_ref.as<uint32_t>(),
+                 ws_.sb_d0.as<uint32_t>(),   ws_.sb_slot.as<uint64_t>(), ws_.sb_code.as<uint64_t>(),
+                 ws_.lcp.as<uint16_t>()};
+  DirtyList dl{dirty_ref_, dirty_depth_};
+  uint8_t *kflags = wsp<uint8_t>(ws_.kflags, (size_t)T, e);
+  uint8_t *knib = wsp<uint8_t>(ws_.knib, (size_t)T, e);
+  unsigned long long *flags = wsp<unsigned long long>(ws_.flags, (size_t)T, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)T, e);
+  uint32_t *act[2] = {wsp<uint32_t>(ws_.act, (size_t)T, e), wsp<uint32_t>(ws_.act2, (size_t)T, e)};
+  uint32_t *aseg[2] = {wsp<uint32_t>(ws_.aseg, (size_t)T, e), wsp<uint32_t>(ws_.aseg2, (size_t)T, e)};
+  SegArrays sg[2];
+  for (int k = 0; k < 2; ++k) {
+    sg[k].start = wsp<uint32_t>(ws_.s_start[k], (size_t)T, e);
+    sg[k].end = wsp<uint32_t>(ws_.s_end[k], (size_t)T, e);
+    sg[k].depth = wsp<uint32_t>(ws_.s_depth[k], (size_t)T, e);
+    sg[k].D = wsp<uint32_t>(ws_.s_D[k], (size_t)T, e);
+    sg[k].branch = wsp<uint32_t>(ws_.s_branch[k], (size_t)T, e);
+    sg[k].slot = wsp<uint64_t>(ws_.s_slot[k], (size_t)T, e);
+  }
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+  if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(T));
+  if (e != cudaSuccess) return check_cuda(e, "build alloc");
+  k_groups_init<<<blocks_for(T), kThreads, 0, st_>>>(tv_, dl, si, T, gen_, kflags, flags);
+  e = exclusive_scan<unsigned long long>(flags, pos, T, d_tot, scan_ws_, st_);
+  if (e != cudaSuccess) return check_cuda(e, "groups scan");
+  k_groups_scatter<<<blocks_for(T), kThreads, 0, st_>>>(si, kflags, pos, T, act[0], aseg[0], sg[0]);
+  if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "groups");
+  int K = (int)(h_small_[0] & 0xFFFFFFFFu);
+  int S = (int)(h_small_[0] >> 32);
+  int cur = 0, levels = 0;
+  while (K > 0) {
+    ++levels;
+    if (levels > kMaxKeyNibbles + 2) return fail(E_INTERNAL, "builder did not converge");
+    k_level_min<<<blocks_for(K), kThreads, 0, st_>>>(si, act[cur], aseg[cur], K, sg[cur]);
+    k_level_nodes<<<blocks_for(S), kThreads, 0, st_>>>(tv_, dl, si, S, sg[cur], gen_);
+    k_level_children<<<blocks_for(K), kThreads, 0, st_>>>(tv_, dl, si, act[cur], aseg[cur], K, sg[cur], gen_,
+                                                          kflags, knib, flags);
+    e = exclusive_scan<unsigned long long>(flags, pos, K, d_tot, scan_ws_, st_);
+    if (e != cudaSuccess) return check_cuda(e, "level scan");
+    k_level_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act[cur], aseg[cur], kflags, knib, pos, K, sg[cur],
+                                                         act[cur ^ 1], aseg[cur ^ 1], sg[cur ^ 1]);
+    if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "level");
+    K = (int)(h_small_[0] & 0xFFFFFFFFu);
+    S = (int)(h_small_[0] >> 32);
+    cur ^= 1;
+  }
+  stats_.build_levels = levels;
+  return OK;
+}
+
+int Trie::put_2phase(const BatchIn &b) {
+  err_.clear();
+  if (b.n < 0 || b.n > (1 << 26)) return fail(E_ARG, "batch size must be in [0, 2^26]");
+  if (b.n == 0) return OK;
+  if (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs) return fail(E_ARG, "null batch array");
+  cudaSetDevice(dev_);
+  cudaEvent_t ev[6];
+  if (timing_)
+    for (auto &x : ev) cudaEventCreate(&x);
+  if (timing_) cudaEventRecord(ev[0], st_);
+  ++epoch_;
+  tv_.epoch = epoch_;
+  tv_.gen = gen_;
+  uint64_t key_base, vid_base;
+  uint64_t *koff;
+  uint32_t *klen;
+  uint32_t maxlen = 0;
+  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen);
+  if (rc) return rc;
+  if ((rc = sync_counters())) return rc;  // key validation
+  if (timing_) cudaEventRecord(ev[1], st_);
+  const int n = b.n;
+  uint32_t *uord;
+  int m = 0;
+  if ((rc = sort_unique(n, koff, klen, maxlen, &uord, &m))) return rc;
+  stats_.last_unique = (uint64_t)m;
+  if (timing_) cudaEventRecord(ev[2], st_);
+
+  // walk
+  cudaError_t e = cudaSuccess;
+  WalkOut wo;
+  wo.status = wsp<uint8_t>(ws_.w_status, (size_t)m, e);
+  wo.code = wsp<uint64_t>(ws_.w_code, (size_t)m, e);
+  wo.d0 = wsp<uint32_t>(ws_.w_d0, (size_t)m, e);
+  wo.slot = wsp<uint64_t>(ws_.w_slot, (size_t)m, e);
+  wo.short_id = wsp<uint32_t>(ws_.w_short, (size_t)m, e);
+  wo.after = wsp<uint8_t>(ws_.w_after, (size_t)m, e);
+  wo.p_short = wsp<uint32_t>(ws_.p_short, (size_t)m, e);
+  wo.p_d0 = wsp<uint32_t>(ws_.p_d0, (size_t)m, e);
+  wo.p_slot = wsp<uint64_t>(ws_.p_slot, (size_t)m, e);
+  wo.p_amin = wsp<uint32_t>(ws_.p_amin, (size_t)m, e);
+  wo.p_max = wsp<uint32_t>(ws_.p_max, (size_t)m, e);
+  unsigned long long *flags = wsp<unsigned long long>(ws_.flags, (size_t)m, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)m, e);
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+  if (e == cudaSuccess) e = cudaMemsetAsync(&ctr_->n_pseudo, 0, 4, st_);
+  if (e != cudaSuccess) return check_cuda(e, "walk alloc");
+  DirtyList dl{dirty_ref_, dirty_depth_};
+  k_walk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, dl, uord, m, koff, klen, vid_base, wo);
+  k_pseudo_ranks<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, m);
+  k_new_flags<<<blocks_for(m), kThreads, 0, st_>>>(wo.status, m, flags);
+  e = exclusive_scan<unsigned long long>(flags, pos, m, d_tot, scan_ws_, st_);
+  if (e != cudaSuccess) return check_cuda(e, "walk scan");
+  if ((rc = sync_counters())) return rc;
+  uint32_t n_pseudo = h_ctr_->n_pseudo;
+  int n_new = (int)(read_u64(d_tot) & 0xFFFFFFFFu);
+  stats_.last_new = (uint64_t)n_new;
+  stats_.last_pseudo = n_pseudo;
+  if (timing_) cudaEventRecord(ev[3], st_);
+  int T = n_new + (int)n_pseudo;
+  if (T > 0) {
+    Items it;
+    it.key = wsp<uint64_t>(ws_.it_key, (size_t)T, e);
+    it.id = wsp<uint32_t>(ws_.it_id, (size_t)T, e);
+    it.base = wsp<uint64_t>(ws_.it_base, (size_t)T, e);
+    it.len = wsp<uint32_t>(ws_.it_len, (size_t)T, e);
+    it.ref = wsp<uint32_t>(ws_.it_ref, (size_t)T, e);
+    it.d0 = wsp<uint32_t>(ws_.it_d0, (size_t)T, e);
+    it.slot = wsp<uint64_t>(ws_.it_slot, (size_t)T, e);
+    uint64_t *sb_base = wsp<uint64_t>(ws_.sb_base, (size_t)T, e);
+    uint32_t *sb_len = wsp<uint32_t>(ws_.sb_len, (size_t)T, e);
+    uint32_t *sb_ref = wsp<uint32_t>(ws_.sb_ref, (size_t)T, e);
+    uint32_t *sb_d0 = wsp<uint32_t>(ws_.sb_d0, (size_t)T, e);
+    uint64_t *sb_slot = wsp<uint64_t>(ws_.sb_slot, (size_t)T, e);
+    uint64_t *sb_code = wsp<uint64_t>(ws_.sb_code, (size_t)T, e);
+    uint16_t *lcp = wsp<uint16_t>(ws_.lcp, (size_t)T + 1, e);
+    if (e != cudaSuccess) return check_cuda(e, "items alloc");
+    if (n_new > 0)
+      k_items_new<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, pos, m, uord, koff, klen, vid_base, it);
+    if (n_pseudo > 0) {
+      k_items_pseudo<<<blocks_for(n_pseudo), kThreads, 0, st_>>>(tv_, wo, (int)n_pseudo, n_new, it);
+      int passes = 0;
+      if ((e = sorter_.sort(it.key, it.id, T, st_, &passes)) != cudaSuccess) return check_cuda(e, "group sort");
+    }
+    k_items_gather<<<blocks_for(T), kThreads, 0, st_>>>(it, n_pseudo > 0 ? it.id : nullptr, T, sb_base, sb_len,
+                                                        sb_ref, sb_d0, sb_slot, sb_code);
+    k_items_lcp<<<blocks_for(T), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, T, lcp);
+    if ((rc = build_levels(T))) return rc;
+  }
+  if ((rc = sync_counters())) return rc;
+  if (timing_) {
+    cudaEventRecord(ev[4], st_);
+    cudaEventSynchronize(ev[4]);
+    cudaEventElapsedTime(&stats_.t_stage_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&stats_.t_sort_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&stats_.t_walk_ms, ev[2], ev[3]);
+    cudaEventElapsedTime(&stats_.t_build_ms, ev[3], ev[4]);
+    for (auto &x : ev) cudaEventDestroy(x);
+  }
+  stats_.n_full = n_full_;
+  stats_.n_short = n_short_;
+  stats_.n_value = n_value_;
+  empty_ = false;
+  return OK;
+}
+
+// PhaseHC over every node marked dirty since the last hash.
+int Trie::bucket_and_hash() {
+  cudaError_t e = cudaSuccess;
+  uint32_t nd = 0;
+  if ((e = cudaMemcpyAsync(h_small_, &ctr_->n_dirty, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "dirty count");
+  nd = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  stats_.last_dirty = nd;
+  stats_.last_hash_levels = 0;
+  if (nd == 0) return OK;
+  uint32_t *bins = wsp<uint32_t>(ws_.bins, kMaxDepthBins + 1, e);
+  uint32_t *cursor = wsp<uint32_t>(ws_.cursor, kMaxDepthBins + 1, e);
+  uint32_t *sorted = wsp<uint32_t>(ws_.sorted_dirty, nd, e);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * (kMaxDepthBins + 1), st_);
+  if (e != cudaSuccess) return check_cuda(e, "hash alloc");
+  int grid = std::min<int>(blocks_for(nd), 148 * 4);
+  k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kMaxDepthBins, st_>>>(dirty_ref_, dirty_depth_, (int)nd, bins,
+                                                                          kMaxDepthBins);
+  std::vector<uint32_t> hb(kMaxDepthBins), off(kMaxDepthBins + 1);
+  if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyDeviceToHost, st_)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "hash bins");
+  off[0] = 0;
+  for (int b = 0; b < kMaxDepthBins; ++b) off[b + 1] = off[b] + hb[b];
+  if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyHostToDevice, st_)) !=
+      cudaSuccess)
+    return check_cuda(e, "hash cursor");
+  k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, (int)nd, cursor, sorted);
+  uint32_t root_ref = 0;
+  if ((e = cudaMemcpyAsync(h_small_, root_, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "root ref");
+  root_ref = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
+  int levels = 0;
+  if ((e = cudaMemsetAsync(&ctr_->hashed, 0, 4, st_)) != cudaSuccess ||
+      (e = cudaMemsetAsync(&ctr_->enc_bytes, 0, 16, st_)) != cudaSuccess)
+    return check_cuda(e, "hash counters");
+  cudaEvent_t ka = nullptr, kz = nullptr;
+  if (timing_) {
+    cudaEventCreate(&ka);
+    cudaEventCreate(&kz);
+    cudaEventRecord(ka, st_);
+  }
+  for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
+    uint32_t a = off[2 * d], z = off[2 * d + 2];
+    if (z == a) continue;
+    ++levels;
+    k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a),
+                                                                               root_ref);
+  }
+  if (timing_) {
+    cudaEventRecord(kz, st_);
+    cudaEventSynchronize(kz);
+    cudaEventElapsedTime(&stats_.t_hash_kernels_ms, ka, kz);
+    cudaEventDestroy(ka);
+    cudaEventDestroy(kz);
+  }
+  stats_.last_hash_levels = levels;
+  stats_.hash_launches = levels;
+  if ((e = cudaMemsetAsync(&ctr_->n_dirty, 0, 4, st_)) != cudaSuccess) return check_cuda(e, "hash reset");
+  if ((e = cudaGetLastError()) != cudaSuccess) return check_cuda(e, "hash launch");
+  ++gen_;
+  tv_.gen = gen_;
+  return OK;
+}
+
+int Trie::hash() {
+  err_.clear();
+  cudaSetDevice(dev_);
+  cudaEvent_t a, z;
+  if (timing_) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&z);
+    cudaEventRecord(a, st_);
+  }
+  int rc = bucket_and_hash();
+  if (rc) return rc;
+  if ((rc = sync_counters())) return rc;
+  stats_.last_hashed = h_ctr_->hashed;
+  stats_.last_enc_bytes = h_ctr_->enc_bytes;
+  stats_.last_keccak_blocks = h_ctr_->keccak_blocks;
+  if (timing_) {
+    cudaEventRecord(z, st_);
+    cudaEventSynchronize(z);
+    cudaEventElapsedTime(&stats_.t_hash_ms, a, z);
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+  }
+  return OK;
+}
+
+int Trie::root(uint8_t out[32], int *len) {
+  err_.clear();
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  uint8_t *d = wsp<uint8_t>(ws_.misc, 256, e) + 128;
+  if (e != cudaSuccess) return check_cuda(e, "root alloc");
+  k_root<<<1, 32, 0, st_>>>(tv_, d);
+  uint8_t h[40];
+  if ((e = cudaMemcpyAsync(h_small_, d, 33, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "root");
+  std::memcpy(h, h_small_, 33);
+  *len = h[32];
+  std::memcpy(out, h, 32);
+  return OK;
+}
+
+int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs, uint64_t *out_hp,
+               int *out_len, int64_t keys_bytes) {
+  err_.clear();
+  if (n <= 0) return OK;
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  if (keys_bytes < 0) {
+    if (device_inputs) return fail(E_ARG, "device lookups need keys_bytes");
+    keys_bytes = (int64_t)keys_indexs[2 * n - 1] + 1;
+  }
+  cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  uint8_t *dk = wsp<uint8_t>(ws_.g_keys, (size_t)keys_bytes + 64, e);
+  int *di = wsp<int>(ws_.g_idx, 2 * (size_t)n, e);
+  uint64_t *dhp = wsp<uint64_t>(ws_.g_hp, (size_t)n, e);
+  int *dlen = wsp<int>(ws_.g_len, (size_t)n, e);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, kind, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  if (e != cudaSuccess) return check_cuda(e, "gets copy");
+  k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr);
+  e = cudaMemcpyAsync(out_hp, dhp, sizeof(uint64_t) * (size_t)n, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out_len, dlen, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  return check_cuda(e, "gets");
+}
+
+int Trie::get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &vals,
+                     std::vector<int64_t> &offs) {
+  err_.clear();
+  vals.clear();
+  offs.assign(2 * (size_t)n, -1);
+  if (n <= 0) return OK;
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  int64_t keys_bytes = (int64_t)keys_indexs[2 * n - 1] + 1;
+  uint8_t *dk = wsp<uint8_t>(ws_.g_keys, (size_t)keys_bytes + 64, e);
+  int *di = wsp<int>(ws_.g_idx, 2 * (size_t)n, e);
+  uint64_t *dhp = wsp<uint64_t>(ws_.g_hp, (size_t)n, e);
+  int *dlen = wsp<int>(ws_.g_len, (size_t)n, e);
+  int64_t *dvid = wsp<int64_t>(ws_.misc, (size_t)n + 64, e);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, cudaMemcpyHostToDevice, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice, st_);
+  if (e != cudaSuccess) return check_cuda(e, "get_values copy");
+  k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, dvid);
+  std::vector<int64_t> vid(n);
+  std::vector<int> len(n);
+  e = cudaMemcpyAsync(vid.data(), dvid, 8 * (size_t)n, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(len.data(), dlen, 4 * (size_t)n, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  if (e != cudaSuccess) return check_cuda(e, "get_values");
+  // value offsets of the found records
+  std::vector<uint64_t> roff(n, 0);
+  for (int i = 0; i < n; ++i) {
+    if (vid[i] < 0) continue;
+    e = cudaMemcpyAsync(&roff[i], tv_.rec_off + vid[i], 8, cudaMemcpyDeviceToHost, st_);
+    if (e != cudaSuccess) return check_cuda(e, "get_values rec");
+  }
+  cudaStreamSynchronize(st_);
+  for (int i = 0; i < n; ++i) {
+    if (vid[i] < 0) continue;
+    size_t at = vals.size();
+    vals.resize(at + (size_t)len[i]);
+    if (len[i] > 0) {
+      e = cudaMemcpy(vals.data() + at, tv_.vals + roff[i], (size_t)len[i], cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return check_cuda(e, "get_values bytes");
+    }
+    offs[2 * i] = (int64_t)at;
+    offs[2 * i + 1] = (int64_t)at + len[i] - 1;
+  }
+  return OK;
+}
+
+const uint32_t *Trie::pending_dirty(int *n) const {
+  cudaMemcpy(h_small_, &ctr_->n_dirty, 4, cudaMemcpyDeviceToHost);
+  *n = (int)(h_small_[0] & 0xFFFFFFFFu);
+  return dirty_ref_;
+}
+
+int Trie::reset() {
+  err_.clear();
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaMemsetAsync(root_, 0, 4, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctr_, 0, sizeof(Counters), st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  if (e != cudaSuccess) return check_cuda(e, "reset");
+  n_full_ = n_short_ = n_value_ = 0;
+  n_rec_ = key_used_ = val_used_ = 0;
+  empty_ = true;
+  ++gen_;
+  tv_.gen = gen_;
+  return OK;
+}
+
+}  // namespace gmpt
+
+namespace gmpt {
+
+// LockNU batch: no sort, every key (duplicates included) inserted concurrently.
+int Trie::put_latching(const BatchIn &b) {
+  err_.clear();
+  if (b.n < 0 || b.n > (1 << 26)) return fail(E_ARG, "batch size must be in [0, 2^26]");
+  if (b.n == 0) return OK;
+  if (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs) return fail(E_ARG, "null batch array");
+  cudaSetDevice(dev_);
+  cudaEvent_t ev[3];
+  if (timing_) {
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], st_);
+  }
+  ++epoch_;
+  tv_.epoch = epoch_;
+  tv_.gen = gen_;
+  uint64_t key_base, vid_base;
+  uint64_t *koff;
+  uint32_t *klen;
+  uint32_t maxlen = 0;
+  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen);
+  if (rc) return rc;
+  if ((rc = sync_counters())) return rc;
+  if (timing_) cudaEventRecord(ev[1], st_);
+  DirtyList dl{dirty_ref_, dirty_depth_};
+  k_latch_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
+  if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
+  if ((rc = sync_counters())) return rc;
+  if (timing_) {
+    cudaEventRecord(ev[2], st_);
+    cudaEventSynchronize(ev[2]);
+    cudaEventElapsedTime(&stats_.t_stage_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&stats_.t_build_ms, ev[1], ev[2]);
+    stats_.t_sort_ms = stats_.t_walk_ms = 0;
+    for (auto &x : ev) cudaEventDestroy(x);
+  }
+  stats_.n_full = n_full_;
+  stats_.n_short = n_short_;
+  stats_.n_value = n_value_;
+  stats_.last_unique = (uint64_t)b.n;
+  empty_ = false;
+  return OK;
+}
+
+}  // namespace gmpt
+
+namespace gmpt {
+
+int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &hashs,
+                      std::vector<uint8_t> &encs, std::vector<unsigned long long> &encs_indexs) {
+  err_.clear();
+  hashs.clear();
+  encs.clear();
+  encs_indexs.clear();
+  if (n <= 0) return OK;
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  int64_t keys_bytes = (int64_t)keys_indexs[2 * n - 1] + 1;
+  uint8_t *dk = wsp<uint8_t>(ws_.g_keys, (size_t)keys_bytes + 64, e);
+  int *di = wsp<int>(ws_.g_idx, 2 * (size_t)n, e);
+  uint32_t *d_cnt = wsp<uint32_t>(ws_.misc, 64, e);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, cudaMemcpyHostToDevice, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice, st_);
+  if (e != cudaSuccess) return check_cuda(e, "flush copy");
+  uint32_t cap = (uint32_t)std::min<uint64_t>((uint64_t)n * 24 + 64, 0x7FFFFFFFull);
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    uint64_t *refs = wsp<uint64_t>(ws_.skey, cap, e);
+    uint32_t *dummy = wsp<uint32_t>(ws_.sval, cap, e);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt, 0, 4, st_);
+    if (e != cudaSuccess) return check_cuda(e, "flush alloc");
+    k_flush_collect<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, refs, d_cnt, cap);
+    uint32_t cnt = (uint32_t)(read_u64(d_cnt) & 0xFFFFFFFFu);
+    if (cnt > cap) {
+      cap = cnt;
+      continue;
+    }
+    if (cnt == 0) return OK;
+    if ((e = sorter_.sort(refs, dummy, cnt, st_)) != cudaSuccess) return check_cuda(e, "flush sort");
+    unsigned long long *flags = wsp<unsigned long long>(ws_.flags, cnt, e);
+    unsigned long long *pos = wsp<unsigned long long>(ws_.pos, cnt, e);
+    uint32_t *uref = wsp<uint32_t>(ws_.act, cnt, e);
+    unsigned long long *sizes = wsp<unsigned long long>(ws_.it_key, cnt, e);
+    unsigned long long *offs = wsp<unsigned long long>(ws_.it_base, cnt, e);
+    unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 64, e) + 4;
+    if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(cnt));
+    if (e != cudaSuccess) return check_cuda(e, "flush alloc2");
+    k_flush_unique_flags<<<blocks_for(cnt), kThreads, 0, st_>>>(refs, (int)cnt, flags);
+    if ((e = exclusive_scan<unsigned long long>(flags, pos, cnt, d_tot, scan_ws_, st_)) != cudaSuccess)
+      return check_cuda(e, "flush scan");
+    int m = (int)read_u64(d_tot);
+    k_flush_sizes<<<blocks_for(cnt), kThreads, 0, st_>>>(tv_, refs, flags, pos, (int)cnt, uref, sizes);
+    if ((e = exclusive_scan<unsigned long long>(sizes, offs, m, d_tot, scan_ws_, st_)) != cudaSuccess)
+      return check_cuda(e, "flush scan2");
+    uint64_t total = read_u64(d_tot);
+    uint8_t *d_encs = wsp<uint8_t>(ws_.sb_base, total + 64, e);
+    unsigned long long *d_idx = wsp<unsigned long long>(ws_.sb_slot, 2 * (size_t)m, e);
+    uint8_t *d_hash = wsp<uint8_t>(ws_.sb_code, 32 * (size_t)m, e);
+    if (e != cudaSuccess) return check_cuda(e, "flush alloc3");
+    k_flush_write<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uref, offs, m, d_encs, d_idx, d_hash);
+    hashs.resize(32 * (size_t)m);
+    encs.resize(total);
+    encs_indexs.resize(2 * (size_t)m);
+    e = cudaMemcpyAsync(hashs.data(), d_hash, hashs.size(), cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess && total) e = cudaMemcpyAsync(encs.data(), d_encs, total, cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(encs_indexs.data(), d_idx, 8 * encs_indexs.size(), cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+    return check_cuda(e, "flush read");
+  }
+  return fail(E_INTERNAL, "flush: node count changed between passes");
+}
+
+}  // namespace gmpt

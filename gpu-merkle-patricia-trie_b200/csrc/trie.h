@@ -1,0 +1,148 @@
+// trie.h -- host side of the B200 MPT: one device-resident trie per object.
+//
+// Mirrors GpuMPT::Compress::MPT (mpt-with-compress/include/mpt/gpu_mpt.cuh:18-192):
+//   put_2phase   <- puts_2phase_with_valuehp        (gpu_mpt.cuh:1262-1399)
+//   put_latching <- puts_latching_with_valuehp_v2   (gpu_mpt.cuh:554-615)
+//   hash         <- hash_onepass_v2                 (gpu_mpt.cuh:1162-1191)
+//   gets         <- gets_parallel                   (gpu_mpt.cuh:984-1036)
+//   root         <- get_root_hash                   (gpu_mpt.cuh:1217-1247)
+// Differences that are deliberate: the trie owns copies of key and value
+// bytes (the reference keeps pointers into per-call buffers it never frees),
+// errors come back as status codes instead of exit(), duplicate keys in a
+// batch resolve to the last occurrence (the reference CPU semantics) in both
+// insert strategies, and an update to an existing key replaces its value in
+// both strategies.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "prims.cuh"
+
+namespace gmpt {
+
+struct BatchIn {
+  const uint8_t *keys_hexs = nullptr;    // nibble bytes
+  const int *keys_indexs = nullptr;      // [2n] inclusive
+  const uint8_t *values = nullptr;
+  const int64_t *values_indexs = nullptr;  // [2n] inclusive
+  const uint64_t *values_hps = nullptr;  // [n] caller host pointers, may be null
+  int n = 0;
+  int64_t keys_bytes = -1;    // total key stream bytes (derived if < 0, host only)
+  int64_t values_bytes = -1;  // total value stream bytes
+  bool device = false;        // pointers are device memory
+};
+
+struct TrieStats {
+  uint64_t n_full, n_short, n_value, n_records;
+  uint64_t key_bytes, value_bytes;
+  uint64_t last_unique, last_new, last_pseudo, last_dirty, last_levels, last_hash_levels;
+  uint64_t device_bytes;
+  uint32_t sort_passes, build_levels;
+  float t_stage_ms, t_sort_ms, t_walk_ms, t_build_ms, t_hash_ms;
+  uint64_t last_hashed, last_enc_bytes, last_keccak_blocks;  // last hash pass
+  float t_hash_kernels_ms;  // hash-level kernels only (timing mode)
+  uint32_t hash_launches, pad;
+};
+
+enum Status : int {
+  OK = 0,
+  E_CUDA = 1,
+  E_BAD_KEY = 2,
+  E_CAPACITY = 3,
+  E_RETRY_LIMIT = 4,
+  E_ARG = 5,
+  E_INTERNAL = 6,
+};
+
+class Trie {
+ public:
+  Trie(int device, int geth_mode);
+  ~Trie();
+  Trie(const Trie &) = delete;
+  Trie &operator=(const Trie &) = delete;
+
+  int put_2phase(const BatchIn &b);
+  int put_latching(const BatchIn &b);
+  int hash();
+  int root(uint8_t out[32], int *len);
+  // out_hp[i] = host pointer given with the value (0 when absent), out_len[i] its size
+  int gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs,
+           uint64_t *out_hp, int *out_len, int64_t keys_bytes = -1);
+  // value bytes of the stored value for each key (test/export helper)
+  int get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &vals,
+                 std::vector<int64_t> &offs);
+  int reset();
+  // dirty node refs pending for hash (device array) and their count
+  const uint32_t *pending_dirty(int *n) const;
+  int flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &hashs,
+                  std::vector<uint8_t> &encs, std::vector<unsigned long long> &encs_indexs);
+  const TrieStats &stats() const { return stats_; }
+  const std::string &error() const { return err_; }
+  cudaStream_t stream() const { return st_; }
+  int device() const { return dev_; }
+  void set_timing(bool on) { timing_ = on; }
+
+ private:
+  int dev_ = 0;
+  int geth_ = 0;
+  cudaStream_t st_ = nullptr;
+  std::string err_;
+  TrieStats stats_{};
+  bool timing_ = false;
+
+  // node pools (capacities in elements)
+  TrieView tv_{};
+  uint32_t cap_full_ = 0, cap_short_ = 0, cap_value_ = 0;
+  uint64_t cap_rec_ = 0;
+  uint64_t cap_keys_ = 0, cap_vals_ = 0;
+  uint32_t n_full_ = 0, n_short_ = 0, n_value_ = 0;
+  uint64_t n_rec_ = 0, key_used_ = 0, val_used_ = 0;
+  uint32_t *root_ = nullptr;
+  Counters *ctr_ = nullptr;
+  Counters *h_ctr_ = nullptr;  // pinned mirror
+  uint32_t epoch_ = 0;         // per put batch (split claims)
+  uint32_t gen_ = 1;           // per hash pass (dirty marks)
+  bool empty_ = true;
+
+  // dirty list pending for hash()
+  uint32_t *dirty_ref_ = nullptr;
+  uint16_t *dirty_depth_ = nullptr;
+  uint64_t cap_dirty_ = 0;
+
+  // per-batch workspaces
+  struct Ws {
+    DevBlock koff, klen, ki, vi, hp, kin;          // staged batch
+    DevBlock order, eqprev, flags, pos, act, skey, sval, uord;  // sort / dedup
+    DevBlock w_status, w_code, w_d0, w_slot, w_short, w_after;  // walk
+    DevBlock p_short, p_d0, p_slot, p_amin, p_max;              // pseudo items
+    DevBlock it_key, it_id, it_base, it_len, it_ref, it_d0, it_slot;  // items
+    DevBlock sb_base, sb_len, sb_ref, sb_d0, sb_slot, sb_code, lcp;   // sorted items
+    DevBlock act2, aseg, aseg2, kflags, knib;                   // builder levels
+    DevBlock s_start[2], s_end[2], s_depth[2], s_slot[2], s_D[2], s_branch[2];
+    DevBlock bins, cursor, sorted_dirty;                        // hash buckets
+    DevBlock g_keys, g_idx, g_hp, g_len;                        // gets
+    DevBlock misc;
+  } ws_;
+  RadixSorter sorter_;
+  DevBlock scan_ws_;
+  uint64_t *h_small_ = nullptr;  // pinned scratch for small readbacks
+
+  int fail(int code, const std::string &msg);
+  int check_cuda(cudaError_t e, const char *what);
+  int sync_counters();
+  int ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
+                      uint64_t add_key_bytes, uint64_t add_val_bytes);
+  int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
+            uint32_t *maxlen);
+  int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, uint32_t **uord,
+                  int *m);
+  int build_levels(int T);
+  int bucket_and_hash();
+  uint64_t read_u64(const void *dptr);
+};
+
+}  // namespace gmpt

@@ -1,0 +1,901 @@
+// trie_kernels.cuh -- sm_100a kernels of the batched MPT update path.
+//
+// Pipeline of one PhaseNU batch (puts_2phase_with_valuehp,
+// mpt-with-compress/include/mpt/gpu_mpt.cuh:1262-1399):
+//   k_stage        key/value records into trie-owned arenas, key validation
+//   k_sort_*       lexicographic sort of the batch by 8-nibble chunks with
+//                  segment refinement; last occurrence of a key wins
+//   k_walk         per unique key: read-only descent from the root, marks
+//                  the path dirty, overwrites values of keys that exist,
+//                  and finds where new keys attach (anchor)
+//   k_items_*      new keys + one "pseudo" item per short node that must be
+//                  split, grouped by anchor
+//   k_level_*      level-synchronous construction of the compressed
+//                  subtries of every group (branch / extension / leaf)
+//   k_hash_level   fused RLP encode + Keccak-256 of every dirty node of one
+//                  nibble depth, deepest first (PhaseHC)
+// The reference instead expands every key into one 240-byte FullNode per
+// nibble and recompresses (K:3655, K:4025, K:4643); building the compressed
+// form directly from the sorted batch writes each node once.
+#pragma once
+#include "common.cuh"
+#include "keccak.cuh"
+
+namespace gmpt {
+
+// ---------------------------------------------------------------------------
+// dirty list
+
+struct DirtyList {
+  uint32_t *ref;
+  uint16_t *depth;
+};
+
+__device__ __forceinline__ void dirty_push(Counters *c, DirtyList d, uint32_t ref, uint32_t depth) {
+  uint32_t i = warp_alloc(&c->n_dirty, 1);
+  d.ref[i] = ref;
+  d.depth[i] = (uint16_t)depth;
+}
+
+// First visitor of a node in this hash generation appends it to the dirty
+// list.  Reads go through L2 (ld.cg): under LockNU the node may have been
+// created by another SM during this launch.
+__device__ __forceinline__ void mark_full(const TrieView &tv, DirtyList d, uint32_t f, uint32_t gen) {
+  if (__ldcg(tv.full_epoch + f) != gen) {
+    if (atomicExch(&tv.full_epoch[f], gen) != gen)
+      dirty_push(tv.ctr, d, make_ref(KIND_FULL, f), __ldcg(tv.full_depth + f));
+  }
+}
+
+__device__ __forceinline__ void mark_short(const TrieView &tv, DirtyList d, uint32_t s, uint32_t gen) {
+  if (__ldcg(tv.short_epoch + s) != gen) {
+    if (atomicExch(&tv.short_epoch[s], gen) != gen)
+      dirty_push(tv.ctr, d, make_ref(KIND_SHORT, s), __ldcg(tv.short_depth + s));
+  }
+}
+
+__device__ __forceinline__ void write_slot(const TrieView &tv, uint64_t slot, uint32_t ref) {
+  if (slot == kSlotRoot)
+    *tv.root = ref;
+  else
+    tv.full_child[(slot >> 5) * 17 + (slot & 31)] = ref;
+}
+
+__device__ __forceinline__ uint32_t new_full(const TrieView &tv, DirtyList d, uint32_t depth, uint32_t gen) {
+  uint32_t f = warp_alloc(&tv.ctr->n_full, 1);
+  if (f >= tv.cap_full) {
+    set_error(tv.ctr, ERR_CAPACITY);
+    return 0xFFFFFFFFu;
+  }
+  uint32_t *ch = tv.full_child + (size_t)f * 17;
+#pragma unroll
+  for (int i = 0; i < 17; ++i) ch[i] = 0;
+  tv.full_depth[f] = (uint16_t)depth;
+  tv.full_epoch[f] = gen;
+  tv.full_hlen[f] = 0;
+  dirty_push(tv.ctr, d, make_ref(KIND_FULL, f), depth);
+  return f;
+}
+
+__device__ __forceinline__ uint32_t new_short(const TrieView &tv, DirtyList d, uint64_t key_off, uint32_t klen,
+                                              uint32_t child, uint32_t depth, uint32_t gen) {
+  uint32_t s = warp_alloc(&tv.ctr->n_short, 1);
+  if (s >= tv.cap_short) {
+    set_error(tv.ctr, ERR_CAPACITY);
+    return 0xFFFFFFFFu;
+  }
+  tv.short_key[s] = key_off;
+  tv.short_klen[s] = klen;
+  tv.short_child[s] = child;
+  tv.short_depth[s] = (uint16_t)depth;
+  tv.short_epoch[s] = gen;
+  tv.short_dead[s] = 0;
+  tv.short_claim[s] = 0;
+  tv.short_hlen[s] = 0;
+  dirty_push(tv.ctr, d, make_ref(KIND_SHORT, s), depth);
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// staging
+
+__global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uint64_t *hp, int n,
+                        uint64_t key_base, uint64_t val_base, uint64_t vid_base, int64_t kbytes,
+                        int64_t vbytes, uint64_t *koff, uint32_t *klen, uint32_t *maxlen) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int ks = ki[2 * i], ke = ki[2 * i + 1];
+  bool bad = ks < 0 || ke < ks || (int64_t)ke >= kbytes;  // index pair outside the key stream
+  if (bad) ks = ke = 0;
+  int len = ke - ks + 1;
+  uint64_t off = key_base + (uint64_t)ks;
+  if (len > kMaxKeyNibbles) {
+    set_error(tv.ctr, ERR_KEY_TOO_LONG);
+    bad = true;
+  }
+  if (!bad) {
+    const uint8_t *k = tv.keys + off;
+    for (int j = 0; j < len; ++j) {
+      uint8_t b = k[j];
+      if (b > 16 || (b == 16 && j != len - 1)) bad = true;
+    }
+  }
+  if (bad) {
+    set_error(tv.ctr, ERR_BAD_KEY);
+    len = 1;  // keep later stages in bounds
+  }
+  koff[i] = off;
+  klen[i] = (uint32_t)len;
+  unsigned am = __activemask();
+  uint32_t wmax = __reduce_max_sync(am, (uint32_t)len);
+  if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(maxlen, wmax);
+  int64_t vs = vi[2 * i], ve = vi[2 * i + 1];
+  if (vs < 0 || ve < vs - 1 || ve >= vbytes || ve - vs + 1 > 0x7FFFFFFF) {  // empty values allowed
+    set_error(tv.ctr, ERR_BAD_KEY);
+    vs = 0;
+    ve = -1;
+  }
+  uint64_t vid = vid_base + (uint64_t)i;
+  tv.rec_off[vid] = val_base + (uint64_t)vs;
+  tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
+  tv.rec_hp[vid] = hp ? hp[i] : 0ull;
+}
+
+// ---------------------------------------------------------------------------
+// sort + dedup (chunked MSD refinement over LSD radix passes)
+
+__device__ __forceinline__ uint32_t key_chunk(const uint8_t *keys, uint64_t off, uint32_t len, int c) {
+  uint32_t start = (uint32_t)c * 8;
+  if (start >= len) return 0;
+  uint64_t x = load_u64_unaligned(keys + off + start);
+  uint32_t rem = len - start;
+  if (rem < 8) x &= (1ull << (8 * rem)) - 1;  // zero bytes beyond the key
+  return pack_nibbles8(x);
+}
+
+// active = tied with a neighbour; packed: low = active, high = segment start
+__global__ void k_sort_flags(const uint8_t *eqprev, int n, unsigned long long *flags) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  uint32_t tl = eqprev[p], tr = eqprev[p + 1];
+  uint32_t active = (tl | tr) ? 1u : 0u;
+  uint32_t start = (active && !tl) ? 1u : 0u;
+  flags[p] = (unsigned long long)active | ((unsigned long long)start << 32);
+}
+
+__global__ void k_sort_build(TrieView tv, const unsigned long long *flags, const unsigned long long *pos,
+                             const uint32_t *order, const uint64_t *koff, const uint32_t *klen, int n, int c,
+                             uint32_t *act, uint64_t *skey, uint32_t *sval) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  unsigned long long f = flags[p];
+  if (!(f & 1ull)) return;
+  unsigned long long q = pos[p];
+  uint32_t k = (uint32_t)q;
+  uint32_t seg = (uint32_t)(q >> 32) + (uint32_t)(f >> 32) - 1u;
+  uint32_t it = order[p];
+  uint32_t ch = c >= 0 ? key_chunk(tv.keys, koff[it], klen[it], c) : klen[it];
+  act[k] = (uint32_t)p;
+  skey[k] = ((uint64_t)seg << 32) | ch;
+  sval[k] = it;
+}
+
+__global__ void k_sort_scatter(const uint32_t *act, const uint64_t *skey, const uint32_t *sval, int K,
+                               uint32_t *order, uint8_t *eqprev) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  uint32_t p = act[k];
+  order[p] = sval[k];
+  eqprev[p] = (k > 0 && skey[k] == skey[k - 1]) ? 1 : 0;
+}
+
+__global__ void k_init_order(uint32_t *order, uint8_t *eqprev, int n) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > n) return;
+  if (p < n) order[p] = (uint32_t)p;
+  eqprev[p] = (p > 0 && p < n) ? 1 : 0;
+}
+
+// keep the last of every run of equal keys
+__global__ void k_keep_flags(const uint8_t *eqprev, int n, unsigned long long *flags) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  flags[p] = eqprev[p + 1] ? 0ull : 1ull;
+}
+
+__global__ void k_keep_scatter(const unsigned long long *flags, const unsigned long long *pos,
+                               const uint32_t *order, int n, uint32_t *uord) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (flags[p]) uord[(uint32_t)pos[p]] = order[p];
+}
+
+// ---------------------------------------------------------------------------
+// walk (PhaseNU against an existing trie)
+
+enum : uint8_t { W_EXISTS = 0, W_NEW = 1, W_SPLIT = 2, W_ERROR = 3 };
+
+// anchor code: kind(2) | index(30) | child(5)  (37 bits, shifted left 27
+// in the item sort key; the low 27 bits hold the rank)
+__device__ __forceinline__ uint64_t code_full(uint32_t f, uint32_t c) {
+  return (1ull << 35) | ((uint64_t)f << 5) | c;
+}
+__device__ __forceinline__ uint64_t code_short(uint32_t s) { return (2ull << 35) | ((uint64_t)s << 5) | 31u; }
+
+// nibble order used by the sort: terminator (16) sorts before 0
+__device__ __forceinline__ int sym_rank(uint8_t b) { return b == 16 ? -1 : (int)b; }
+
+struct WalkOut {
+  uint8_t *status;
+  uint64_t *code;
+  uint32_t *d0;
+  uint64_t *slot;
+  uint32_t *short_id;
+  uint8_t *after;
+  // pseudo items
+  uint32_t *p_short;
+  uint32_t *p_d0;
+  uint64_t *p_slot;
+  uint32_t *p_amin;
+  uint32_t *p_max;
+};
+
+__global__ void k_walk(TrieView tv, DirtyList dl, const uint32_t *uord, int m, const uint64_t *koff,
+                       const uint32_t *klen, uint64_t vid_base, WalkOut wo) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint32_t item = uord[j];
+  const uint8_t *kb = tv.keys + koff[item];
+  uint32_t len = klen[item];
+  uint32_t ref = *tv.root;
+  uint32_t x = 0;
+  uint64_t slot = kSlotRoot;
+  uint32_t gen = tv.gen;
+  for (uint32_t guard = 0; guard <= len + 1; ++guard) {
+    uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
+    if (kind == KIND_NULL) {
+      wo.status[j] = W_NEW;
+      wo.code[j] = (slot == kSlotRoot) ? 0ull : code_full((uint32_t)(slot >> 5), (uint32_t)(slot & 31));
+      wo.d0[j] = x;
+      wo.slot[j] = slot;
+      return;
+    }
+    if (kind == KIND_FULL) {
+      mark_full(tv, dl, idx, gen);
+      if (x >= len) break;
+      uint32_t c = kb[x];
+      slot = ((uint64_t)idx << 5) | c;
+      ref = tv.full_child[(size_t)idx * 17 + c];
+      ++x;
+      continue;
+    }
+    if (kind == KIND_SHORT) {
+      const uint8_t *sk = tv.keys + tv.short_key[idx];
+      uint32_t sl = tv.short_klen[idx];
+      uint32_t lim = min(sl, len - x);
+      uint32_t mm = (uint32_t)match_nibbles(sk, kb + x, (int)lim);
+      if (mm == sl) {
+        mark_short(tv, dl, idx, gen);
+        ref = tv.short_child[idx];
+        x += sl;
+        continue;
+      }
+      if (mm == len - x) break;  // key ends inside a stored key: prefix
+      wo.status[j] = W_SPLIT;
+      wo.code[j] = code_short(idx);
+      wo.d0[j] = x;
+      wo.slot[j] = slot;
+      wo.short_id[j] = idx;
+      wo.after[j] = sym_rank(kb[x + mm]) > sym_rank(sk[mm]) ? 1 : 0;
+      // first diverger claims the split and creates the pseudo item
+      uint32_t ep = tv.epoch;
+      if (tv.short_claim[idx] != ep) {
+        if (atomicExch(&tv.short_claim[idx], ep) != ep) {
+          uint32_t p = atomicAdd(&tv.ctr->n_pseudo, 1u);
+          wo.p_short[p] = idx;
+          wo.p_d0[p] = x;
+          wo.p_slot[p] = slot;
+          wo.p_amin[p] = 0xFFFFFFFFu;
+          wo.p_max[p] = 0;
+          tv.short_pseudo[idx] = p;
+          tv.short_dead[idx] = 1;
+        }
+      }
+      return;
+    }
+    // value node
+    if (x == len) {
+      atomicMax(&tv.value_vid[idx], (unsigned long long)(vid_base + item));
+      wo.status[j] = W_EXISTS;
+      return;
+    }
+    break;
+  }
+  wo.status[j] = W_ERROR;
+  set_error(tv.ctr, ERR_BAD_KEY);
+}
+
+__global__ void k_new_flags(const uint8_t *status, int m, unsigned long long *flags) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint8_t st = status[j];
+  flags[j] = (st == W_NEW || st == W_SPLIT) ? 1ull : 0ull;
+}
+
+__global__ void k_pseudo_ranks(TrieView tv, const WalkOut wo, int m) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  if (wo.status[j] != W_SPLIT) return;
+  uint32_t p = tv.short_pseudo[wo.short_id[j]];
+  if (wo.after[j]) atomicMin(&wo.p_amin[p], (uint32_t)j);
+  atomicMax(&wo.p_max[p], (uint32_t)j);
+}
+
+struct Items {
+  uint64_t *key;
+  uint32_t *id;
+  uint64_t *base;
+  uint32_t *len;
+  uint32_t *ref;
+  uint32_t *d0;
+  uint64_t *slot;
+};
+
+// new keys (status NEW / SPLIT) -> items [0, n_new)
+__global__ void k_items_new(TrieView tv, const WalkOut wo, const unsigned long long *pos, int m,
+                            const uint32_t *uord, const uint64_t *koff, const uint32_t *klen, uint64_t vid_base,
+                            Items it) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint8_t st = wo.status[j];
+  if (st != W_NEW && st != W_SPLIT) return;
+  uint32_t i = (uint32_t)pos[j];
+  uint32_t item = uord[j];
+  uint32_t v = warp_alloc(&tv.ctr->n_value, 1);
+  if (v >= tv.cap_value) {
+    set_error(tv.ctr, ERR_CAPACITY);
+    v = 0;
+  }
+  tv.value_vid[v] = vid_base + item;
+  it.key[i] = (wo.code[j] << 27) | (2ull * (uint64_t)j + 1ull);
+  it.id[i] = i;
+  it.base[i] = koff[item];
+  it.len[i] = klen[item];
+  it.ref[i] = make_ref(KIND_VALUE, v);
+  it.d0[i] = wo.d0[j];
+  it.slot[i] = wo.slot[j];
+}
+
+// pseudo items [n_new, n_new + n_pseudo): the existing short node re-inserted
+// as a key ending in its old child
+__global__ void k_items_pseudo(TrieView tv, const WalkOut wo, int n_pseudo, int n_new, Items it) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_pseudo) return;
+  uint32_t s = wo.p_short[p];
+  uint32_t d0 = wo.p_d0[p];
+  uint32_t amin = wo.p_amin[p];
+  // real keys rank 2j+1; the pseudo item sits just before the first key
+  // that sorts after the short node's key, else after the last diverger
+  uint64_t rank = (amin != 0xFFFFFFFFu) ? (2ull * amin) : (2ull * wo.p_max[p] + 2ull);
+  uint32_t i = (uint32_t)n_new + (uint32_t)p;
+  it.key[i] = (code_short(s) << 27) | rank;
+  it.id[i] = i;
+  it.base[i] = tv.short_key[s] - d0;
+  it.len[i] = d0 + tv.short_klen[s];
+  it.ref[i] = tv.short_child[s];
+  it.d0[i] = d0;
+  it.slot[i] = wo.p_slot[p];
+}
+
+// gather items into sorted order, group starts, and adjacent LCPs
+__global__ void k_items_gather(const Items it, const uint32_t *order, int T, uint64_t *sb_base, uint32_t *sb_len,
+                               uint32_t *sb_ref, uint32_t *sb_d0, uint64_t *sb_slot, uint64_t *sb_code) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  uint32_t s = order ? order[i] : (uint32_t)i;
+  sb_base[i] = it.base[s];
+  sb_len[i] = it.len[s];
+  sb_ref[i] = it.ref[s];
+  sb_d0[i] = it.d0[s];
+  sb_slot[i] = it.slot[s];
+  sb_code[i] = it.key[order ? i : s] >> 27;
+}
+
+__global__ void k_items_lcp(TrieView tv, const uint64_t *sb_base, const uint32_t *sb_len, const uint32_t *sb_d0,
+                            const uint64_t *sb_code, int T, uint16_t *lcp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  if (i == 0 || sb_code[i] != sb_code[i - 1]) {
+    lcp[i] = kLcpInf;
+    return;
+  }
+  uint32_t d0 = sb_d0[i];
+  uint32_t la = sb_len[i - 1], lb = sb_len[i];
+  uint32_t lim = min(la, lb);
+  uint32_t m = d0 + (uint32_t)match_nibbles(tv.keys + sb_base[i - 1] + d0, tv.keys + sb_base[i] + d0, (int)(lim - d0));
+  if (m >= lim) {  // equal keys or one is a prefix of the other
+    set_error(tv.ctr, ERR_BAD_KEY);
+    m = lim - 1;
+  }
+  lcp[i] = (uint16_t)m;
+}
+
+// ---------------------------------------------------------------------------
+// level-synchronous subtrie construction
+
+struct SegArrays {
+  uint32_t *start, *end, *depth, *D, *branch;
+  uint64_t *slot;
+};
+
+struct SortedItems {
+  const uint64_t *base;
+  const uint32_t *len;
+  const uint32_t *ref;
+  const uint32_t *d0;
+  const uint64_t *slot;
+  const uint64_t *code;
+  const uint16_t *lcp;
+};
+
+// leaf for item i whose path is consumed up to nibble depth x
+__device__ __forceinline__ void make_leaf(const TrieView &tv, DirtyList dl, const SortedItems &si, uint32_t i,
+                                          uint32_t x, uint64_t slot, uint32_t gen) {
+  uint32_t len = si.len[i];
+  uint32_t child = si.ref[i];
+  if (x < len) {
+    uint32_t s = new_short(tv, dl, si.base[i] + x, len - x, child, x, gen);
+    if (s == 0xFFFFFFFFu) return;
+    write_slot(tv, slot, make_ref(KIND_SHORT, s));
+  } else {
+    write_slot(tv, slot, child);
+  }
+}
+
+// groups -> leaves (singletons) or first-level segments
+// kflags bits: 0 keep, 1 child/segment start, 2 child/segment end
+__global__ void k_groups_init(TrieView tv, DirtyList dl, SortedItems si, int T, uint32_t gen, uint8_t *kflags,
+                              unsigned long long *flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  bool gs = (i == 0) || si.code[i] != si.code[i - 1];
+  bool ge = (i + 1 == T) || si.code[i + 1] != si.code[i];
+  if (gs && ge) {
+    make_leaf(tv, dl, si, i, si.d0[i], si.slot[i], gen);
+    kflags[i] = 0;
+    flags[i] = 0;
+    return;
+  }
+  kflags[i] = 1 | (gs ? 2 : 0) | (ge ? 4 : 0);
+  flags[i] = 1ull | ((unsigned long long)(gs ? 1 : 0) << 32);
+}
+
+__global__ void k_groups_scatter(SortedItems si, const uint8_t *kflags, const unsigned long long *pos, int T,
+                                 uint32_t *act, uint32_t *aseg, SegArrays sg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  uint8_t f = kflags[i];
+  if (!(f & 1)) return;
+  unsigned long long q = pos[i];
+  uint32_t k = (uint32_t)q;
+  uint32_t s = (uint32_t)(q >> 32) + ((f & 2) ? 1u : 0u) - 1u;
+  act[k] = (uint32_t)i;
+  aseg[k] = s;
+  if (f & 2) {
+    sg.start[s] = (uint32_t)i;
+    sg.depth[s] = si.d0[i];
+    sg.slot[s] = si.slot[i];
+    sg.D[s] = 0xFFFFFFFFu;
+  }
+  if (f & 4) sg.end[s] = (uint32_t)i + 1;
+}
+
+// D[s] = min LCP over the interior boundaries of segment s
+__global__ void k_level_min(SortedItems si, const uint32_t *act, const uint32_t *aseg, int K, SegArrays sg) {
+  __shared__ uint32_t s_first;
+  __shared__ uint32_t wmin[32];
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool ok = k < K;
+  uint32_t s = ok ? aseg[k] : 0xFFFFFFFFu;
+  uint32_t v = 0xFFFFFFFFu;
+  if (ok) {
+    uint32_t i = act[k];
+    if (i != sg.start[s]) v = si.lcp[i];
+  }
+  if (threadIdx.x == 0) s_first = s;
+  __syncthreads();
+  int same = __syncthreads_and(!ok || s == s_first);
+  if (same) {
+    uint32_t w = __reduce_min_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t b = wmin[0];
+      for (int i = 1; i < (int)(blockDim.x >> 5); ++i) b = min(b, wmin[i]);
+      if (b != 0xFFFFFFFFu && s_first != 0xFFFFFFFFu) atomicMin(&sg.D[s_first], b);
+    }
+    return;
+  }
+  unsigned peers = __match_any_sync(0xffffffffu, s);
+  uint32_t w = __reduce_min_sync(peers, v);
+  if (ok && (int)(threadIdx.x & 31) == __ffs(peers) - 1 && w != 0xFFFFFFFFu) atomicMin(&sg.D[s], w);
+}
+
+// one branch (+ extension) per segment
+__global__ void k_level_nodes(TrieView tv, DirtyList dl, SortedItems si, int S, SegArrays sg, uint32_t gen) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  uint32_t D = sg.D[s];
+  uint32_t d = sg.depth[s];
+  uint32_t i0 = sg.start[s];
+  if (D == 0xFFFFFFFFu || D < d || D >= si.len[i0]) {
+    set_error(tv.ctr, ERR_INTERNAL);
+    sg.branch[s] = 0xFFFFFFFFu;
+    return;
+  }
+  uint32_t f = new_full(tv, dl, D, gen);
+  sg.branch[s] = f;
+  if (f == 0xFFFFFFFFu) return;
+  uint32_t top = make_ref(KIND_FULL, f);
+  if (D > d) {
+    uint32_t e = new_short(tv, dl, si.base[i0] + d, D - d, top, d, gen);
+    if (e == 0xFFFFFFFFu) return;
+    top = make_ref(KIND_SHORT, e);
+  }
+  write_slot(tv, sg.slot[s], top);
+}
+
+// children of every branch: leaves now, larger children become segments of
+// the next level
+__global__ void k_level_children(TrieView tv, DirtyList dl, SortedItems si, const uint32_t *act,
+                                 const uint32_t *aseg, int K, SegArrays sg, uint32_t gen, uint8_t *kflags,
+                                 uint8_t *knib, unsigned long long *flags) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  uint32_t i = act[k];
+  uint32_t s = aseg[k];
+  uint32_t D = sg.D[s];
+  uint32_t f = sg.branch[s];
+  if (f == 0xFFFFFFFFu) {
+    kflags[k] = 0;
+    flags[k] = 0;
+    return;
+  }
+  bool cs = (i == sg.start[s]) || si.lcp[i] == D;
+  bool ce = (i + 1 == sg.end[s]) || si.lcp[i + 1] == D;
+  uint8_t nib = tv.keys[si.base[i] + D];
+  uint64_t slot = ((uint64_t)f << 5) | nib;
+  if (cs && ce) {
+    make_leaf(tv, dl, si, i, D + 1, slot, gen);
+    kflags[k] = 0;
+    flags[k] = 0;
+    return;
+  }
+  kflags[k] = 1 | (cs ? 2 : 0) | (ce ? 4 : 0);
+  knib[k] = nib;
+  flags[k] = 1ull | ((unsigned long long)(cs ? 1 : 0) << 32);
+}
+
+__global__ void k_level_scatter(const uint32_t *act, const uint32_t *aseg, const uint8_t *kflags,
+                                const uint8_t *knib, const unsigned long long *pos, int K, SegArrays cur,
+                                uint32_t *nact, uint32_t *naseg, SegArrays nxt) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  uint8_t f = kflags[k];
+  if (!(f & 1)) return;
+  unsigned long long q = pos[k];
+  uint32_t nk = (uint32_t)q;
+  uint32_t ns = (uint32_t)(q >> 32) + ((f & 2) ? 1u : 0u) - 1u;
+  uint32_t i = act[k];
+  uint32_t s = aseg[k];
+  nact[nk] = i;
+  naseg[nk] = ns;
+  if (f & 2) {
+    nxt.start[ns] = i;
+    nxt.depth[ns] = cur.D[s] + 1;
+    nxt.slot[ns] = ((uint64_t)cur.branch[s] << 5) | knib[k];
+    nxt.D[ns] = 0xFFFFFFFFu;
+  }
+  if (f & 4) nxt.end[ns] = i + 1;
+}
+
+// ---------------------------------------------------------------------------
+// PhaseHC: dirty nodes bucketed by (nibble depth, kind), deepest first
+
+__global__ void k_dirty_hist(const uint32_t *ref, const uint16_t *depth, int n, uint32_t *bins, int nbins) {
+  extern __shared__ uint32_t h[];
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t b = 2u * depth[i] + (ref_kind(ref[i]) == KIND_FULL ? 1u : 0u);
+    atomicAdd(&h[b], 1u);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+    if (h[b]) atomicAdd(&bins[b], h[b]);
+}
+
+__global__ void k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, int n, uint32_t *cursor, uint32_t *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t r = ref[i];
+  uint32_t b = 2u * depth[i] + (ref_kind(r) == KIND_FULL ? 1u : 0u);
+  unsigned peers = __match_any_sync(__activemask(), b);
+  int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&cursor[b], (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  out[base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1u))] = r;
+}
+
+// one message item: <= 8 prefix bytes, then a body read from memory
+struct EncItem {
+  uint64_t pre;
+  uint32_t pren;
+  uint32_t nib;  // body holds nibbles, packed in pairs
+  const uint8_t *body;
+  uint32_t blen;
+};
+
+__device__ __forceinline__ int be_size(uint64_t v) {
+  int s = 1;
+  while (v >>= 8) ++s;
+  return s;
+}
+
+// RLP header bytes (tag small/large) for a payload of `size`, little-endian
+__device__ __forceinline__ void rlp_head(uint64_t size, uint32_t small_tag, uint32_t large_tag, uint64_t &pre,
+                                         uint32_t &pren) {
+  if (size < 56) {
+    pre = small_tag + size;
+    pren = 1;
+    return;
+  }
+  int s = be_size(size);
+  pre = large_tag + (uint32_t)s;
+  for (int k = 0; k < s; ++k) pre |= ((size >> (8 * (s - 1 - k))) & 0xFF) << (8 * (1 + k));
+  pren = 1 + s;
+}
+
+// the item a parent writes for child `r` (node.cuh:437-450 / 548-557;
+// rlp.cuh:132-155 write_bytes; a value node's "hash" is its raw value)
+__device__ __forceinline__ EncItem child_item(const TrieView &tv, uint32_t r) {
+  EncItem it{0, 0, 0, nullptr, 0};
+  uint32_t kind = ref_kind(r), idx = ref_idx(r);
+  if (kind == KIND_NULL) {
+    it.pre = 0x80;
+    it.pren = 1;
+    return it;
+  }
+  const uint8_t *h;
+  uint32_t hl;
+  if (kind == KIND_VALUE) {
+    unsigned long long vid = tv.value_vid[idx];
+    h = tv.vals + tv.rec_off[vid];
+    hl = tv.rec_len[vid];
+  } else {
+    if (kind == KIND_FULL) {
+      h = tv.full_hash + (size_t)idx * 32;
+      hl = tv.full_hlen[idx];
+    } else {
+      h = tv.short_hash + (size_t)idx * 32;
+      hl = tv.short_hlen[idx];
+    }
+    if (tv.geth_mode && hl < 32) {  // go-ethereum embeds small nodes
+      it.body = h;
+      it.blen = hl;
+      return it;
+    }
+  }
+  it.body = h;
+  it.blen = hl;
+  if (hl == 1 && h[0] < 0x80) return it;  // single byte is its own encoding
+  rlp_head(hl, 0x80, 0xb7, it.pre, it.pren);
+  return it;
+}
+
+// compact (hex-prefix) key item: utils.cuh:361-396 hex_to_compact
+__device__ __forceinline__ EncItem compact_item(const TrieView &tv, uint64_t koff, uint32_t klen) {
+  EncItem it{0, 0, 1, nullptr, 0};
+  const uint8_t *k = tv.keys + koff;
+  uint32_t term = (klen > 0 && k[klen - 1] == 16) ? 1 : 0;
+  uint32_t ln = klen - term;
+  uint32_t odd = ln & 1;
+  uint32_t clen = ln / 2 + 1;
+  uint32_t flag = (term << 5) | (odd ? (0x10u | k[0]) : 0u);
+  it.body = k + odd;
+  it.blen = clen - 1;
+  if (clen == 1) {  // one byte < 0x80: written as itself
+    it.pre = flag;
+    it.pren = 1;
+    return it;
+  }
+  uint64_t h;
+  uint32_t hn;
+  rlp_head(clen, 0x80, 0xb7, h, hn);
+  it.pre = h | ((uint64_t)flag << (8 * hn));
+  it.pren = hn + 1;
+  return it;
+}
+
+// 16 nibble bytes -> 8 bytes (hi << 4 | lo)
+__device__ __forceinline__ uint64_t pack_pairs8(const uint8_t *p) {
+  uint64_t r = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint64_t x = load_u64_unaligned(p + 8 * h);
+    uint64_t z = ((x & 0x000F000F000F000Full) << 4) | ((x >> 8) & 0x000F000F000F000Full);
+    z = (z | (z >> 8)) & 0x0000FFFF0000FFFFull;
+    z = (z | (z >> 16)) & 0x00000000FFFFFFFFull;
+    r |= z << (32 * h);
+  }
+  return r;
+}
+
+__device__ __forceinline__ EncItem node_item(const TrieView &tv, bool full, uint32_t idx, int item,
+                                             uint64_t payload) {
+  EncItem it{0, 0, 0, nullptr, 0};
+  if (item == 0) {
+    rlp_head(payload, 0xc0, 0xf7, it.pre, it.pren);
+    return it;
+  }
+  if (full) return child_item(tv, tv.full_child[(size_t)idx * 17 + (item - 1)]);
+  if (item == 1) return compact_item(tv, tv.short_key[idx], tv.short_klen[idx]);
+  return child_item(tv, tv.short_child[idx]);
+}
+
+// Thread per dirty node: RLP-encode straight into the sponge, Keccak-256 if
+// the encoding is >= 32 bytes, else keep it raw (gpu_mpt_kernels.cuh:2885-3045
+// semantics; cpu_mpt.cuh:380-496).
+__global__ void __launch_bounds__(128) k_hash_level(TrieView tv, const uint32_t *refs, int count, uint32_t root_ref) {
+  extern __shared__ uint64_t stage_all[];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  uint32_t ref = refs[t];
+  uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
+  bool full = kind == KIND_FULL;
+  if (!full && tv.short_dead[idx]) return;
+  bool force = tv.geth_mode && ref == root_ref;
+  int nitems = full ? 18 : 3;
+  // pass 1: payload size
+  uint64_t payload = 0;
+  for (int k = 1; k < nitems; ++k) {
+    EncItem it = node_item(tv, full, idx, k, 0);
+    payload += it.pren + it.blen;
+  }
+  uint64_t hdr;
+  uint32_t hn;
+  rlp_head(payload, 0xc0, 0xf7, hdr, hn);
+  uint64_t total = payload + hn;
+  bool raw = total < 32 && !force;
+  // pass 2: stream
+  Sponge sp;
+  sp.reset(stage_all + threadIdx.x, blockDim.x);
+  int item = 0;
+  EncItem cur{hdr, hn, 0, nullptr, 0};
+  uint32_t off = 0;
+  bool pre_pending = true, last = false;
+  while (true) {
+    while (!sp.full()) {
+      if (pre_pending) {
+        pre_pending = false;
+        if (cur.pren) sp.push(cur.pre, cur.pren);
+        continue;
+      }
+      if (off < cur.blen) {
+        uint32_t nb = min(8u, cur.blen - off);
+        uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : load_u64_unaligned(cur.body + off);
+        sp.push(v & low_bytes_mask(nb), nb);
+        off += nb;
+        continue;
+      }
+      if (++item == nitems) {
+        sp.pad();
+        last = true;
+        break;
+      }
+      cur = node_item(tv, full, idx, item, payload);
+      off = 0;
+      pre_pending = true;
+    }
+    if (raw) break;
+    sp.absorb();
+    if (last) break;
+  }
+  {  // accounting: encoding bytes and absorbed blocks of this pass
+    unsigned am = __activemask();
+    unsigned long long eb = __reduce_add_sync(am, (uint32_t)total);
+    unsigned long long kb = __reduce_add_sync(am, raw ? 0u : (uint32_t)((total + 1 + 135) / 136));
+    uint32_t nh = __popc(am);
+    if ((int)(threadIdx.x & 31) == __ffs(am) - 1) {
+      atomicAdd(&tv.ctr->enc_bytes, eb);
+      atomicAdd(&tv.ctr->keccak_blocks, kb);
+      atomicAdd(&tv.ctr->hashed, nh);
+    }
+  }
+  uint8_t *hout = (full ? tv.full_hash : tv.short_hash) + (size_t)idx * 32;
+  uint64_t *o = reinterpret_cast<uint64_t *>(hout);
+  if (raw) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      uint64_t v = sp.stage[w * sp.stride];
+      int keep = (int)total - 8 * w;
+      o[w] = keep >= 8 ? v : (keep <= 0 ? 0ull : (v & ((1ull << (8 * keep)) - 1)));
+    }
+    (full ? tv.full_hlen : tv.short_hlen)[idx] = (uint8_t)total;
+  } else {
+    o[0] = sp.a[0];
+    o[1] = sp.a[1];
+    o[2] = sp.a[2];
+    o[3] = sp.a[3];
+    (full ? tv.full_hlen : tv.short_hlen)[idx] = 32;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gets (gpu_mpt_kernels.cuh:2267-2340)
+
+__device__ __forceinline__ int64_t lookup(const TrieView &tv, const uint8_t *kb, uint32_t len) {
+  uint32_t ref = *tv.root;
+  uint32_t x = 0;
+  for (uint32_t guard = 0; guard <= len + 1; ++guard) {
+    uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
+    if (kind == KIND_NULL) return -1;
+    if (kind == KIND_VALUE) return x == len ? (int64_t)tv.value_vid[idx] : -1;
+    if (kind == KIND_FULL) {
+      if (x >= len) return -1;
+      uint32_t c = kb[x];
+      if (c > 16) return -1;
+      ref = tv.full_child[(size_t)idx * 17 + c];
+      ++x;
+      continue;
+    }
+    uint32_t sl = tv.short_klen[idx];
+    if (len - x < sl) return -1;
+    if ((uint32_t)match_nibbles(tv.keys + tv.short_key[idx], kb + x, (int)sl) != sl) return -1;
+    x += sl;
+    ref = tv.short_child[idx];
+  }
+  return -1;
+}
+
+__global__ void k_gets(TrieView tv, const uint8_t *keys, const int *idx, int n, int64_t keys_bytes,
+                       uint64_t *out_hp, int *out_len, int64_t *out_vid) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int ks = idx[2 * i], ke = idx[2 * i + 1];
+  int len = ke - ks + 1;
+  bool ok = ks >= 0 && len > 0 && (int64_t)ke < keys_bytes;
+  int64_t vid = ok ? lookup(tv, keys + ks, (uint32_t)len) : -1;
+  if (out_vid) out_vid[i] = vid;
+  if (vid < 0) {
+    out_hp[i] = 0;
+    out_len[i] = 0;
+  } else {
+    out_hp[i] = tv.rec_hp[vid];
+    out_len[i] = (int)tv.rec_len[vid];
+  }
+}
+
+__global__ void k_root(TrieView tv, uint8_t *out) {
+  int t = threadIdx.x;
+  uint32_t r = *tv.root;
+  uint32_t kind = ref_kind(r), idx = ref_idx(r);
+  uint32_t len = 0;
+  const uint8_t *h = nullptr;
+  if (kind == KIND_FULL) {
+    h = tv.full_hash + (size_t)idx * 32;
+    len = tv.full_hlen[idx];
+  } else if (kind == KIND_SHORT) {
+    h = tv.short_hash + (size_t)idx * 32;
+    len = tv.short_hlen[idx];
+  } else if (kind == KIND_VALUE) {
+    unsigned long long vid = tv.value_vid[idx];
+    h = tv.vals + tv.rec_off[vid];
+    len = min(32u, tv.rec_len[vid]);
+  }
+  if (t < 32) out[t] = (h && (uint32_t)t < len) ? h[t] : 0;
+  if (t == 0) out[32] = (uint8_t)len;
+}
+
+}  // namespace gmpt

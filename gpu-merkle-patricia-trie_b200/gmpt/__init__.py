@@ -1,0 +1,219 @@
+"""Python binding of the B200 MPT library through its C ABI (include/gmpt.h).
+
+``MPT`` mirrors the reference's ``GpuMPT::Compress::MPT`` surface
+(mpt-with-compress/include/mpt/gpu_mpt.cuh:18-192) for the batched update
+path: ``puts_2phase_with_valuehp`` (PhaseNU), ``puts_latching_with_valuehp_v2``
+(LockNU), ``hash_onepass_v2`` (PhaseHC), ``gets_parallel`` and
+``get_root_hash``.  Every call goes through ``libgmpt_b200.so``; there is no
+other implementation behind it, so a missing or unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "lib" / "libgmpt_b200.so"
+
+MODE_REF = 0
+MODE_GETH = 1
+
+STATUS = {0: "ok", 1: "cuda error", 2: "bad key", 3: "capacity", 4: "retry limit", 5: "bad argument",
+          6: "internal"}
+
+# every symbol include/gmpt.h and include/libgmpt.h declare
+EXPORTS = [
+    "gmpt_version", "gmpt_create", "gmpt_destroy", "gmpt_reset", "gmpt_puts_2phase", "gmpt_puts_latching",
+    "gmpt_puts_2phase_device", "gmpt_puts_latching_device", "gmpt_hash_onepass", "gmpt_pending_targets",
+    "gmpt_get_root_hash", "gmpt_gets_parallel", "gmpt_get_values", "gmpt_get_stats", "gmpt_set_timing",
+    "gmpt_last_error", "gmpt_last_error_message", "gmpt_free_buffer", "gmpt_stream",
+    "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
+    "insert_mpt_olc", "free_mpt",
+]
+
+
+class GmptError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Stats(C.Structure):
+    _fields_ = ([(n, C.c_uint64) for n in (
+        "n_full", "n_short", "n_value", "n_records", "key_bytes", "value_bytes", "last_unique", "last_new",
+        "last_pseudo", "last_dirty", "last_levels", "last_hash_levels", "device_bytes")]
+        + [("sort_passes", C.c_uint32), ("build_levels", C.c_uint32)]
+        + [(n, C.c_float) for n in ("t_stage_ms", "t_sort_ms", "t_walk_ms", "t_build_ms", "t_hash_ms")]
+        + [(n, C.c_uint64) for n in ("last_hashed", "last_enc_bytes", "last_keccak_blocks")]
+        + [("t_hash_kernels_ms", C.c_float), ("hash_launches", C.c_uint32), ("pad", C.c_uint32)])
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class NodeSet(C.Structure):
+    _fields_ = [("hashs", C.c_void_p), ("encs", C.c_void_p), ("encs_indexs", C.c_void_p), ("num", C.c_ulonglong)]
+
+
+def build(quiet: bool = True) -> Path:
+    """Compile libgmpt_b200.so for sm_100a (nvcc; no GPU needed)."""
+    r = subprocess.run(["make", "-C", str(PKG_DIR)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("libgmpt_b200 build failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    """Load libgmpt_b200.so (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is not built; run gmpt.build() / make")
+    L = C.CDLL(str(LIB_PATH))
+    vp, i32, i64 = C.c_void_p, C.c_int, C.c_int64
+    L.gmpt_version.restype = i32
+    L.gmpt_create.restype = vp
+    L.gmpt_create.argtypes = [i32, i32]
+    L.gmpt_destroy.argtypes = [vp]
+    L.gmpt_reset.argtypes = [vp]
+    for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
+        getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, i32]
+        getattr(L, f).restype = i32
+    for f in ("gmpt_puts_2phase_device", "gmpt_puts_latching_device"):
+        getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, i32, i64, i64]
+        getattr(L, f).restype = i32
+    L.gmpt_hash_onepass.argtypes = [vp]
+    L.gmpt_pending_targets.argtypes = [vp, vp, vp]
+    L.gmpt_get_root_hash.argtypes = [vp, vp, vp]
+    L.gmpt_gets_parallel.argtypes = [vp, vp, vp, i32, vp, vp]
+    L.gmpt_get_values.argtypes = [vp, vp, vp, i32, vp, i64, vp, vp]
+    L.gmpt_get_stats.argtypes = [vp, vp]
+    L.gmpt_set_timing.argtypes = [vp, i32]
+    L.gmpt_last_error_message.restype = C.c_char_p
+    L.gmpt_stream.restype = vp
+    L.gmpt_stream.argtypes = [vp]
+    L.gmpt_free_buffer.argtypes = [vp]
+    L.preprocess.restype = i32
+    for f in ("build_mpt_2phase", "build_mpt_olc"):
+        getattr(L, f).argtypes = [i32, vp, vp, vp, vp, vp, i32]
+        getattr(L, f).restype = vp
+    for f in ("insert_mpt_2phase", "insert_mpt_olc"):
+        getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, i32]
+        getattr(L, f).restype = vp
+    L.get_all_nodes.argtypes = [i32, vp, vp, i32]
+    L.get_all_nodes.restype = NodeSet
+    L.init_mpt.restype = vp
+    L.free_mpt.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise GmptError(rc, lib().gmpt_last_error_message().decode())
+
+
+def _arrays(keys_hexs, keys_indexs, values=None, values_indexs=None):
+    kh = np.ascontiguousarray(keys_hexs, dtype=np.uint8)
+    ki = np.ascontiguousarray(keys_indexs, dtype=np.int32)
+    vb = None if values is None else np.ascontiguousarray(values, dtype=np.uint8)
+    vi = None if values_indexs is None else np.ascontiguousarray(values_indexs, dtype=np.int64)
+    return kh, ki, vb, vi
+
+
+class MPT:
+    """A device-resident trie (GpuMPT::Compress::MPT)."""
+
+    def __init__(self, device: int = 0, mode: int = MODE_REF):
+        self._L = lib()
+        self._h = self._L.gmpt_create(device, mode)
+        if not self._h:
+            raise GmptError(self._L.gmpt_last_error(), self._L.gmpt_last_error_message().decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gmpt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def reset(self):
+        _check(self._L.gmpt_reset(self._h))
+
+    # -- puts --------------------------------------------------------------
+    def puts_2phase_with_valuehp(self, keys_hexs, keys_indexs, values, values_indexs, values_hps=None):
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        hp = None if values_hps is None else np.ascontiguousarray(values_hps, dtype=np.uint64)
+        _check(self._L.gmpt_puts_2phase(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), len(ki) // 2))
+
+    def puts_latching_with_valuehp_v2(self, keys_hexs, keys_indexs, values, values_indexs, values_hps=None):
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        hp = None if values_hps is None else np.ascontiguousarray(values_hps, dtype=np.uint64)
+        _check(self._L.gmpt_puts_latching(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), len(ki) // 2))
+
+    def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
+                    values_bytes: int, d_hps: int = 0):
+        """Inputs already in HBM (raw device addresses, e.g. tensor.data_ptr())."""
+        f = self._L.gmpt_puts_2phase_device if two_phase else self._L.gmpt_puts_latching_device
+        _check(f(self._h, C.c_void_p(d_keys), C.c_void_p(d_kidx), C.c_void_p(d_vals), C.c_void_p(d_vidx),
+                 C.c_void_p(d_hps) if d_hps else None, n, keys_bytes, values_bytes))
+
+    # -- hash / root ---------------------------------------------------------
+    def hash_onepass_v2(self):
+        _check(self._L.gmpt_hash_onepass(self._h))
+
+    def pending_targets(self) -> int:
+        p = C.c_void_p()
+        n = C.c_int()
+        _check(self._L.gmpt_pending_targets(self._h, C.byref(p), C.byref(n)))
+        return n.value
+
+    def get_root_hash(self) -> bytes:
+        out = (C.c_uint8 * 32)()
+        size = C.c_int()
+        _check(self._L.gmpt_get_root_hash(self._h, out, C.byref(size)))
+        return bytes(out)[: size.value]
+
+    # -- lookups -------------------------------------------------------------
+    def gets_parallel(self, keys_hexs, keys_indexs):
+        kh, ki, _, _ = _arrays(keys_hexs, keys_indexs)
+        n = len(ki) // 2
+        hps = np.zeros(n, dtype=np.uint64)
+        sizes = np.zeros(n, dtype=np.int32)
+        _check(self._L.gmpt_gets_parallel(self._h, _p(kh), _p(ki), n, _p(hps), _p(sizes)))
+        return hps, sizes
+
+    def get_values(self, keys_hexs, keys_indexs):
+        kh, ki, _, _ = _arrays(keys_hexs, keys_indexs)
+        n = len(ki) // 2
+        idx = np.zeros(2 * n, dtype=np.int64)
+        need = C.c_int64()
+        rc = self._L.gmpt_get_values(self._h, _p(kh), _p(ki), n, None, 0, _p(idx), C.byref(need))
+        buf = np.zeros(max(need.value, 1), dtype=np.uint8)
+        _check(self._L.gmpt_get_values(self._h, _p(kh), _p(ki), n, _p(buf), len(buf), _p(idx), C.byref(need)))
+        del rc
+        return [None if idx[2 * i] < 0 else buf[idx[2 * i]: idx[2 * i + 1] + 1].tobytes() for i in range(n)]
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self._L.gmpt_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def stream_ptr(self) -> int:
+        return self._L.gmpt_stream(self._h) or 0
+
+    def set_timing(self, on: bool = True):
+        _check(self._L.gmpt_set_timing(self._h, 1 if on else 0))

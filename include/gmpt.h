@@ -1,0 +1,131 @@
+/*
+ * gmpt.h -- handle-based C ABI of the B200 MPT library (libgmpt_b200.so).
+ *
+ * One call per method of the reference's GpuMPT::Compress::MPT surface
+ * (mpt-with-compress/include/mpt/gpu_mpt.cuh:18-192) that the batched update
+ * path uses, plus the additive status / buffer calls the reference lacks.
+ * Plain pointers and sizes only; every call is synchronous on the trie's own
+ * CUDA stream and returns a gmpt_status (0 = ok).
+ *
+ * Batch layout (as in the reference): keys_hexs holds hex-nibble keys (one
+ * byte per nibble, 16 = terminator, util/utils.cuh:340-349); keys_indexs and
+ * values_indexs hold inclusive [start, end] pairs (int / int64_t); values_hps
+ * (may be NULL) are the caller's host pointers that lookups echo back.
+ * Semantics: keys of one batch are applied as if inserted in index order
+ * (the last occurrence of a key wins) and an existing key's value is
+ * replaced, for both insert strategies.
+ */
+#ifndef GMPT_H
+#define GMPT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gmpt_trie gmpt_trie;
+
+enum gmpt_status {
+  GMPT_OK = 0,
+  GMPT_E_CUDA = 1,        /* CUDA runtime error (message in gmpt_last_error_message) */
+  GMPT_E_BAD_KEY = 2,     /* nibble > 16, terminator not last, prefix key, too long */
+  GMPT_E_CAPACITY = 3,    /* more than 2^30 nodes of one kind, or out of memory */
+  GMPT_E_RETRY_LIMIT = 4, /* a LockNU insert exceeded its CAS retry budget */
+  GMPT_E_ARG = 5,         /* invalid argument */
+  GMPT_E_INTERNAL = 6
+};
+
+/* Encoding of children shorter than 32 bytes and of the root. */
+enum gmpt_encode_mode {
+  GMPT_MODE_REF = 0,  /* the reference: RLP string of the raw child, raw small root */
+  GMPT_MODE_GETH = 1  /* go-ethereum: embedded child, root always hashed */
+};
+
+typedef struct gmpt_stats {
+  uint64_t n_full, n_short, n_value, n_records;
+  uint64_t key_bytes, value_bytes;
+  uint64_t last_unique, last_new, last_pseudo, last_dirty, last_levels, last_hash_levels;
+  uint64_t device_bytes;
+  uint32_t sort_passes, build_levels;
+  float t_stage_ms, t_sort_ms, t_walk_ms, t_build_ms, t_hash_ms;
+  uint64_t last_hashed, last_enc_bytes, last_keccak_blocks; /* last PhaseHC pass */
+  float t_hash_kernels_ms; /* encode+Keccak kernels of the last pass (timing mode) */
+  uint32_t hash_launches, pad;
+} gmpt_stats;
+
+int gmpt_version(void);
+
+/* MPT::MPT() (gpu_mpt.cuh:162-173): an empty trie on `device`. */
+gmpt_trie *gmpt_create(int device, int encode_mode);
+void gmpt_destroy(gmpt_trie *t);
+/* drop every node (capacity is kept) */
+int gmpt_reset(gmpt_trie *t);
+
+/* puts_2phase_with_valuehp (gpu_mpt.cuh:95-97, 1262-1399): PhaseNU batch
+ * insert from HOST arrays.  Marks the touched nodes dirty; call
+ * gmpt_hash_onepass() to rehash. */
+int gmpt_puts_2phase(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                     const uint8_t *values_bytes, const int64_t *values_indexs,
+                     const uint8_t *const *values_hps, int n);
+
+/* puts_latching_with_valuehp_v2 (gpu_mpt.cuh:69-71, 554-615): LockNU batch
+ * insert from HOST arrays. */
+int gmpt_puts_latching(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                       const uint8_t *values_bytes, const int64_t *values_indexs,
+                       const uint8_t *const *values_hps, int n);
+
+/* Same two inserts with DEVICE-resident inputs (d_values_hps: n uint64 host
+ * addresses in device memory, or NULL); keys_bytes / values_bytes are the
+ * lengths of the key and value streams. */
+int gmpt_puts_2phase_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                            const uint8_t *d_values_bytes, const int64_t *d_values_indexs,
+                            const uint64_t *d_values_hps, int n, int64_t keys_bytes,
+                            int64_t values_bytes);
+int gmpt_puts_latching_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                              const uint8_t *d_values_bytes, const int64_t *d_values_indexs,
+                              const uint64_t *d_values_hps, int n, int64_t keys_bytes,
+                              int64_t values_bytes);
+
+/* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
+ * dirty since the last call. */
+int gmpt_hash_onepass(gmpt_trie *t);
+
+/* The device array of dirty node references pending for gmpt_hash_onepass
+ * (the reference returns it from the puts as std::tuple<Node**, int>). */
+int gmpt_pending_targets(gmpt_trie *t, const uint32_t **d_targets, int *n);
+
+/* get_root_hash (gpu_mpt.cuh:151-152, 1217-1247): *size = 0 for an empty
+ * trie, < 32 for a raw root in GMPT_MODE_REF, else 32. */
+int gmpt_get_root_hash(gmpt_trie *t, uint8_t out[32], int *size);
+
+/* gets_parallel (gpu_mpt.cuh:139-140, 984-1036): values_hps[i] receives the
+ * host pointer given with the stored value (NULL when the key is absent or
+ * none was given) and values_sizes[i] its length (0 when absent). */
+int gmpt_gets_parallel(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int n,
+                       const uint8_t **values_hps, int *values_sizes);
+
+/* Value bytes stored for each key, concatenated into out (capacity out_cap);
+ * out_indexs[2i], out_indexs[2i+1] = inclusive range, or -1, -1 if absent.
+ * *out_len = bytes written (or needed, when out_cap is too small). */
+int gmpt_get_values(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int n,
+                    uint8_t *out, int64_t out_cap, int64_t *out_indexs, int64_t *out_len);
+
+int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
+/* per-phase CUDA-event timing into gmpt_stats (adds synchronisation) */
+int gmpt_set_timing(gmpt_trie *t, int on);
+
+/* The trie's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or events against it. */
+void *gmpt_stream(gmpt_trie *t);
+
+/* Status of the last failed call on this thread, and its message. */
+int gmpt_last_error(void);
+const char *gmpt_last_error_message(void);
+/* Free memory returned by the libgmpt.h calls (roots, nodesets). */
+void gmpt_free_buffer(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

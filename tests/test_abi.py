@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+import gmpt
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = set()
+    for h in sorted((REPO / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"([A-Za-z_][A-Za-z0-9_]*)\s*\(", text):
+            name = m.group(1)
+            if name in ("if", "defined", "sizeof", "extern"):
+                continue
+            # function declarations end with ');' at top level
+            rest = text[m.end():]
+            depth, i = 1, 0
+            while depth and i < len(rest):
+                depth += {"(": 1, ")": -1}.get(rest[i], 0)
+                i += 1
+            if rest[i:].lstrip().startswith(";"):
+                names.add(name)
+    return names
+
+
+def test_library_builds_and_loads():
+    if not gmpt.LIB_PATH.exists():
+        gmpt.build()
+    L = gmpt.lib()
+    assert L.gmpt_version() == 1
+
+
+def test_every_declared_symbol_is_exported():
+    gmpt.lib()
+    so = ctypes.CDLL(str(gmpt.LIB_PATH))
+    names = declared_functions()
+    assert {"build_mpt_2phase", "build_mpt_olc", "preprocess", "get_all_nodes", "init_mpt",
+            "insert_mpt_2phase", "insert_mpt_olc", "free_mpt"} <= names
+    missing = [n for n in sorted(names) if not hasattr(so, n)]
+    assert not missing, missing
+    assert set(gmpt.EXPORTS) >= names
+
+
+def test_reference_abi_types_match():
+    # struct nodeset and enum TrieType keep the reference layout (lib/libgmpt.h:7-18)
+    assert ctypes.sizeof(gmpt.NodeSet) == 32
+    text = (REPO / "include" / "libgmpt.h").read_text()
+    assert "STATE_TRIE = 0" in text and "TRANSACTION_TRIE = 1" in text and "RECEIPT_TRIE = 2" in text
