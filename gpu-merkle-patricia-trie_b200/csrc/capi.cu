@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI (include/gmpt.h and the reference's include/libgmpt.h)
 // over gmpt::Trie.  No exceptions or exits cross the boundary.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -186,6 +187,48 @@ int gmpt_set_timing(gmpt_trie *t, int on) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   t->t->set_timing(on != 0);
   return record(0, "");
+}
+
+uint64_t gmpt_launch_count(void) { return gmpt::launch_count(); }
+
+int gmpt_keccak256_batch(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32) {
+  if (n < 0 || (n > 0 && (!data || !indexs || !out32))) return record(GMPT_E_ARG, "null argument");
+  if (n == 0) return record(0, "");
+  int64_t bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    if (indexs[2 * i] < 0 || indexs[2 * i + 1] < indexs[2 * i] - 1) return record(GMPT_E_ARG, "bad index pair");
+    bytes = std::max<int64_t>(bytes, indexs[2 * i + 1] + 1);
+  }
+  uint8_t *d_data = nullptr, *d_out = nullptr;
+  int64_t *d_idx = nullptr;
+  cudaStream_t st = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&d_data, (size_t)bytes + 64);
+  if (e == cudaSuccess) e = cudaMalloc(&d_idx, sizeof(int64_t) * 2 * (size_t)n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, 32 * (size_t)n);
+  if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d_data, data, (size_t)bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, indexs, sizeof(int64_t) * 2 * (size_t)n, cudaMemcpyHostToDevice, st);
+  int rc = e == cudaSuccess ? gmpt::keccak256_batch_device(d_data, d_idx, n, d_out, st) : GMPT_E_CUDA;
+  if (rc == 0) e = cudaMemcpyAsync(out32, d_out, 32 * (size_t)n, cudaMemcpyDeviceToHost, st);
+  if (rc == 0 && e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_data);
+  cudaFree(d_idx);
+  cudaFree(d_out);
+  if (st) cudaStreamDestroy(st);
+  if (rc == 0 && e != cudaSuccess) rc = GMPT_E_CUDA;
+  return record(rc, rc ? std::string("keccak batch: ") + cudaGetErrorString(e) : std::string());
+}
+
+int gmpt_keccak256_batch_device(const uint8_t *d_data, const int64_t *d_indexs, int n, uint8_t *d_out32,
+                                void *stream) {
+  if (n < 0 || (n > 0 && (!d_data || !d_indexs || !d_out32))) return record(GMPT_E_ARG, "null argument");
+  return record(gmpt::keccak256_batch_device(d_data, d_indexs, n, d_out32, static_cast<cudaStream_t>(stream)),
+                "keccak batch failed");
+}
+
+int gmpt_keccak_peak(int device, double *perm_per_s) {
+  if (!perm_per_s) return record(GMPT_E_ARG, "null argument");
+  return record(gmpt::keccak_peak(device, perm_per_s), "keccak probe failed");
 }
 
 void *gmpt_stream(gmpt_trie *t) { return t ? static_cast<void *>(t->t->stream()) : nullptr; }

@@ -17,6 +17,10 @@
 
 namespace gmpt {
 
+// Kernel launches issued by this library (process-wide, host side).
+uint64_t launch_count();
+void count_launch();
+
 // ---------------------------------------------------------------------------
 // device buffer with grow-on-demand (workspace)
 
@@ -133,18 +137,18 @@ cudaError_t exclusive_scan(const T *in, T *out, int64_t n, T *total_out, DevBloc
   }
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles == 1) {
-    k_scan_tiles<T><<<1, kScanThreads, 0, st>>>(in, out, nullptr, n, total_out);
+    count_launch(), k_scan_tiles<T><<<1, kScanThreads, 0, st>>>(in, out, nullptr, n, total_out);
     return cudaGetLastError();
   }
   size_t need = ws_off + (size_t)(2 * tiles + 64) * sizeof(T);
   if (ws.bytes < need) return cudaErrorMemoryAllocation;  // caller sizes ws
   T *sums = reinterpret_cast<T *>(static_cast<char *>(ws.p) + ws_off);
   T *offs = sums + tiles;
-  k_scan_reduce<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, sums, n);
+  count_launch(), k_scan_reduce<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, sums, n);
   cudaError_t e = exclusive_scan<T>(sums, offs, tiles, (T *)nullptr, ws, st,
                                     ws_off + (size_t)(2 * tiles + 32) * sizeof(T));
   if (e != cudaSuccess) return e;
-  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, offs, n, total_out);
+  count_launch(), k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, offs, n, total_out);
   return cudaGetLastError();
 }
 
@@ -279,7 +283,7 @@ struct RadixSorter {
     if ((e = cudaMemsetAsync(mask.p, 0, 8, st)) != cudaSuccess) return e;
     int grid = (int)((n + 1023) / 1024);
     if (grid > 2048) grid = 2048;
-    k_or_diff<<<grid, 256, 0, st>>>(keys, n, mask.as<unsigned long long>());
+    count_launch(), k_or_diff<<<grid, 256, 0, st>>>(keys, n, mask.as<unsigned long long>());
     if ((e = cudaMemcpyAsync(h_mask, mask.p, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     uint64_t m = *h_mask;
@@ -296,10 +300,10 @@ struct RadixSorter {
     int np = 0;
     for (int shift = 0; shift < 64; shift += 8) {
       if (((m >> shift) & 0xFF) == 0) continue;
-      k_radix_hist<<<tiles, kSortThreads, 0, st>>>(kin, n, shift, cnt, tiles);
+      count_launch(), k_radix_hist<<<tiles, kSortThreads, 0, st>>>(kin, n, shift, cnt, tiles);
       if ((e = exclusive_scan<uint32_t>(cnt, off, (int64_t)tiles * 256, nullptr, scan_ws, st)) != cudaSuccess)
         return e;
-      k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, off, tiles);
+      count_launch(), k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, off, tiles);
       std::swap(kin, kout);
       std::swap(vin, vout);
       ++np;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -11,6 +12,7 @@
 #include "trie_kernels.cuh"
 #include "latch_kernels.cuh"
 #include "export_kernels.cuh"
+#include "keccak_batch.cuh"
 
 namespace gmpt {
 
@@ -266,7 +268,7 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (e == cudaSuccess) e = cudaMemsetAsync(karena + key_base + kbytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "stage copy");
-  k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
+  count_launch(), k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
                                                 *koff, *klen, d_max);
   e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
@@ -298,27 +300,27 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
   if (e != cudaSuccess) return check_cuda(e, "sort alloc");
-  k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
+  count_launch(), k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
   int nchunks = (int)((maxlen + 7) / 8);
   stats_.sort_passes = 0;
   for (int c = 0; c <= nchunks; ++c) {
     int cc = (c == nchunks) ? -1 : c;  // final pass: key length
-    k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
+    count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
     if (e != cudaSuccess) return check_cuda(e, "sort flags");
     int K = (int)(h_small_[0] & 0xFFFFFFFFu);
     if (K == 0) break;
-    k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval);
+    count_launch(), k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval);
     int passes = 0;
     if ((e = sorter_.sort(skey, sval, K, st_, &passes)) != cudaSuccess) return check_cuda(e, "radix sort");
     stats_.sort_passes += passes;
-    k_sort_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act, skey, sval, K, order, eqprev);
+    count_launch(), k_sort_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act, skey, sval, K, order, eqprev);
   }
-  k_keep_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
+  count_launch(), k_keep_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
-  if (e == cudaSuccess) k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, order, n, uord);
+  if (e == cudaSuccess) count_launch(), k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, order, n, uord);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "unique");
@@ -352,10 +354,10 @@ int Trie::build_levels(int T) {
   unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(T));
   if (e != cudaSuccess) return check_cuda(e, "build alloc");
-  k_groups_init<<<blocks_for(T), kThreads, 0, st_>>>(tv_, dl, si, T, gen_, kflags, flags);
+  count_launch(), k_groups_init<<<blocks_for(T), kThreads, 0, st_>>>(tv_, dl, si, T, gen_, kflags, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, T, d_tot, scan_ws_, st_);
   if (e != cudaSuccess) return check_cuda(e, "groups scan");
-  k_groups_scatter<<<blocks_for(T), kThreads, 0, st_>>>(si, kflags, pos, T, act[0], aseg[0], sg[0]);
+  count_launch(), k_groups_scatter<<<blocks_for(T), kThreads, 0, st_>>>(si, kflags, pos, T, act[0], aseg[0], sg[0]);
   if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
     return check_cuda(e, "groups");
@@ -365,13 +367,13 @@ int Trie::build_levels(int T) {
   while (K > 0) {
     ++levels;
     if (levels > kMaxKeyNibbles + 2) return fail(E_INTERNAL, "builder did not converge");
-    k_level_min<<<blocks_for(K), kThreads, 0, st_>>>(si, act[cur], aseg[cur], K, sg[cur]);
-    k_level_nodes<<<blocks_for(S), kThreads, 0, st_>>>(tv_, dl, si, S, sg[cur], gen_);
-    k_level_children<<<blocks_for(K), kThreads, 0, st_>>>(tv_, dl, si, act[cur], aseg[cur], K, sg[cur], gen_,
+    count_launch(), k_level_min<<<blocks_for(K), kThreads, 0, st_>>>(si, act[cur], aseg[cur], K, sg[cur]);
+    count_launch(), k_level_nodes<<<blocks_for(S), kThreads, 0, st_>>>(tv_, dl, si, S, sg[cur], gen_);
+    count_launch(), k_level_children<<<blocks_for(K), kThreads, 0, st_>>>(tv_, dl, si, act[cur], aseg[cur], K, sg[cur], gen_,
                                                           kflags, knib, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, K, d_tot, scan_ws_, st_);
     if (e != cudaSuccess) return check_cuda(e, "level scan");
-    k_level_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act[cur], aseg[cur], kflags, knib, pos, K, sg[cur],
+    count_launch(), k_level_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act[cur], aseg[cur], kflags, knib, pos, K, sg[cur],
                                                          act[cur ^ 1], aseg[cur ^ 1], sg[cur ^ 1]);
     if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st_)) != cudaSuccess)
@@ -432,9 +434,9 @@ int Trie::put_2phase(const BatchIn &b) {
   if (e == cudaSuccess) e = cudaMemsetAsync(&ctr_->n_pseudo, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "walk alloc");
   DirtyList dl{dirty_ref_, dirty_depth_};
-  k_walk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, dl, uord, m, koff, klen, vid_base, wo);
-  k_pseudo_ranks<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, m);
-  k_new_flags<<<blocks_for(m), kThreads, 0, st_>>>(wo.status, m, flags);
+  count_launch(), k_walk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, dl, uord, m, koff, klen, vid_base, wo);
+  count_launch(), k_pseudo_ranks<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, m);
+  count_launch(), k_new_flags<<<blocks_for(m), kThreads, 0, st_>>>(wo.status, m, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, m, d_tot, scan_ws_, st_);
   if (e != cudaSuccess) return check_cuda(e, "walk scan");
   if ((rc = sync_counters())) return rc;
@@ -462,15 +464,15 @@ int Trie::put_2phase(const BatchIn &b) {
     uint16_t *lcp = wsp<uint16_t>(ws_.lcp, (size_t)T + 1, e);
     if (e != cudaSuccess) return check_cuda(e, "items alloc");
     if (n_new > 0)
-      k_items_new<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, pos, m, uord, koff, klen, vid_base, it);
+      count_launch(), k_items_new<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, pos, m, uord, koff, klen, vid_base, it);
     if (n_pseudo > 0) {
-      k_items_pseudo<<<blocks_for(n_pseudo), kThreads, 0, st_>>>(tv_, wo, (int)n_pseudo, n_new, it);
+      count_launch(), k_items_pseudo<<<blocks_for(n_pseudo), kThreads, 0, st_>>>(tv_, wo, (int)n_pseudo, n_new, it);
       int passes = 0;
       if ((e = sorter_.sort(it.key, it.id, T, st_, &passes)) != cudaSuccess) return check_cuda(e, "group sort");
     }
-    k_items_gather<<<blocks_for(T), kThreads, 0, st_>>>(it, n_pseudo > 0 ? it.id : nullptr, T, sb_base, sb_len,
+    count_launch(), k_items_gather<<<blocks_for(T), kThreads, 0, st_>>>(it, n_pseudo > 0 ? it.id : nullptr, T, sb_base, sb_len,
                                                         sb_ref, sb_d0, sb_slot, sb_code);
-    k_items_lcp<<<blocks_for(T), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, T, lcp);
+    count_launch(), k_items_lcp<<<blocks_for(T), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, T, lcp);
     if ((rc = build_levels(T))) return rc;
   }
   if ((rc = sync_counters())) return rc;
@@ -507,7 +509,7 @@ int Trie::bucket_and_hash() {
   if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * (kMaxDepthBins + 1), st_);
   if (e != cudaSuccess) return check_cuda(e, "hash alloc");
   int grid = std::min<int>(blocks_for(nd), 148 * 4);
-  k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kMaxDepthBins, st_>>>(dirty_ref_, dirty_depth_, (int)nd, bins,
+  count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kMaxDepthBins, st_>>>(dirty_ref_, dirty_depth_, (int)nd, bins,
                                                                           kMaxDepthBins);
   std::vector<uint32_t> hb(kMaxDepthBins), off(kMaxDepthBins + 1);
   if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyDeviceToHost, st_)) !=
@@ -519,7 +521,7 @@ int Trie::bucket_and_hash() {
   if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
-  k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, (int)nd, cursor, sorted);
+  count_launch(), k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, (int)nd, cursor, sorted);
   uint32_t root_ref = 0;
   if ((e = cudaMemcpyAsync(h_small_, root_, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
@@ -540,7 +542,7 @@ int Trie::bucket_and_hash() {
     uint32_t a = off[2 * d], z = off[2 * d + 2];
     if (z == a) continue;
     ++levels;
-    k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a),
+    count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a),
                                                                                root_ref);
   }
   if (timing_) {
@@ -590,7 +592,7 @@ int Trie::root(uint8_t out[32], int *len) {
   cudaError_t e = cudaSuccess;
   uint8_t *d = wsp<uint8_t>(ws_.misc, 256, e) + 128;
   if (e != cudaSuccess) return check_cuda(e, "root alloc");
-  k_root<<<1, 32, 0, st_>>>(tv_, d);
+  count_launch(), k_root<<<1, 32, 0, st_>>>(tv_, d);
   uint8_t h[40];
   if ((e = cudaMemcpyAsync(h_small_, d, 33, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
@@ -620,7 +622,7 @@ int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool dev
   if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
   if (e != cudaSuccess) return check_cuda(e, "gets copy");
-  k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr);
+  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr);
   e = cudaMemcpyAsync(out_hp, dhp, sizeof(uint64_t) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(out_len, dlen, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
@@ -645,7 +647,7 @@ int Trie::get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, st
   if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice, st_);
   if (e != cudaSuccess) return check_cuda(e, "get_values copy");
-  k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, dvid);
+  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, dvid);
   std::vector<int64_t> vid(n);
   std::vector<int> len(n);
   e = cudaMemcpyAsync(vid.data(), dvid, 8 * (size_t)n, cudaMemcpyDeviceToHost, st_);
@@ -723,7 +725,7 @@ int Trie::put_latching(const BatchIn &b) {
   if ((rc = sync_counters())) return rc;
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
-  k_latch_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
+  count_launch(), k_latch_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) {
@@ -769,7 +771,7 @@ int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, s
     uint32_t *dummy = wsp<uint32_t>(ws_.sval, cap, e);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt, 0, 4, st_);
     if (e != cudaSuccess) return check_cuda(e, "flush alloc");
-    k_flush_collect<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, refs, d_cnt, cap);
+    count_launch(), k_flush_collect<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, refs, d_cnt, cap);
     uint32_t cnt = (uint32_t)(read_u64(d_cnt) & 0xFFFFFFFFu);
     if (cnt > cap) {
       cap = cnt;
@@ -785,11 +787,11 @@ int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, s
     unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 64, e) + 4;
     if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(cnt));
     if (e != cudaSuccess) return check_cuda(e, "flush alloc2");
-    k_flush_unique_flags<<<blocks_for(cnt), kThreads, 0, st_>>>(refs, (int)cnt, flags);
+    count_launch(), k_flush_unique_flags<<<blocks_for(cnt), kThreads, 0, st_>>>(refs, (int)cnt, flags);
     if ((e = exclusive_scan<unsigned long long>(flags, pos, cnt, d_tot, scan_ws_, st_)) != cudaSuccess)
       return check_cuda(e, "flush scan");
     int m = (int)read_u64(d_tot);
-    k_flush_sizes<<<blocks_for(cnt), kThreads, 0, st_>>>(tv_, refs, flags, pos, (int)cnt, uref, sizes);
+    count_launch(), k_flush_sizes<<<blocks_for(cnt), kThreads, 0, st_>>>(tv_, refs, flags, pos, (int)cnt, uref, sizes);
     if ((e = exclusive_scan<unsigned long long>(sizes, offs, m, d_tot, scan_ws_, st_)) != cudaSuccess)
       return check_cuda(e, "flush scan2");
     uint64_t total = read_u64(d_tot);
@@ -797,7 +799,7 @@ int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, s
     unsigned long long *d_idx = wsp<unsigned long long>(ws_.sb_slot, 2 * (size_t)m, e);
     uint8_t *d_hash = wsp<uint8_t>(ws_.sb_code, 32 * (size_t)m, e);
     if (e != cudaSuccess) return check_cuda(e, "flush alloc3");
-    k_flush_write<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uref, offs, m, d_encs, d_idx, d_hash);
+    count_launch(), k_flush_write<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uref, offs, m, d_encs, d_idx, d_hash);
     hashs.resize(32 * (size_t)m);
     encs.resize(total);
     encs_indexs.resize(2 * (size_t)m);
@@ -809,6 +811,55 @@ int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, s
     return check_cuda(e, "flush read");
   }
   return fail(E_INTERNAL, "flush: node count changed between passes");
+}
+
+}  // namespace gmpt
+
+namespace gmpt {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// Keccak-256 of n messages (inclusive [start, end] int64 index pairs into
+// data); device pointers, synchronous.
+int keccak256_batch_device(const uint8_t *d_data, const int64_t *d_idx, int n, uint8_t *d_out, cudaStream_t st) {
+  if (n <= 0) return OK;
+  size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
+  count_launch(), k_keccak256_batch<<<blocks_for(n, kHashThreads), kHashThreads, smem, st>>>(d_data, d_idx, n, d_out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? OK : E_CUDA;
+}
+
+// Permutations per second of the register-only Keccak loop on `device`.
+int keccak_peak(int device, double *perm_per_s) {
+  cudaError_t e = cudaSetDevice(device);
+  int sms = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint64_t *sink = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&sink, 64);
+  cudaEvent_t a, z;
+  cudaEventCreate(&a);
+  cudaEventCreate(&z);
+  const int blocks = sms * 16, threads = 128, iters = 64;
+  double best = 0;
+  for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    cudaEventRecord(a);
+    count_launch(), k_keccak_peak<<<blocks, threads>>>(sink, iters);
+    cudaEventRecord(z);
+    e = cudaEventSynchronize(z);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, z);
+    double r = (double)blocks * threads * iters / (ms / 1e3);
+    if (rep > 0 && r > best) best = r;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(z);
+  if (sink) cudaFree(sink);
+  if (e != cudaSuccess) return E_CUDA;
+  *perm_per_s = best;
+  return OK;
 }
 
 }  // namespace gmpt

@@ -145,4 +145,7 @@ class Trie {
   uint64_t read_u64(const void *dptr);
 };
 
+int keccak256_batch_device(const uint8_t *d_data, const int64_t *d_idx, int n, uint8_t *d_out, cudaStream_t st);
+int keccak_peak(int device, double *perm_per_s);
+
 }  // namespace gmpt

@@ -31,6 +31,7 @@ EXPORTS = [
     "gmpt_puts_2phase_device", "gmpt_puts_latching_device", "gmpt_hash_onepass", "gmpt_pending_targets",
     "gmpt_get_root_hash", "gmpt_gets_parallel", "gmpt_get_values", "gmpt_get_stats", "gmpt_set_timing",
     "gmpt_last_error", "gmpt_last_error_message", "gmpt_free_buffer", "gmpt_stream",
+    "gmpt_keccak256_batch", "gmpt_keccak256_batch_device", "gmpt_keccak_peak", "gmpt_launch_count",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -101,6 +102,10 @@ def lib():
     L.gmpt_stream.restype = vp
     L.gmpt_stream.argtypes = [vp]
     L.gmpt_free_buffer.argtypes = [vp]
+    L.gmpt_keccak256_batch.argtypes = [vp, vp, i32, vp]
+    L.gmpt_keccak256_batch_device.argtypes = [vp, vp, i32, vp, vp]
+    L.gmpt_keccak_peak.argtypes = [i32, vp]
+    L.gmpt_launch_count.restype = C.c_uint64
     L.preprocess.restype = i32
     for f in ("build_mpt_2phase", "build_mpt_olc"):
         getattr(L, f).argtypes = [i32, vp, vp, vp, vp, vp, i32]
@@ -131,6 +136,30 @@ def _arrays(keys_hexs, keys_indexs, values=None, values_indexs=None):
     vb = None if values is None else np.ascontiguousarray(values, dtype=np.uint8)
     vi = None if values_indexs is None else np.ascontiguousarray(values_indexs, dtype=np.int64)
     return kh, ki, vb, vi
+
+
+def keccak256_batch(messages) -> list:
+    """Keccak-256 of each message (bytes) on the GPU."""
+    msgs = [bytes(m) for m in messages]
+    data = np.frombuffer(b"".join(msgs) + b"\0", dtype=np.uint8)
+    idx = np.zeros(2 * len(msgs), dtype=np.int64)
+    pos = 0
+    for i, m in enumerate(msgs):
+        idx[2 * i], idx[2 * i + 1] = pos, pos + len(m) - 1
+        pos += len(m)
+    out = np.zeros(32 * max(len(msgs), 1), dtype=np.uint8)
+    _check(lib().gmpt_keccak256_batch(_p(data), _p(idx), len(msgs), _p(out)))
+    return [out[32 * i: 32 * i + 32].tobytes() for i in range(len(msgs))]
+
+
+def keccak_peak(device: int = 0) -> float:
+    v = C.c_double()
+    _check(lib().gmpt_keccak_peak(device, C.byref(v)))
+    return v.value
+
+
+def launch_count() -> int:
+    return int(lib().gmpt_launch_count())
 
 
 class MPT:

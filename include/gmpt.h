@@ -119,6 +119,21 @@ int gmpt_set_timing(gmpt_trie *t, int on);
  * work or events against it. */
 void *gmpt_stream(gmpt_trie *t);
 
+/* Keccak-256 (Ethereum padding) of n messages: data + inclusive int64
+ * [start, end] pairs -> out32[32 * n].  Host arrays; the reference's
+ * standalone batch kernel is keccak_kernel_batch
+ * (hash/batch_mode_hash.cuh:89-115). */
+int gmpt_keccak256_batch(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32);
+/* Same with device arrays, on `stream` (a cudaStream_t, or NULL). */
+int gmpt_keccak256_batch_device(const uint8_t *d_data, const int64_t *d_indexs, int n, uint8_t *d_out32,
+                                void *stream);
+/* Measurement aid: Keccak-f[1600] permutations per second of a
+ * register-only loop on `device` (the integer-pipe ceiling of the hash
+ * stage's permutation code). */
+int gmpt_keccak_peak(int device, double *perm_per_s);
+/* Number of kernels this library has launched in this process. */
+uint64_t gmpt_launch_count(void);
+
 /* Status of the last failed call on this thread, and its message. */
 int gmpt_last_error(void);
 const char *gmpt_last_error_message(void);

@@ -52,3 +52,14 @@ def test_reference_abi_types_match():
     assert ctypes.sizeof(gmpt.NodeSet) == 32
     text = (REPO / "include" / "libgmpt.h").read_text()
     assert "STATE_TRIE = 0" in text and "TRANSACTION_TRIE = 1" in text and "RECEIPT_TRIE = 2" in text
+
+
+def test_cpp_facade_compiles_against_the_headers(tmp_path):
+    import subprocess
+
+    exe = tmp_path / "facade_example"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(REPO / "include"),
+                        str(REPO / "tests" / "cpp" / "facade_example.cpp"),
+                        "-L", str(gmpt.LIB_PATH.parent), "-lgmpt_b200", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

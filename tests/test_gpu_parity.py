@@ -223,3 +223,27 @@ def test_get_all_nodes_exports_hash_consistent_encodings(gpu_lib):
     assert seen_root
     for p in (ns.hashs, ns.encs, ns.encs_indexs):
         L.gmpt_free_buffer(p)
+
+
+def test_batched_keccak256_matches_oracle(gpu_lib):
+    rng = np.random.default_rng(17)
+    msgs = [rng.integers(0, 256, n, dtype=np.uint8).tobytes()
+            for n in list(range(0, 300)) + [543, 544, 1087, 1088, 1089, 4096, 5000]]
+    assert gpu_lib.keccak256_batch(msgs) == [O.keccak256(m) for m in msgs]
+
+
+def test_cpp_facade_runs_reference_fixture(gpu_lib, golden, tmp_path):
+    import os
+    import subprocess
+    from pathlib import Path
+
+    repo = Path(__file__).resolve().parents[1]
+    exe = tmp_path / "facade_example"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(repo / "include"),
+                    str(repo / "tests" / "cpp" / "facade_example.cpp"), "-L", str(gpu_lib.LIB_PATH.parent),
+                    "-lgmpt_b200", "-o", str(exe)], check=True)
+    env = dict(os.environ, LD_LIBRARY_PATH=str(gpu_lib.LIB_PATH.parent) + ":" + os.environ.get("LD_LIBRARY_PATH", ""))
+    r = subprocess.run([str(exe)], capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stderr
+    doe = [c for c in golden if c["name"] == "doe_dog_dogglesworth"][0]
+    assert bytes.fromhex(r.stdout.strip()) == doe["roots"][0]
