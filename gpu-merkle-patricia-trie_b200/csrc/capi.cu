@@ -226,6 +226,12 @@ int gmpt_keccak256_batch_device(const uint8_t *d_data, const int64_t *d_indexs, 
                 "keccak batch failed");
 }
 
+int gmpt_keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32) {
+  std::string err;
+  int rc = gmpt::keccak256_batch_noalloc(data, indexs, n, out32, err);
+  return record(rc, err);
+}
+
 int gmpt_keccak_peak(int device, double *perm_per_s) {
   if (!perm_per_s) return record(GMPT_E_ARG, "null argument");
   return record(gmpt::keccak_peak(device, perm_per_s), "keccak probe failed");

@@ -863,3 +863,94 @@ int keccak_peak(int device, double *perm_per_s) {
 }
 
 }  // namespace gmpt
+
+// ---------------------------------------------------------------------------
+// Allocation-free batched Keccak-256 for callers that cannot allocate device
+// memory.  All device-side staging lives in one file-scope array of fixed
+// size that every GPU loading the library keeps until process exit.
+
+#include <mutex>
+
+namespace gmpt {
+
+namespace {
+
+constexpr int64_t kNoAllocMaxMessages = 32768;
+constexpr int64_t kNoAllocMaxBytes = 2ll << 20;  // message bytes per call
+constexpr int64_t kNoAllocTail = 64;             // zeroed, covers 8-byte over-reads
+constexpr int64_t kNoAllocIdxOff = kNoAllocMaxBytes + 256;
+constexpr int64_t kNoAllocOutOff = kNoAllocIdxOff + kNoAllocMaxMessages * 16;
+constexpr int64_t kNoAllocBytes = kNoAllocOutOff + kNoAllocMaxMessages * 32;  // 3.5 MiB + 256 B
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint8_t *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32, std::string &err) {
+  if (n < 0 || (n > 0 && (!data || !indexs || !out32))) {
+    err = "null argument";
+    return E_ARG;
+  }
+  if (n == 0) return OK;
+  if (n > kNoAllocMaxMessages) {
+    err = "gmpt_keccak256_batch_noalloc: " + std::to_string(n) + " messages exceed the limit of " +
+          std::to_string(kNoAllocMaxMessages);
+    return E_ARG;
+  }
+  int64_t bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    if (indexs[2 * i] < 0 || indexs[2 * i + 1] < indexs[2 * i] - 1) {
+      err = "bad index pair";
+      return E_ARG;
+    }
+    bytes = std::max<int64_t>(bytes, indexs[2 * i + 1] + 1);
+  }
+  if (bytes > kNoAllocMaxBytes) {
+    err = "gmpt_keccak256_batch_noalloc: " + std::to_string(bytes) + " message bytes exceed the limit of " +
+          std::to_string(kNoAllocMaxBytes);
+    return E_ARG;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    err = "no usable current device";
+    return E_CUDA;
+  }
+  std::lock_guard<std::mutex> g(g_noalloc_mu);  // calls share the array
+  if (!g_noalloc_ptr[dev]) {
+    // one-time set-up on this device (the current one): the device address
+    // of the array; the host-side symbol is not a device address
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return E_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<uint8_t *>(p);
+  }
+  uint8_t *base = g_noalloc_ptr[dev];
+  uint8_t *d_data = base;
+  int64_t *d_idx = reinterpret_cast<int64_t *>(base + kNoAllocIdxOff);
+  uint8_t *d_out = base + kNoAllocOutOff;
+  // legacy default stream, synchronous copies from pageable memory
+  if (bytes) e = cudaMemcpy(d_data, data, (size_t)bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(d_data + bytes, 0, kNoAllocTail);  // what the over-reads see
+  if (e == cudaSuccess) e = cudaMemcpy(d_idx, indexs, sizeof(int64_t) * 2 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
+    count_launch(), k_keccak256_batch<<<blocks_for(n, kHashThreads), kHashThreads, smem>>>(d_data, d_idx, n, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out32, d_out, 32 * (size_t)n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = std::string("keccak no-alloc: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  return OK;
+}
+
+}  // namespace gmpt

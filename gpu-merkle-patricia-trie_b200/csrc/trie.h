@@ -147,5 +147,6 @@ class Trie {
 
 int keccak256_batch_device(const uint8_t *d_data, const int64_t *d_idx, int n, uint8_t *d_out, cudaStream_t st);
 int keccak_peak(int device, double *perm_per_s);
+int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32, std::string &err);
 
 }  // namespace gmpt

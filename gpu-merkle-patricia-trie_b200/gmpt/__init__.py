@@ -32,6 +32,7 @@ EXPORTS = [
     "gmpt_get_root_hash", "gmpt_gets_parallel", "gmpt_get_values", "gmpt_get_stats", "gmpt_set_timing",
     "gmpt_last_error", "gmpt_last_error_message", "gmpt_free_buffer", "gmpt_stream",
     "gmpt_keccak256_batch", "gmpt_keccak256_batch_device", "gmpt_keccak_peak", "gmpt_launch_count",
+    "gmpt_keccak256_batch_noalloc",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -104,6 +105,8 @@ def lib():
     L.gmpt_free_buffer.argtypes = [vp]
     L.gmpt_keccak256_batch.argtypes = [vp, vp, i32, vp]
     L.gmpt_keccak256_batch_device.argtypes = [vp, vp, i32, vp, vp]
+    L.gmpt_keccak256_batch_noalloc.argtypes = [vp, vp, i32, vp]
+    L.gmpt_keccak256_batch_noalloc.restype = i32
     L.gmpt_keccak_peak.argtypes = [i32, vp]
     L.gmpt_launch_count.restype = C.c_uint64
     L.preprocess.restype = i32

@@ -127,6 +127,23 @@ int gmpt_keccak256_batch(const uint8_t *data, const int64_t *indexs, int n, uint
 /* Same with device arrays, on `stream` (a cudaStream_t, or NULL). */
 int gmpt_keccak256_batch_device(const uint8_t *d_data, const int64_t *d_indexs, int n, uint8_t *d_out32,
                                 void *stream);
+/* gmpt_keccak256_batch without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory at the point of
+ * the call: a process whose device memory is already owned by another
+ * allocator (a framework's caching allocator that reserved the GPU), or code
+ * that must not trigger cudaMalloc/cudaFree and the device-wide
+ * synchronisation they can cause.  Same inputs, outputs and results as
+ * gmpt_keccak256_batch (host arrays), but every device-side copy goes
+ * through one fixed 3.5 MiB array inside the library that each GPU loading
+ * the library keeps until the process exits.
+ * Limits: at most 32768 messages and 2 MiB of message bytes per call
+ * (larger calls fail with GMPT_E_ARG and a message naming the limit).
+ * The first call on a device looks up that array's device address (set-up,
+ * done once per device, on the current device); make that first call before
+ * any stream capture.  All calls share the one array, so calls from this
+ * process are serialised; work that overlaps a call on the same GPU through
+ * other means races with it. */
+int gmpt_keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32);
 /* Measurement aid: Keccak-f[1600] permutations per second of a
  * register-only loop on `device` (the integer-pipe ceiling of the hash
  * stage's permutation code). */
