@@ -183,6 +183,11 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out) {
   return record(0, "");
 }
 
+int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value) {
+  if (!t || !name) return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->set_option(name, value), t->t);
+}
+
 int gmpt_set_timing(gmpt_trie *t, int on) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   t->t->set_timing(on != 0);

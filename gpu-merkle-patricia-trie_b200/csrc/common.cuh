@@ -125,6 +125,10 @@ __device__ __forceinline__ uint64_t load_u64_unaligned_cg(const uint8_t *p) {
   return (lo >> sh) | (hi << (64 - sh));
 }
 
+__device__ __forceinline__ uint64_t low_mask64(int nbytes) {
+  return nbytes >= 8 ? ~0ull : ((1ull << (8 * nbytes)) - 1);
+}
+
 // 8 nibble bytes (little-endian in a u64, each 0..16) -> 32-bit big-endian
 // nibble chunk, terminator mapped to 0 (byte & 15).
 __device__ __forceinline__ uint32_t pack_nibbles8(uint64_t x) {

@@ -13,6 +13,8 @@
 #include "latch_kernels.cuh"
 #include "export_kernels.cuh"
 #include "keccak_batch.cuh"
+#include "local_build.cuh"
+#include "local_sort.cuh"
 
 namespace gmpt {
 
@@ -311,7 +313,31 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
     if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
     if (e != cudaSuccess) return check_cuda(e, "sort flags");
     int K = (int)(h_small_[0] & 0xFFFFFFFFu);
+    int S = (int)(h_small_[0] >> 32);
     if (K == 0) break;
+    if (opt_local_sort_) {
+      // still-tied runs; if the largest fits one CTA, finish every run there
+      uint32_t *rs = wsp<uint32_t>(ws_.it_id, (size_t)S, e);
+      uint32_t *re = wsp<uint32_t>(ws_.it_len, (size_t)S, e);
+      uint32_t *d_max = reinterpret_cast<uint32_t *>(d_tot + 1);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
+      if (e != cudaSuccess) return check_cuda(e, "sort runs alloc");
+      count_launch(), k_sort_runs<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, eqprev, n, rs, re);
+      count_launch(), k_run_max<<<blocks_for(S), kThreads, 0, st_>>>(rs, re, S, d_max);
+      if ((e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+          (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+        return check_cuda(e, "sort runs");
+      uint32_t maxrun = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+      if (maxrun <= (uint32_t)kSortLocalCap) {
+        const size_t smem = sizeof(LocalSortSmem);
+        if ((e = cudaFuncSetAttribute(k_local_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+          return check_cuda(e, "local sort attr");
+        count_launch(), k_local_sort<<<S, kSortLocalThreads, smem, st_>>>(tv_, rs, re, c, order, eqprev, koff, klen);
+        if ((e = cudaGetLastError()) != cudaSuccess) return check_cuda(e, "local sort");
+        break;
+      }
+    }
     count_launch(), k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval);
     int passes = 0;
     if ((e = sorter_.sort(skey, sval, K, st_, &passes)) != cudaSuccess) return check_cuda(e, "radix sort");
@@ -358,15 +384,36 @@ int Trie::build_levels(int T) {
   e = exclusive_scan<unsigned long long>(flags, pos, T, d_tot, scan_ws_, st_);
   if (e != cudaSuccess) return check_cuda(e, "groups scan");
   count_launch(), k_groups_scatter<<<blocks_for(T), kThreads, 0, st_>>>(si, kflags, pos, T, act[0], aseg[0], sg[0]);
+  uint32_t *d_max = reinterpret_cast<uint32_t *>(d_tot + 1);
+  auto read_level = [&](int S_now, int cur_now) -> cudaError_t {
+    cudaError_t x = cudaMemsetAsync(d_max, 0, 4, st_);
+    if (x == cudaSuccess && S_now > 0 && opt_local_build_)
+      count_launch(), k_seg_max<<<blocks_for(S_now), kThreads, 0, st_>>>(sg[cur_now], S_now, d_max);
+    if (x == cudaSuccess) x = cudaMemcpyAsync(h_small_, d_tot, 16, cudaMemcpyDeviceToHost, st_);
+    if (x == cudaSuccess) x = cudaStreamSynchronize(st_);
+    return x;
+  };
   if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
     return check_cuda(e, "groups");
   int K = (int)(h_small_[0] & 0xFFFFFFFFu);
   int S = (int)(h_small_[0] >> 32);
+  if ((e = read_level(S, 0)) != cudaSuccess) return check_cuda(e, "groups max");
+  uint32_t maxseg = (uint32_t)(h_small_[1] & 0xFFFFFFFFu);
   int cur = 0, levels = 0;
   while (K > 0) {
     ++levels;
     if (levels > kMaxKeyNibbles + 2) return fail(E_INTERNAL, "builder did not converge");
+    if (opt_local_build_ && maxseg <= (uint32_t)kLocalCap) {
+      // every remaining segment fits one CTA: finish all subtries there
+      const size_t smem = sizeof(LocalSmem);
+      if ((e = cudaFuncSetAttribute(k_local_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+          cudaSuccess)
+        return check_cuda(e, "local build attr");
+      count_launch(), k_local_build<<<S, kLocalThreads, smem, st_>>>(tv_, dl, si, sg[cur], gen_);
+      if ((e = cudaGetLastError()) != cudaSuccess) return check_cuda(e, "local build");
+      break;
+    }
     count_launch(), k_level_min<<<blocks_for(K), kThreads, 0, st_>>>(si, act[cur], aseg[cur], K, sg[cur]);
     count_launch(), k_level_nodes<<<blocks_for(S), kThreads, 0, st_>>>(tv_, dl, si, S, sg[cur], gen_);
     count_launch(), k_level_children<<<blocks_for(K), kThreads, 0, st_>>>(tv_, dl, si, act[cur], aseg[cur], K, sg[cur], gen_,
@@ -375,12 +422,18 @@ int Trie::build_levels(int T) {
     if (e != cudaSuccess) return check_cuda(e, "level scan");
     count_launch(), k_level_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act[cur], aseg[cur], kflags, knib, pos, K, sg[cur],
                                                          act[cur ^ 1], aseg[cur ^ 1], sg[cur ^ 1]);
+    K = 0;
+    cur ^= 1;
+    // K, S of the next level are in d_tot; the largest segment comes with them
     if ((e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st_)) != cudaSuccess)
       return check_cuda(e, "level");
     K = (int)(h_small_[0] & 0xFFFFFFFFu);
     S = (int)(h_small_[0] >> 32);
-    cur ^= 1;
+    if (K > 0 && opt_local_build_) {
+      if ((e = read_level(S, cur)) != cudaSuccess) return check_cuda(e, "level max");
+      maxseg = (uint32_t)(h_small_[1] & 0xFFFFFFFFu);
+    }
   }
   stats_.build_levels = levels;
   return OK;
@@ -413,9 +466,28 @@ int Trie::put_2phase(const BatchIn &b) {
   if ((rc = sort_unique(n, koff, klen, maxlen, &uord, &m))) return rc;
   stats_.last_unique = (uint64_t)m;
   if (timing_) cudaEventRecord(ev[2], st_);
-
-  // walk
   cudaError_t e = cudaSuccess;
+
+  if (empty_) {
+    // bulk load: one group (the root), items already sorted, no walk
+    uint64_t *sb_base = wsp<uint64_t>(ws_.sb_base, (size_t)m, e);
+    uint32_t *sb_len = wsp<uint32_t>(ws_.sb_len, (size_t)m, e);
+    uint32_t *sb_ref = wsp<uint32_t>(ws_.sb_ref, (size_t)m, e);
+    uint32_t *sb_d0 = wsp<uint32_t>(ws_.sb_d0, (size_t)m, e);
+    uint64_t *sb_slot = wsp<uint64_t>(ws_.sb_slot, (size_t)m, e);
+    uint64_t *sb_code = wsp<uint64_t>(ws_.sb_code, (size_t)m, e);
+    uint16_t *lcp = wsp<uint16_t>(ws_.lcp, (size_t)m + 1, e);
+    if (e != cudaSuccess) return check_cuda(e, "bulk alloc");
+    if ((uint64_t)n_value_ + (uint64_t)m > cap_value_) return fail(E_CAPACITY, "value pool bound");
+    count_launch(), k_items_bulk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uord, m, koff, klen, vid_base, n_value_,
+                                                                      sb_base, sb_len, sb_ref, sb_d0, sb_slot, sb_code);
+    count_launch(), k_items_lcp<<<blocks_for(m), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, m, lcp);
+    stats_.last_new = (uint64_t)m;
+    stats_.last_pseudo = 0;
+    if (timing_) cudaEventRecord(ev[3], st_);
+    if ((rc = build_levels(m))) return rc;
+  } else {
+  // walk
   WalkOut wo;
   wo.status = wsp<uint8_t>(ws_.w_status, (size_t)m, e);
   wo.code = wsp<uint64_t>(ws_.w_code, (size_t)m, e);
@@ -474,6 +546,7 @@ int Trie::put_2phase(const BatchIn &b) {
                                                         sb_ref, sb_d0, sb_slot, sb_code);
     count_launch(), k_items_lcp<<<blocks_for(T), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, T, lcp);
     if ((rc = build_levels(T))) return rc;
+  }
   }
   if ((rc = sync_counters())) return rc;
   if (timing_) {
@@ -951,6 +1024,23 @@ int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, u
     return E_CUDA;
   }
   return OK;
+}
+
+}  // namespace gmpt
+
+namespace gmpt {
+
+int Trie::set_option(const std::string &name, int64_t value) {
+  err_.clear();
+  if (name == "local_build") {
+    opt_local_build_ = value != 0;
+    return OK;
+  }
+  if (name == "local_sort") {
+    opt_local_sort_ = value != 0;
+    return OK;
+  }
+  return fail(E_ARG, "unknown option: " + name);
 }
 
 }  // namespace gmpt

@@ -85,6 +85,8 @@ class Trie {
   cudaStream_t stream() const { return st_; }
   int device() const { return dev_; }
   void set_timing(bool on) { timing_ = on; }
+  // tuning knobs (names: "local_build", "local_sort")
+  int set_option(const std::string &name, int64_t value);
 
  private:
   int dev_ = 0;
@@ -93,6 +95,8 @@ class Trie {
   std::string err_;
   TrieStats stats_{};
   bool timing_ = false;
+  bool opt_local_build_ = true;  // finish small build segments in one CTA each
+  bool opt_local_sort_ = true;   // finish small tied sort runs in one CTA each
 
   // node pools (capacities in elements)
   TrieView tv_{};

@@ -114,11 +114,14 @@ __global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uin
     bad = true;
   }
   if (!bad) {
+    // every byte but the last is a nibble (< 16); the last is <= 16
     const uint8_t *k = tv.keys + off;
-    for (int j = 0; j < len; ++j) {
-      uint8_t b = k[j];
-      if (b > 16 || (b == 16 && j != len - 1)) bad = true;
+    uint64_t acc = 0;
+    for (int j = 0; j < len - 1; j += 8) {
+      int m = min(8, len - 1 - j);
+      acc |= load_u64_unaligned(k + j) & low_mask64(m);
     }
+    if ((acc & 0xF0F0F0F0F0F0F0F0ull) || k[len - 1] > 16) bad = true;
   }
   if (bad) {
     set_error(tv.ctr, ERR_BAD_KEY);
@@ -385,6 +388,25 @@ __global__ void k_items_pseudo(TrieView tv, const WalkOut wo, int n_pseudo, int 
   it.ref[i] = tv.short_child[s];
   it.d0[i] = d0;
   it.slot[i] = wo.p_slot[p];
+}
+
+// Empty trie: every unique key is a new item of the single root group, already
+// in sorted order (no walk, no grouping sort).  Value node j = vbase + j.
+__global__ void k_items_bulk(TrieView tv, const uint32_t *uord, int m, const uint64_t *koff, const uint32_t *klen,
+                             uint64_t vid_base, uint32_t vbase, uint64_t *sb_base, uint32_t *sb_len,
+                             uint32_t *sb_ref, uint32_t *sb_d0, uint64_t *sb_slot, uint64_t *sb_code) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  if (j == 0) atomicAdd(&tv.ctr->n_value, (uint32_t)m);
+  uint32_t item = uord[j];
+  uint32_t v = vbase + (uint32_t)j;
+  tv.value_vid[v] = vid_base + item;
+  sb_base[j] = koff[item];
+  sb_len[j] = klen[item];
+  sb_ref[j] = make_ref(KIND_VALUE, v);
+  sb_d0[j] = 0;
+  sb_slot[j] = kSlotRoot;
+  sb_code[j] = 0;
 }
 
 // gather items into sorted order, group starts, and adjacent LCPs

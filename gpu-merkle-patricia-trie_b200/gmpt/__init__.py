@@ -32,7 +32,7 @@ EXPORTS = [
     "gmpt_get_root_hash", "gmpt_gets_parallel", "gmpt_get_values", "gmpt_get_stats", "gmpt_set_timing",
     "gmpt_last_error", "gmpt_last_error_message", "gmpt_free_buffer", "gmpt_stream",
     "gmpt_keccak256_batch", "gmpt_keccak256_batch_device", "gmpt_keccak_peak", "gmpt_launch_count",
-    "gmpt_keccak256_batch_noalloc",
+    "gmpt_keccak256_batch_noalloc", "gmpt_set_option",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -99,6 +99,7 @@ def lib():
     L.gmpt_get_values.argtypes = [vp, vp, vp, i32, vp, i64, vp, vp]
     L.gmpt_get_stats.argtypes = [vp, vp]
     L.gmpt_set_timing.argtypes = [vp, i32]
+    L.gmpt_set_option.argtypes = [vp, C.c_char_p, i64]
     L.gmpt_last_error_message.restype = C.c_char_p
     L.gmpt_stream.restype = vp
     L.gmpt_stream.argtypes = [vp]
@@ -243,6 +244,9 @@ class MPT:
         s = Stats()
         _check(self._L.gmpt_get_stats(self._h, C.byref(s)))
         return s.as_dict()
+
+    def set_option(self, name: str, value: int):
+        _check(self._L.gmpt_set_option(self._h, name.encode(), int(value)))
 
     def stream_ptr(self) -> int:
         return self._L.gmpt_stream(self._h) or 0

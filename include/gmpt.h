@@ -112,6 +112,11 @@ int gmpt_get_values(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_inde
                     uint8_t *out, int64_t out_cap, int64_t *out_indexs, int64_t *out_len);
 
 int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
+/* Tuning knobs of the batch pipeline (results never depend on them):
+ *   "local_build" 1/0: finish build segments of <= 2048 keys inside one CTA
+ *                      each (default 1) or keep every level device-wide;
+ *   "local_sort"  1/0: same for the still-tied runs of the batch sort. */
+int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value);
 /* per-phase CUDA-event timing into gmpt_stats (adds synchronisation) */
 int gmpt_set_timing(gmpt_trie *t, int on);
 

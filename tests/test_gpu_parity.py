@@ -247,3 +247,24 @@ def test_cpp_facade_runs_reference_fixture(gpu_lib, golden, tmp_path):
     assert r.returncode == 0, r.stderr
     doe = [c for c in golden if c["name"] == "doe_dog_dogglesworth"][0]
     assert bytes.fromhex(r.stdout.strip()) == doe["roots"][0]
+
+
+@pytest.mark.parametrize("local", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_pipeline_knobs_do_not_change_results(gpu_lib, local):
+    # device-wide levels vs CTA-local completion of the sort and the build
+    rng = W.Xoshiro256ss(1234)
+    batches = [W.vocab_keys(3000, seed=77, vmin=40, vmax=300, vmu=4.5),
+               W.ycsb_load(6000, seed=78), W.random_keys(5000, seed=79)]
+    # small alphabet: deep tries and many ties
+    keys = [nib(bytes(int(x) % 3 for x in rng.words(3 + int(rng.words(1)[0] % 9)))) for _ in range(4000)]
+    batches.append(make_batch(keys, [rng.bytes(40).tobytes() for _ in keys]))
+    roots, o = oracle_root(batches)
+    t = gpu_lib.MPT()
+    t.set_option("local_build", local[0])
+    t.set_option("local_sort", local[1])
+    for b, r in zip(batches, roots):
+        t.puts_2phase_with_valuehp(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+        t.hash_onepass_v2()
+        assert t.get_root_hash() == r
+    for b in batches:
+        assert t.get_values(b.keys_hexs, b.keys_indexs) == o.gets(b.keys_hexs, b.keys_indexs)
