@@ -54,18 +54,13 @@ __device__ __forceinline__ void init_short(const TrieView &tv, uint32_t s, uint6
   tv.short_hlen[s] = 0;
 }
 
-__global__ void k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff, const uint32_t *klen, int n,
-                               uint64_t vid_base, uint32_t retry_limit) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Insert key i continuing from slot `sp` at nibble depth `x` (the root and
+// depth 0 for a fresh start): CAS-based, retries bounded by retry_limit.
+__device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp, uint32_t x, uint64_t ko,
+                                        uint32_t len, unsigned long long vid, uint32_t retry_limit) {
   const uint32_t gen = tv.gen;
-  const uint64_t ko = koff[i];
   const uint8_t *kb = tv.keys + ko;
-  const uint32_t len = klen[i];
-  const unsigned long long vid = vid_base + (unsigned long long)i;
   uint32_t vnode = 0xFFFFFFFFu, leaf = 0xFFFFFFFFu, br = 0xFFFFFFFFu, up = 0xFFFFFFFFu, left = 0xFFFFFFFFu;
-  uint32_t *sp = tv.root;
-  uint32_t x = 0;
   uint32_t fails = 0;
   for (uint32_t guard = 0; guard < len + 2 + retry_limit; ++guard) {
     uint32_t ref = load_slot(sp);
@@ -177,6 +172,80 @@ __global__ void k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff, 
     set_error(tv.ctr, ERR_RETRY_LIMIT);
   else
     set_error(tv.ctr, ERR_BAD_KEY);
+}
+
+// Thread per kLatchWays keys: the keys advance one node per round together,
+// so a thread keeps several independent pointer chases in flight.  The
+// read-only descent marks the path dirty and resolves keys that exist
+// (atomicMax of the record id); a key that needs a new leaf or a split is
+// handed to latch_from at the slot where its descent stopped.
+constexpr int kLatchWays = 4;
+
+__global__ void __launch_bounds__(256, 3) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
+                                                      const uint32_t *klen, int n, uint64_t vid_base,
+                                                      uint32_t retry_limit) {
+  const uint32_t gen = tv.gen;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t *sp[kLatchWays];
+  uint32_t x[kLatchWays], len[kLatchWays];
+  uint64_t ko[kLatchWays];
+  uint8_t st[kLatchWays];  // 0 done, 1 walking, 2 hand off to latch_from
+#pragma unroll
+  for (int w = 0; w < kLatchWays; ++w) {
+    const int i = t + w * nthreads;
+    st[w] = i < n ? 1 : 0;
+    sp[w] = tv.root;
+    x[w] = 0;
+    ko[w] = i < n ? koff[i] : 0;
+    len[w] = i < n ? klen[i] : 0;
+  }
+  for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
+    uint32_t ref[kLatchWays];
+#pragma unroll
+    for (int w = 0; w < kLatchWays; ++w) ref[w] = st[w] == 1 ? __ldcg(sp[w]) : 0u;
+    bool any = false;
+#pragma unroll
+    for (int w = 0; w < kLatchWays; ++w) {
+      if (st[w] != 1) continue;
+      const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
+      const uint8_t *kb = tv.keys + ko[w];
+      if (kind == KIND_FULL) {
+        mark_full(tv, dl, idx, gen);
+        if (x[w] >= len[w]) {
+          st[w] = 2;
+          continue;
+        }
+        sp[w] = tv.full_child + (size_t)idx * 17 + kb[x[w]];
+        ++x[w];
+        any = true;
+      } else if (kind == KIND_SHORT) {
+        const uint64_t sko = __ldcg(tv.short_key + idx);
+        const uint32_t sl = __ldcg(tv.short_klen + idx);
+        const uint32_t lim = min(sl, len[w] - x[w]);
+        const uint32_t mm = (uint32_t)match_nibbles(tv.keys + sko, kb + x[w], (int)lim);
+        if (mm != sl) {
+          st[w] = 2;  // split (or a malformed key): CAS path
+          continue;
+        }
+        mark_short(tv, dl, idx, gen);
+        sp[w] = tv.short_child + idx;
+        x[w] += sl;
+        any = true;
+      } else if (kind == KIND_VALUE && x[w] == len[w]) {
+        atomicMax(&tv.value_vid[idx], vid_base + (unsigned long long)(t + w * nthreads));
+        st[w] = 0;
+      } else {
+        st[w] = 2;  // empty slot (new leaf) or malformed key
+      }
+    }
+    if (!any) break;
+  }
+#pragma unroll
+  for (int w = 0; w < kLatchWays; ++w)
+    if (st[w] != 0)
+      latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)(t + w * nthreads),
+                 retry_limit);
 }
 
 }  // namespace gmpt

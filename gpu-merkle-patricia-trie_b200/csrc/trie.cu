@@ -506,7 +506,8 @@ int Trie::put_2phase(const BatchIn &b) {
   if (e == cudaSuccess) e = cudaMemsetAsync(&ctr_->n_pseudo, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "walk alloc");
   DirtyList dl{dirty_ref_, dirty_depth_};
-  count_launch(), k_walk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, dl, uord, m, koff, klen, vid_base, wo);
+  count_launch(), k_walk<<<blocks_for((m + kWalkWays - 1) / kWalkWays), kThreads, 0, st_>>>(tv_, dl, uord, m, koff,
+                                                                                             klen, vid_base, wo);
   count_launch(), k_pseudo_ranks<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, m);
   count_launch(), k_new_flags<<<blocks_for(m), kThreads, 0, st_>>>(wo.status, m, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, m, d_tot, scan_ws_, st_);
@@ -798,7 +799,8 @@ int Trie::put_latching(const BatchIn &b) {
   if ((rc = sync_counters())) return rc;
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
-  count_launch(), k_latch_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
+  count_launch(), k_latch_insert<<<blocks_for((b.n + kLatchWays - 1) / kLatchWays), kThreads, 0, st_>>>(
+      tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) {

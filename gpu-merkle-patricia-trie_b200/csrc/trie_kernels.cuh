@@ -243,79 +243,114 @@ struct WalkOut {
   uint32_t *p_max;
 };
 
-__global__ void k_walk(TrieView tv, DirtyList dl, const uint32_t *uord, int m, const uint64_t *koff,
-                       const uint32_t *klen, uint64_t vid_base, WalkOut wo) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= m) return;
-  uint32_t item = uord[j];
-  const uint8_t *kb = tv.keys + koff[item];
-  uint32_t len = klen[item];
-  uint32_t ref = *tv.root;
-  uint32_t x = 0;
-  uint64_t slot = kSlotRoot;
-  uint32_t gen = tv.gen;
-  for (uint32_t guard = 0; guard <= len + 1; ++guard) {
-    uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
-    if (kind == KIND_NULL) {
-      wo.status[j] = W_NEW;
-      wo.code[j] = (slot == kSlotRoot) ? 0ull : code_full((uint32_t)(slot >> 5), (uint32_t)(slot & 31));
-      wo.d0[j] = x;
-      wo.slot[j] = slot;
-      return;
-    }
-    if (kind == KIND_FULL) {
-      mark_full(tv, dl, idx, gen);
-      if (x >= len) break;
-      uint32_t c = kb[x];
-      slot = ((uint64_t)idx << 5) | c;
-      ref = tv.full_child[(size_t)idx * 17 + c];
-      ++x;
-      continue;
-    }
-    if (kind == KIND_SHORT) {
-      const uint8_t *sk = tv.keys + tv.short_key[idx];
-      uint32_t sl = tv.short_klen[idx];
-      uint32_t lim = min(sl, len - x);
-      uint32_t mm = (uint32_t)match_nibbles(sk, kb + x, (int)lim);
-      if (mm == sl) {
-        mark_short(tv, dl, idx, gen);
-        ref = tv.short_child[idx];
-        x += sl;
+// Thread per kWalkWays unique keys advancing together, so each thread keeps
+// several independent pointer chases in flight (the walk is latency bound).
+constexpr int kWalkWays = 4;
+
+__global__ void __launch_bounds__(256, 2) k_walk(TrieView tv, DirtyList dl, const uint32_t *uord, int m,
+                                                 const uint64_t *koff, const uint32_t *klen, uint64_t vid_base,
+                                                 WalkOut wo) {
+  const int nthreads = gridDim.x * blockDim.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gen = tv.gen;
+  const uint32_t root = *tv.root;
+  uint32_t ref[kWalkWays], x[kWalkWays], len[kWalkWays], item[kWalkWays];
+  uint64_t slot[kWalkWays];
+  bool act[kWalkWays];
+#pragma unroll
+  for (int w = 0; w < kWalkWays; ++w) {
+    const int j = t + w * nthreads;
+    act[w] = j < m;
+    item[w] = act[w] ? uord[j] : 0;
+    len[w] = act[w] ? klen[item[w]] : 0;
+    ref[w] = root;
+    x[w] = 0;
+    slot[w] = kSlotRoot;
+  }
+  for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
+    bool any = false;
+#pragma unroll
+    for (int w = 0; w < kWalkWays; ++w) {
+      if (!act[w]) continue;
+      const int j = t + w * nthreads;
+      const uint8_t *kb = tv.keys + koff[item[w]];
+      const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
+      if (kind == KIND_NULL) {
+        wo.status[j] = W_NEW;
+        wo.code[j] = (slot[w] == kSlotRoot) ? 0ull
+                                            : code_full((uint32_t)(slot[w] >> 5), (uint32_t)(slot[w] & 31));
+        wo.d0[j] = x[w];
+        wo.slot[j] = slot[w];
+        act[w] = false;
         continue;
       }
-      if (mm == len - x) break;  // key ends inside a stored key: prefix
-      wo.status[j] = W_SPLIT;
-      wo.code[j] = code_short(idx);
-      wo.d0[j] = x;
-      wo.slot[j] = slot;
-      wo.short_id[j] = idx;
-      wo.after[j] = sym_rank(kb[x + mm]) > sym_rank(sk[mm]) ? 1 : 0;
-      // first diverger claims the split and creates the pseudo item
-      uint32_t ep = tv.epoch;
-      if (tv.short_claim[idx] != ep) {
-        if (atomicExch(&tv.short_claim[idx], ep) != ep) {
-          uint32_t p = atomicAdd(&tv.ctr->n_pseudo, 1u);
-          wo.p_short[p] = idx;
-          wo.p_d0[p] = x;
-          wo.p_slot[p] = slot;
-          wo.p_amin[p] = 0xFFFFFFFFu;
-          wo.p_max[p] = 0;
-          tv.short_pseudo[idx] = p;
-          tv.short_dead[idx] = 1;
+      if (kind == KIND_FULL) {
+        mark_full(tv, dl, idx, gen);
+        if (x[w] >= len[w]) {
+          wo.status[j] = W_ERROR;
+          set_error(tv.ctr, ERR_BAD_KEY);
+          act[w] = false;
+          continue;
         }
+        const uint32_t c = kb[x[w]];
+        slot[w] = ((uint64_t)idx << 5) | c;
+        ref[w] = tv.full_child[(size_t)idx * 17 + c];
+        ++x[w];
+        any = true;
+        continue;
       }
-      return;
+      if (kind == KIND_SHORT) {
+        const uint8_t *sk = tv.keys + tv.short_key[idx];
+        const uint32_t sl = tv.short_klen[idx];
+        const uint32_t lim = min(sl, len[w] - x[w]);
+        const uint32_t mm = (uint32_t)match_nibbles(sk, kb + x[w], (int)lim);
+        if (mm == sl) {
+          mark_short(tv, dl, idx, gen);
+          ref[w] = tv.short_child[idx];
+          x[w] += sl;
+          any = true;
+          continue;
+        }
+        act[w] = false;
+        if (mm == len[w] - x[w]) {  // key ends inside a stored key: prefix
+          wo.status[j] = W_ERROR;
+          set_error(tv.ctr, ERR_BAD_KEY);
+          continue;
+        }
+        wo.status[j] = W_SPLIT;
+        wo.code[j] = code_short(idx);
+        wo.d0[j] = x[w];
+        wo.slot[j] = slot[w];
+        wo.short_id[j] = idx;
+        wo.after[j] = sym_rank(kb[x[w] + mm]) > sym_rank(sk[mm]) ? 1 : 0;
+        // the first diverger claims the split and creates the pseudo item
+        const uint32_t ep = tv.epoch;
+        if (tv.short_claim[idx] != ep) {
+          if (atomicExch(&tv.short_claim[idx], ep) != ep) {
+            const uint32_t p = atomicAdd(&tv.ctr->n_pseudo, 1u);
+            wo.p_short[p] = idx;
+            wo.p_d0[p] = x[w];
+            wo.p_slot[p] = slot[w];
+            wo.p_amin[p] = 0xFFFFFFFFu;
+            wo.p_max[p] = 0;
+            tv.short_pseudo[idx] = p;
+            tv.short_dead[idx] = 1;
+          }
+        }
+        continue;
+      }
+      // value node
+      act[w] = false;
+      if (x[w] == len[w]) {
+        atomicMax(&tv.value_vid[idx], (unsigned long long)(vid_base + item[w]));
+        wo.status[j] = W_EXISTS;
+      } else {
+        wo.status[j] = W_ERROR;
+        set_error(tv.ctr, ERR_BAD_KEY);
+      }
     }
-    // value node
-    if (x == len) {
-      atomicMax(&tv.value_vid[idx], (unsigned long long)(vid_base + item));
-      wo.status[j] = W_EXISTS;
-      return;
-    }
-    break;
+    if (!any) break;
   }
-  wo.status[j] = W_ERROR;
-  set_error(tv.ctr, ERR_BAD_KEY);
 }
 
 __global__ void k_new_flags(const uint8_t *status, int m, unsigned long long *flags) {
@@ -769,7 +804,33 @@ __device__ __forceinline__ EncItem node_item(const TrieView &tv, bool full, uint
 // Thread per dirty node: RLP-encode straight into the sponge, Keccak-256 if
 // the encoding is >= 32 bytes, else keep it raw (gpu_mpt_kernels.cuh:2885-3045
 // semantics; cpu_mpt.cuh:380-496).
-__global__ void __launch_bounds__(128) k_hash_level(TrieView tv, const uint32_t *refs, int count, uint32_t root_ref) {
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// OR the low n bytes of v into the message at byte position p (the staged
+// block is zeroed first); a chunk may straddle two 8-byte words.
+__device__ __forceinline__ void or_bytes(uint64_t *st, uint32_t S, uint64_t v, uint32_t n, uint32_t p) {
+  if (n == 0) return;
+  const uint32_t q = p >> 3, r = p & 7;
+  st[q * S] |= v << (8 * r);
+  if (r != 0 && r + n > 8) st[(q + 1) * S] |= v >> (64 - 8 * r);
+}
+
+// Start the loads of a child item's bytes early (hash line, or the first
+// lines of a value) so the encoder's streaming reads hit L1.
+__device__ __forceinline__ void prefetch_child(const TrieView &tv, uint32_t r) {
+  uint32_t kind = ref_kind(r), idx = ref_idx(r);
+  if (kind == KIND_FULL)
+    prefetch_l1(tv.full_hash + (size_t)idx * 32);
+  else if (kind == KIND_SHORT)
+    prefetch_l1(tv.short_hash + (size_t)idx * 32);
+}
+
+// 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
+// lanes in registers without spilling at this bound.
+__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count,
+                                                        uint32_t root_ref) {
   extern __shared__ uint64_t stage_all[];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
@@ -779,20 +840,78 @@ __global__ void __launch_bounds__(128) k_hash_level(TrieView tv, const uint32_t 
   if (!full && tv.short_dead[idx]) return;
   bool force = tv.geth_mode && ref == root_ref;
   int nitems = full ? 18 : 3;
-  // pass 1: payload size
+  // pass 1: payload size (all child loads issued together, sources prefetched)
   uint64_t payload = 0;
-  for (int k = 1; k < nitems; ++k) {
-    EncItem it = node_item(tv, full, idx, k, 0);
-    payload += it.pren + it.blen;
+  EncItem it1{0, 0, 0, nullptr, 0}, it2{0, 0, 0, nullptr, 0};  // short: key, child
+  if (full) {
+    const uint32_t *chp = tv.full_child + (size_t)idx * 17;
+    uint32_t ch[17];
+#pragma unroll
+    for (int k = 0; k < 17; ++k) ch[k] = chp[k];
+#pragma unroll
+    for (int k = 0; k < 17; ++k) prefetch_child(tv, ch[k]);
+#pragma unroll
+    for (int k = 0; k < 17; ++k) {
+      EncItem it = child_item(tv, ch[k]);
+      payload += it.pren + it.blen;
+    }
+  } else {
+    uint32_t child = tv.short_child[idx];
+    const uint8_t *kp = tv.keys + tv.short_key[idx];
+    prefetch_l1(kp);
+    if (ref_kind(child) == KIND_VALUE) {
+      unsigned long long vid = tv.value_vid[ref_idx(child)];
+      const uint8_t *vp = tv.vals + tv.rec_off[vid];
+      prefetch_l1(vp);
+      if (tv.rec_len[vid] > 120) prefetch_l1(vp + 128);
+    } else {
+      prefetch_child(tv, child);
+    }
+    it1 = node_item(tv, false, idx, 1, 0);
+    it2 = node_item(tv, false, idx, 2, 0);
+    payload = it1.pren + it1.blen + it2.pren + it2.blen;
   }
   uint64_t hdr;
   uint32_t hn;
   rlp_head(payload, 0xc0, 0xf7, hdr, hn);
   uint64_t total = payload + hn;
   bool raw = total < 32 && !force;
-  // pass 2: stream
   Sponge sp;
   sp.reset(stage_all + threadIdx.x, blockDim.x);
+  if (!full && total <= 135) {
+    // One-block short node (every leaf with a value up to ~100 bytes, every
+    // extension): place each segment's 8-byte chunks into the zeroed block
+    // with shared-memory OR, pad, and permute once.
+    uint64_t *st = sp.stage;
+    const uint32_t S = sp.stride;
+#pragma unroll
+    for (int w = 0; w < 17; ++w) st[w * S] = 0;
+    uint32_t p = 0;
+    or_bytes(st, S, hdr, hn, p);
+    p += hn;
+    or_bytes(st, S, it1.pre, it1.pren, p);
+    p += it1.pren;
+    for (uint32_t o = 0; o < it1.blen; o += 8) {
+      uint32_t nb = min(8u, it1.blen - o);
+      or_bytes(st, S, pack_pairs8(it1.body + 2 * o) & low_bytes_mask(nb), nb, p + o);
+    }
+    p += it1.blen;
+    or_bytes(st, S, it2.pre, it2.pren, p);
+    p += it2.pren;
+    for (uint32_t o = 0; o < it2.blen; o += 8) {
+      uint32_t nb = min(8u, it2.blen - o);
+      or_bytes(st, S, load_u64_unaligned(it2.body + o) & low_bytes_mask(nb), nb, p + o);
+    }
+    p += it2.blen;
+    if (!raw) {
+      or_bytes(st, S, 0x01, 1, p);
+      st[16 * S] |= 0x8000000000000000ull;
+#pragma unroll
+      for (int w = 0; w < 17; ++w) sp.a[w] = st[w * S];
+      keccak_f1600(sp.a);
+    }
+  } else {
+  // pass 2: stream
   int item = 0;
   EncItem cur{hdr, hn, 0, nullptr, 0};
   uint32_t off = 0;
@@ -823,6 +942,7 @@ __global__ void __launch_bounds__(128) k_hash_level(TrieView tv, const uint32_t 
     if (raw) break;
     sp.absorb();
     if (last) break;
+  }
   }
   {  // accounting: encoding bytes and absorbed blocks of this pass
     unsigned am = __activemask();
