@@ -42,6 +42,12 @@ struct Counters {
   uint64_t key_used, val_used;
   uint32_t n_pseudo, retries_max, hashed, pad2;
   unsigned long long enc_bytes, keccak_blocks;  // last hash pass
+  // staging checks of the last batch
+  unsigned long long stream_terms;  // bytes == 16 in the key stream
+  uint32_t key_terms;               // keys whose last byte is 16
+  uint32_t noncontig;               // key index pairs do not tile the stream
+  uint32_t bad_byte;                // a byte > 16 in the stream
+  uint32_t pad3;
 };
 
 // Everything a kernel needs to reach the trie; passed by value.

@@ -181,7 +181,7 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
 // handed to latch_from at the slot where its descent stopped.
 constexpr int kLatchWays = 4;
 
-__global__ void __launch_bounds__(256, 3) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
+__global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
                                                       const uint32_t *klen, int n, uint64_t vid_base,
                                                       uint32_t retry_limit) {
   const uint32_t gen = tv.gen;
@@ -200,43 +200,103 @@ __global__ void __launch_bounds__(256, 3) k_latch_insert(TrieView tv, DirtyList 
     ko[w] = i < n ? koff[i] : 0;
     len[w] = i < n ? klen[i] : 0;
   }
+  // Each round moves every walking key down one node in phases, so the loads
+  // of all ways are in flight together: (1) slot + node fields + dirty
+  // epoch, (2) key comparison chunks of short nodes, (3) advance / resolve,
+  // (4) dirty marks (their atomics are off the descent's critical path).
   for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
-    uint32_t ref[kLatchWays];
+    uint32_t ref[kLatchWays], ep[kLatchWays], nib[kLatchWays], sl[kLatchWays], sch[kLatchWays];
+    uint64_t sko[kLatchWays];
 #pragma unroll
     for (int w = 0; w < kLatchWays; ++w) ref[w] = st[w] == 1 ? __ldcg(sp[w]) : 0u;
+#pragma unroll
+    for (int w = 0; w < kLatchWays; ++w) {
+      const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
+      ep[w] = gen;
+      nib[w] = 0;
+      sl[w] = 0;
+      sch[w] = 0;
+      sko[w] = 0;
+      if (st[w] != 1) continue;
+      if (kind == KIND_FULL) {
+        ep[w] = __ldcg(tv.full_epoch + idx);
+        nib[w] = x[w] < len[w] ? tv.keys[ko[w] + x[w]] : 0u;
+      } else if (kind == KIND_SHORT) {
+        ep[w] = __ldcg(tv.short_epoch + idx);
+        sko[w] = __ldcg(tv.short_key + idx);
+        sl[w] = __ldcg(tv.short_klen + idx);
+      }
+    }
+    // short nodes: compare the key chunk by chunk, all ways together
+    uint32_t lim[kLatchWays], mm[kLatchWays];
+    bool cmp[kLatchWays];
+#pragma unroll
+    for (int w = 0; w < kLatchWays; ++w) {
+      cmp[w] = st[w] == 1 && ref_kind(ref[w]) == KIND_SHORT;
+      lim[w] = cmp[w] ? min(sl[w], len[w] - x[w]) : 0u;
+      mm[w] = 0;
+    }
+    for (int c = 0; c < kMaxKeyNibbles / 8 + 1; ++c) {
+      bool more = false;
+#pragma unroll
+      for (int w = 0; w < kLatchWays; ++w) {
+        if (!cmp[w]) continue;
+        const uint32_t o = 8u * c;
+        if (o >= lim[w]) {
+          mm[w] = lim[w];
+          cmp[w] = false;
+          continue;
+        }
+        uint64_t d = load_u64_unaligned(tv.keys + sko[w] + o) ^ load_u64_unaligned(tv.keys + ko[w] + x[w] + o);
+        d &= low_mask64((int)min(8u, lim[w] - o));
+        if (d) {
+          mm[w] = o + (__ffsll((long long)d) - 1) / 8;
+          cmp[w] = false;
+        } else {
+          more = true;
+        }
+      }
+      if (!more) break;
+    }
     bool any = false;
 #pragma unroll
     for (int w = 0; w < kLatchWays; ++w) {
       if (st[w] != 1) continue;
       const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
-      const uint8_t *kb = tv.keys + ko[w];
       if (kind == KIND_FULL) {
-        mark_full(tv, dl, idx, gen);
         if (x[w] >= len[w]) {
           st[w] = 2;
           continue;
         }
-        sp[w] = tv.full_child + (size_t)idx * 17 + kb[x[w]];
+        sp[w] = tv.full_child + (size_t)idx * 17 + nib[w];
         ++x[w];
         any = true;
       } else if (kind == KIND_SHORT) {
-        const uint64_t sko = __ldcg(tv.short_key + idx);
-        const uint32_t sl = __ldcg(tv.short_klen + idx);
-        const uint32_t lim = min(sl, len[w] - x[w]);
-        const uint32_t mm = (uint32_t)match_nibbles(tv.keys + sko, kb + x[w], (int)lim);
-        if (mm != sl) {
+        if (mm[w] != sl[w]) {
           st[w] = 2;  // split (or a malformed key): CAS path
+          ep[w] = gen;  // a node being replaced is not marked here
           continue;
         }
-        mark_short(tv, dl, idx, gen);
         sp[w] = tv.short_child + idx;
-        x[w] += sl;
+        x[w] += sl[w];
         any = true;
       } else if (kind == KIND_VALUE && x[w] == len[w]) {
         atomicMax(&tv.value_vid[idx], vid_base + (unsigned long long)(t + w * nthreads));
         st[w] = 0;
       } else {
         st[w] = 2;  // empty slot (new leaf) or malformed key
+      }
+    }
+#pragma unroll
+    for (int w = 0; w < kLatchWays; ++w) {
+      if (ep[w] == gen) continue;
+      const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
+      if (kind == KIND_FULL) {
+        if (atomicExch(&tv.full_epoch[idx], gen) != gen)
+          dirty_push(tv.ctr, dl, ref[w], __ldcg(tv.full_depth + idx));
+      } else if (kind == KIND_SHORT) {
+        if (atomicExch(&tv.short_epoch[idx], gen) != gen)
+          dirty_push(tv.ctr, dl, ref[w], __ldcg(tv.short_depth + idx));
       }
     }
     if (!any) break;

@@ -270,12 +270,23 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (e == cudaSuccess) e = cudaMemsetAsync(karena + key_base + kbytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "stage copy");
+  if ((e = cudaMemsetAsync(&ctr_->stream_terms, 0, 24, st_)) != cudaSuccess) return check_cuda(e, "stage reset");
   count_launch(), k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
                                                 *koff, *klen, d_max);
+  if (kbytes > 0)
+    count_launch(), k_stage_stream<<<std::min<unsigned>(blocks_for(kbytes / 8 + 1), 148 * 8), kThreads, 0, st_>>>(
+        tv_, karena + key_base, kbytes);
   e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctr_, ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "stage");
   *maxlen = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  if (h_ctr_->noncontig) {
+    // index pairs do not tile the stream: check every key's interior
+    count_launch(), k_stage_keys<<<blocks_for(n), kThreads, 0, st_>>>(tv_, *koff, *klen, n);
+  } else if (h_ctr_->bad_byte || h_ctr_->stream_terms != h_ctr_->key_terms) {
+    return fail(E_BAD_KEY, "malformed key: nibble > 16 or a terminator inside a key");
+  }
   // keys are 8-aligned in the arena so chunk loads start aligned more often
   key_used_ += ((uint64_t)kbytes + 7) & ~7ull;
   val_used_ += (uint64_t)vbytes;

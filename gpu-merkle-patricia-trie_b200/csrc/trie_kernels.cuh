@@ -113,15 +113,22 @@ __global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uin
     set_error(tv.ctr, ERR_KEY_TOO_LONG);
     bad = true;
   }
+  // Interior nibbles are checked by k_stage_stream over the whole stream when
+  // the index pairs tile it (the usual layout), else by k_stage_keys.
+  bool term = false;
   if (!bad) {
-    // every byte but the last is a nibble (< 16); the last is <= 16
-    const uint8_t *k = tv.keys + off;
-    uint64_t acc = 0;
-    for (int j = 0; j < len - 1; j += 8) {
-      int m = min(8, len - 1 - j);
-      acc |= load_u64_unaligned(k + j) & low_mask64(m);
+    uint8_t last = tv.keys[off + len - 1];
+    if (last > 16) bad = true;
+    term = last == 16;
+  }
+  bool gap = (i == 0) ? (ks != 0) : (ks != ki[2 * i - 1] + 1);
+  {
+    unsigned am = __activemask();
+    unsigned tb = __ballot_sync(am, term && !bad), gb = __ballot_sync(am, gap);
+    if ((int)(threadIdx.x & 31) == __ffs(am) - 1) {
+      if (tb) atomicAdd(&tv.ctr->key_terms, (uint32_t)__popc(tb));
+      if (gb) atomicOr(&tv.ctr->noncontig, 1u);
     }
-    if ((acc & 0xF0F0F0F0F0F0F0F0ull) || k[len - 1] > 16) bad = true;
   }
   if (bad) {
     set_error(tv.ctr, ERR_BAD_KEY);
@@ -142,6 +149,45 @@ __global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uin
   tv.rec_off[vid] = val_base + (uint64_t)vs;
   tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
   tv.rec_hp[vid] = hp ? hp[i] : 0ull;
+}
+
+// Coalesced check of a key stream that the index pairs tile: no byte > 16,
+// and exactly as many 16s as keys that end in one (so none is interior).
+__global__ void k_stage_stream(TrieView tv, const uint8_t *stream, int64_t nbytes) {
+  unsigned long long terms = 0;
+  uint32_t bad = 0;
+  const int64_t nvec = nbytes / 8;
+  const uint64_t *v = reinterpret_cast<const uint64_t *>(stream);  // 8-aligned arena base
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nvec; q += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t x = __ldg(v + q);
+    bad |= (x & 0xE0E0E0E0E0E0E0E0ull) != 0;                    // >= 32
+    uint64_t hi = x & 0x1010101010101010ull;                      // bit 4 set: 16..31
+    bad |= (x & ((hi >> 4) * 0x0Full)) ? 1u : 0u;                 // 17..31: low nibble != 0
+    terms += __popcll(hi);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (nbytes & 7)) {
+    uint8_t b = stream[nvec * 8 + threadIdx.x];
+    bad |= b > 16;
+    terms += b == 16;
+  }
+  unsigned am = __activemask();
+  terms = __reduce_add_sync(am, (uint32_t)terms);
+  bad = __reduce_or_sync(am, bad);
+  if ((int)(threadIdx.x & 31) == __ffs(am) - 1) {
+    if (terms) atomicAdd(&tv.ctr->stream_terms, terms);
+    if (bad) atomicOr(&tv.ctr->bad_byte, 1u);
+  }
+}
+
+// Per-key interior check for streams the index pairs do not tile.
+__global__ void k_stage_keys(TrieView tv, const uint64_t *koff, const uint32_t *klen, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t *k = tv.keys + koff[i];
+  int len = (int)klen[i];
+  uint64_t acc = 0;
+  for (int j = 0; j < len - 1; j += 8) acc |= load_u64_unaligned(k + j) & low_mask64(min(8, len - 1 - j));
+  if (acc & 0xF0F0F0F0F0F0F0F0ull) set_error(tv.ctr, ERR_BAD_KEY);
 }
 
 // ---------------------------------------------------------------------------

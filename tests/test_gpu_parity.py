@@ -268,3 +268,27 @@ def test_pipeline_knobs_do_not_change_results(gpu_lib, local):
         assert t.get_root_hash() == r
     for b in batches:
         assert t.get_values(b.keys_hexs, b.keys_indexs) == o.gets(b.keys_hexs, b.keys_indexs)
+
+
+def test_key_streams_with_gaps_between_keys(gpu_lib):
+    # index pairs need not tile the key stream; bytes between keys are ignored
+    b = W.random_keys(2000, seed=91)
+    gap = 3
+    kh = np.zeros(len(b.keys_hexs) + gap * b.n, dtype=np.uint8) + 0xEE  # junk > 16 in the gaps
+    ki = np.zeros_like(b.keys_indexs)
+    for i in range(b.n):
+        s, e = b.keys_indexs[2 * i], b.keys_indexs[2 * i + 1]
+        ns = s + gap * (i + 1)
+        kh[ns: ns + (e - s + 1)] = b.keys_hexs[s: e + 1]
+        ki[2 * i], ki[2 * i + 1] = ns, ns + (e - s)
+    roots, _ = oracle_root([b])
+    for strategy in STRATEGIES:
+        t = gpu_lib.MPT()
+        f = t.puts_2phase_with_valuehp if strategy == "2phase" else t.puts_latching_with_valuehp_v2
+        f(kh, ki, b.values, b.values_indexs)
+        t.hash_onepass_v2()
+        assert t.get_root_hash() == roots[0]
+        bad = kh.copy()
+        bad[ki[10] + 5] = 16  # a terminator inside a key
+        with pytest.raises(gpu_lib.GmptError):
+            f(bad, ki, b.values, b.values_indexs)
