@@ -59,13 +59,17 @@ extern "C" {
 
 int gmpt_version(void) { return 1; }
 
-gmpt_trie *gmpt_create(int device, int encode_mode) {
+gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries) {
+  if (max_tries < 1 || max_tries > (1 << 30)) {
+    record(GMPT_E_ARG, "max_tries must be in [1, 2^30]");
+    return nullptr;
+  }
   gmpt_trie *h = new (std::nothrow) gmpt_trie{nullptr};
   if (!h) {
     record(GMPT_E_CAPACITY, "out of host memory");
     return nullptr;
   }
-  h->t = new (std::nothrow) gmpt::Trie(device, encode_mode);
+  h->t = new (std::nothrow) gmpt::Trie(device, encode_mode, max_tries);
   if (!h->t || !h->t->error().empty()) {
     record(GMPT_E_CUDA, h->t ? h->t->error() : "out of host memory");
     delete h->t;
@@ -75,6 +79,10 @@ gmpt_trie *gmpt_create(int device, int encode_mode) {
   record(0, "");
   return h;
 }
+
+gmpt_trie *gmpt_create(int device, int encode_mode) { return gmpt_create_forest(device, encode_mode, 1); }
+
+int gmpt_max_tries(gmpt_trie *t) { return t ? t->t->max_tries() : 0; }
 
 void gmpt_destroy(gmpt_trie *t) {
   if (!t) return;
@@ -101,6 +109,42 @@ int gmpt_puts_latching(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_i
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(
       t->t->put_latching(host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n)), t->t);
+}
+
+int gmpt_puts_2phase_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                            const uint8_t *values_bytes, const int64_t *values_indexs,
+                            const uint8_t *const *values_hps, const int *trie_ids, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (n > 0 && !trie_ids) return record(GMPT_E_ARG, "null trie_ids");
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  return record_trie(t->t->put_2phase(b), t->t);
+}
+
+int gmpt_puts_latching_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                              const uint8_t *values_bytes, const int64_t *values_indexs,
+                              const uint8_t *const *values_hps, const int *trie_ids, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (n > 0 && !trie_ids) return record(GMPT_E_ARG, "null trie_ids");
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  return record_trie(t->t->put_latching(b), t->t);
+}
+
+int gmpt_get_roots(gmpt_trie *t, const int *trie_ids, int n, uint8_t *out32, int *sizes) {
+  if (!t || (n > 0 && (!out32 || !sizes))) return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->roots(trie_ids, n, out32, sizes), t->t);
+}
+
+int gmpt_gets_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const int *trie_ids, int n,
+                     const uint8_t **values_hps, int *values_sizes) {
+  if (!t || (n > 0 && (!keys_hexs || !keys_indexs || !trie_ids || !values_hps || !values_sizes)))
+    return record(GMPT_E_ARG, "null argument");
+  for (int i = 0; i < n; ++i)
+    if (trie_ids[i] < 0 || trie_ids[i] >= t->t->max_tries()) return record(GMPT_E_ARG, "trie id outside [0, max_tries)");
+  return record_trie(t->t->gets(keys_hexs, keys_indexs, n, false, reinterpret_cast<uint64_t *>(values_hps),
+                                values_sizes, -1, trie_ids),
+                     t->t);
 }
 
 static gmpt::BatchIn device_batch(const uint8_t *k, const int *ki, const uint8_t *v, const int64_t *vi,

@@ -30,11 +30,17 @@ enum : uint32_t {
   ERR_RETRY_LIMIT = 1u << 2,   // LockNU insert exceeded its retry budget
   ERR_KEY_TOO_LONG = 1u << 3,
   ERR_INTERNAL = 1u << 4,
+  ERR_BAD_TRIE = 1u << 5,      // trie id outside [0, number of tries)
+  ERR_BARRIER = 1u << 6,       // a grid barrier wait gave up (persistent launch)
 };
 
-// Where a new subtree gets linked: a branch child slot, or the root word.
-// slot = (full index << 5) | child, or kSlotRoot.
-constexpr uint64_t kSlotRoot = ~0ull;
+// Where a new subtree gets linked: a branch child slot, or the root word of
+// one trie of the forest.  slot = (full index << 5) | child (< 2^35), or
+// ~trie for the root word of `trie` (>= 2^64 - 2^32).
+constexpr uint64_t kSlotRoot = ~0ull;  // root of trie 0
+__host__ __device__ __forceinline__ uint64_t root_slot(uint32_t trie) { return ~(uint64_t)trie; }
+__host__ __device__ __forceinline__ bool is_root_slot(uint64_t slot) { return slot >= 0xFFFFFFFF00000000ull; }
+__host__ __device__ __forceinline__ uint32_t slot_trie(uint64_t slot) { return (uint32_t)~slot; }
 
 struct Counters {
   uint32_t n_full, n_short, n_value, pad0;
@@ -77,9 +83,10 @@ struct TrieView {
   // arenas
   const uint8_t *keys;    // nibble arena (one byte per nibble, 16 = term.)
   const uint8_t *vals;    // value byte arena
-  uint32_t *root;         // root ref word
+  uint32_t *roots;        // root ref word of every trie of the forest
   Counters *ctr;
   uint32_t cap_full, cap_short, cap_value;
+  uint32_t n_tries;       // entries of roots[]
   uint32_t epoch;         // put batch number (split claims)
   uint32_t gen;           // hash generation (dirty marks)
   int geth_mode;          // 1 = embed <32 B children, hash the root always

@@ -18,13 +18,14 @@ __global__ void k_flush_collect(TrieView tv, const uint8_t *keys, const int *idx
   int ks = idx[2 * i], len = idx[2 * i + 1] - ks + 1;
   if (ks < 0 || len <= 0 || (int64_t)idx[2 * i + 1] >= keys_bytes) return;
   const uint8_t *kb = keys + ks;
-  uint32_t ref = *tv.root;
+  const uint32_t root = tv.roots[0];  // the state trie (trie 0)
+  uint32_t ref = root;
   int x = 0;
   for (int guard = 0; guard <= len + 1; ++guard) {
     uint32_t kind = ref_kind(ref), id = ref_idx(ref);
     if (kind == KIND_NULL || kind == KIND_VALUE) return;
     uint8_t hl = kind == KIND_FULL ? tv.full_hlen[id] : tv.short_hlen[id];
-    if (hl == 32 || ref == *tv.root) {
+    if (hl == 32 || ref == root) {
       uint32_t slot = atomicAdd(count, 1u);
       if (slot < cap) out[slot] = ref;
     }

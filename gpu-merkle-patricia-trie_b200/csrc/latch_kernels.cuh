@@ -183,7 +183,7 @@ constexpr int kLatchWays = 4;
 
 __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
                                                       const uint32_t *klen, int n, uint64_t vid_base,
-                                                      uint32_t retry_limit) {
+                                                      uint32_t retry_limit, const int *tid) {
   const uint32_t gen = tv.gen;
   const int nthreads = gridDim.x * blockDim.x;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList 
   for (int w = 0; w < kLatchWays; ++w) {
     const int i = t + w * nthreads;
     st[w] = i < n ? 1 : 0;
-    sp[w] = tv.root;
+    sp[w] = tv.roots + ((i < n && tid) ? tid[i] : 0);
     x[w] = 0;
     ko[w] = i < n ? koff[i] : 0;
     len[w] = i < n ? klen[i] : 0;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList 
   // epoch, (2) key comparison chunks of short nodes, (3) advance / resolve,
   // (4) dirty marks (their atomics are off the descent's critical path).
   for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
-    uint32_t ref[kLatchWays], ep[kLatchWays], nib[kLatchWays], sl[kLatchWays], sch[kLatchWays];
+    uint32_t ref[kLatchWays], ep[kLatchWays], nib[kLatchWays], sl[kLatchWays];
     uint64_t sko[kLatchWays];
 #pragma unroll
     for (int w = 0; w < kLatchWays; ++w) ref[w] = st[w] == 1 ? __ldcg(sp[w]) : 0u;
@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList 
       ep[w] = gen;
       nib[w] = 0;
       sl[w] = 0;
-      sch[w] = 0;
       sko[w] = 0;
       if (st[w] != 1) continue;
       if (kind == KIND_FULL) {

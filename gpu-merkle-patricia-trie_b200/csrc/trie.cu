@@ -53,20 +53,22 @@ T *wsp(DevBlock &b, size_t n, cudaError_t &e) {
 
 // ---------------------------------------------------------------------------
 
-Trie::Trie(int device, int geth_mode) : dev_(device), geth_(geth_mode ? 1 : 0) {
+Trie::Trie(int device, int geth_mode, int max_tries)
+    : dev_(device), geth_(geth_mode ? 1 : 0), n_tries_(max_tries > 1 ? (uint32_t)max_tries : 1u) {
   cudaError_t e = cudaSetDevice(dev_);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&root_, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&roots_, sizeof(uint32_t) * n_tries_ + 64);
   if (e == cudaSuccess) e = cudaMalloc(&ctr_, sizeof(Counters));
   if (e == cudaSuccess) e = cudaMallocHost(&h_ctr_, sizeof(Counters));
   if (e == cudaSuccess) e = cudaMallocHost(&h_small_, 256);
-  if (e == cudaSuccess) e = cudaMemset(root_, 0, 64);
+  if (e == cudaSuccess) e = cudaMemset(roots_, 0, sizeof(uint32_t) * n_tries_ + 64);
   if (e == cudaSuccess) e = cudaMemset(ctr_, 0, sizeof(Counters));
   if (e != cudaSuccess) {
     err_ = std::string("trie init: ") + cudaGetErrorString(e);
     return;
   }
-  tv_.root = root_;
+  tv_.roots = roots_;
+  tv_.n_tries = n_tries_;
   tv_.ctr = ctr_;
   tv_.geth_mode = geth_;
   ensure_capacity(1024, 1024, 1024, 1024, 4096, 4096);
@@ -79,7 +81,7 @@ Trie::~Trie() {
                   tv_.short_key, tv_.short_klen, tv_.short_child, tv_.short_epoch, tv_.short_depth,
                   tv_.short_dead, tv_.short_hash, tv_.short_hlen, tv_.short_claim, tv_.short_pseudo,
                   tv_.value_vid, tv_.rec_off, tv_.rec_len, tv_.rec_hp, (void *)tv_.keys, (void *)tv_.vals,
-                  root_, ctr_, dirty_ref_, dirty_depth_};
+                  roots_, ctr_, dirty_ref_, dirty_depth_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   DevBlock *blocks[] = {&ws_.koff, &ws_.klen, &ws_.ki, &ws_.vi, &ws_.hp, &ws_.kin, &ws_.order, &ws_.eqprev,
@@ -89,7 +91,8 @@ Trie::~Trie() {
                         &ws_.it_base, &ws_.it_len, &ws_.it_ref, &ws_.it_d0, &ws_.it_slot, &ws_.sb_base,
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
-                        &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.misc};
+                        &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
+                        &ws_.tid, &ws_.misc};
   for (DevBlock *b : blocks) b->release();
   for (int k = 0; k < 2; ++k) {
     ws_.s_start[k].release();
@@ -129,6 +132,8 @@ int Trie::sync_counters() {
     if (err & ERR_CAPACITY) return fail(E_CAPACITY, "node pool capacity exceeded");
     if (err & ERR_RETRY_LIMIT) return fail(E_RETRY_LIMIT, "insert retry limit exceeded");
     if (err & ERR_KEY_TOO_LONG) return fail(E_BAD_KEY, "key longer than the supported maximum");
+    if (err & ERR_BAD_TRIE) return fail(E_ARG, "trie id outside [0, max_tries)");
+    if (err & ERR_BARRIER) return fail(E_INTERNAL, "grid barrier wait gave up");
     if (err & ERR_BAD_KEY)
       return fail(E_BAD_KEY, "malformed key: nibble > 16, terminator not last, or a key that is a prefix of another");
     return fail(E_INTERNAL, "internal consistency check failed");
@@ -238,7 +243,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
 
 // Copy the batch into the arenas and build per-key records.
 int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
-                uint32_t *maxlen) {
+                uint32_t *maxlen, const int **tid_out) {
   const int n = b.n;
   cudaError_t e = cudaSuccess;
   int64_t kbytes = b.keys_bytes, vbytes = b.values_bytes;
@@ -261,18 +266,21 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   *koff = wsp<uint64_t>(ws_.koff, (size_t)n, e);
   *klen = wsp<uint32_t>(ws_.klen, (size_t)n, e);
   uint32_t *d_max = wsp<uint32_t>(ws_.misc, 16, e);
+  int *tid = b.trie_ids ? wsp<int>(ws_.tid, (size_t)n, e) : nullptr;
   if (e != cudaSuccess) return check_cuda(e, "stage alloc");
+  *tid_out = tid;
   e = cudaMemcpyAsync(karena + key_base, b.keys_hexs, (size_t)kbytes, kind, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(varena + val_base, b.values, (size_t)vbytes, kind, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ki, b.keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(vi, b.values_indexs, sizeof(int64_t) * 2 * (size_t)n, kind, st_);
   if (e == cudaSuccess && hp) e = cudaMemcpyAsync(hp, b.values_hps, sizeof(uint64_t) * (size_t)n, kind, st_);
+  if (e == cudaSuccess && tid) e = cudaMemcpyAsync(tid, b.trie_ids, sizeof(int) * (size_t)n, kind, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(karena + key_base + kbytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "stage copy");
   if ((e = cudaMemsetAsync(&ctr_->stream_terms, 0, 24, st_)) != cudaSuccess) return check_cuda(e, "stage reset");
   count_launch(), k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
-                                                *koff, *klen, d_max);
+                                                *koff, *klen, d_max, tid);
   if (kbytes > 0)
     count_launch(), k_stage_stream<<<std::min<unsigned>(blocks_for(kbytes / 8 + 1), 148 * 8), kThreads, 0, st_>>>(
         tv_, karena + key_base, kbytes);
@@ -299,8 +307,8 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
 
 // Lexicographic order of the batch (terminator before nibble 0) with the last
 // occurrence of every key kept: uord[0..m) are batch indices.
-int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, uint32_t **uord_out,
-                      int *m_out) {
+int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                      uint32_t **uord_out, int *m_out) {
   cudaError_t e = cudaSuccess;
   uint32_t *order = wsp<uint32_t>(ws_.order, (size_t)n, e);
   uint8_t *eqprev = wsp<uint8_t>(ws_.eqprev, (size_t)n + 1, e);
@@ -316,8 +324,9 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   count_launch(), k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
   int nchunks = (int)((maxlen + 7) / 8);
   stats_.sort_passes = 0;
-  for (int c = 0; c <= nchunks; ++c) {
-    int cc = (c == nchunks) ? -1 : c;  // final pass: key length
+  // forest batches: a first pass orders by trie id
+  for (int c = tid ? -1 : 0; c <= nchunks; ++c) {
+    int cc = (c == nchunks) ? -1 : (c < 0 ? -2 : c);  // final pass: key length
     count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
@@ -326,7 +335,7 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
     int K = (int)(h_small_[0] & 0xFFFFFFFFu);
     int S = (int)(h_small_[0] >> 32);
     if (K == 0) break;
-    if (opt_local_sort_) {
+    if (opt_local_sort_ && c >= 0) {
       // still-tied runs; if the largest fits one CTA, finish every run there
       uint32_t *rs = wsp<uint32_t>(ws_.it_id, (size_t)S, e);
       uint32_t *re = wsp<uint32_t>(ws_.it_len, (size_t)S, e);
@@ -349,7 +358,8 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
         break;
       }
     }
-    count_launch(), k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval);
+    count_launch(), k_sort_build<<<blocks_for(n), kThreads, 0, st_>>>(tv_, flags, pos, order, koff, klen, n, cc, act, skey, sval,
+                                                                       tid);
     int passes = 0;
     if ((e = sorter_.sort(skey, sval, K, st_, &passes)) != cudaSuccess) return check_cuda(e, "radix sort");
     stats_.sort_passes += passes;
@@ -467,14 +477,15 @@ int Trie::put_2phase(const BatchIn &b) {
   uint64_t *koff;
   uint32_t *klen;
   uint32_t maxlen = 0;
-  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen);
+  const int *tid = nullptr;
+  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen, &tid);
   if (rc) return rc;
   if ((rc = sync_counters())) return rc;  // key validation
   if (timing_) cudaEventRecord(ev[1], st_);
   const int n = b.n;
   uint32_t *uord;
   int m = 0;
-  if ((rc = sort_unique(n, koff, klen, maxlen, &uord, &m))) return rc;
+  if ((rc = sort_unique(n, koff, klen, maxlen, tid, &uord, &m))) return rc;
   stats_.last_unique = (uint64_t)m;
   if (timing_) cudaEventRecord(ev[2], st_);
   cudaError_t e = cudaSuccess;
@@ -491,7 +502,8 @@ int Trie::put_2phase(const BatchIn &b) {
     if (e != cudaSuccess) return check_cuda(e, "bulk alloc");
     if ((uint64_t)n_value_ + (uint64_t)m > cap_value_) return fail(E_CAPACITY, "value pool bound");
     count_launch(), k_items_bulk<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uord, m, koff, klen, vid_base, n_value_,
-                                                                      sb_base, sb_len, sb_ref, sb_d0, sb_slot, sb_code);
+                                                                      sb_base, sb_len, sb_ref, sb_d0, sb_slot, sb_code,
+                                                                      tid);
     count_launch(), k_items_lcp<<<blocks_for(m), kThreads, 0, st_>>>(tv_, sb_base, sb_len, sb_d0, sb_code, m, lcp);
     stats_.last_new = (uint64_t)m;
     stats_.last_pseudo = 0;
@@ -518,7 +530,7 @@ int Trie::put_2phase(const BatchIn &b) {
   if (e != cudaSuccess) return check_cuda(e, "walk alloc");
   DirtyList dl{dirty_ref_, dirty_depth_};
   count_launch(), k_walk<<<blocks_for((m + kWalkWays - 1) / kWalkWays), kThreads, 0, st_>>>(tv_, dl, uord, m, koff,
-                                                                                             klen, vid_base, wo);
+                                                                                             klen, vid_base, wo, tid);
   count_launch(), k_pseudo_ranks<<<blocks_for(m), kThreads, 0, st_>>>(tv_, wo, m);
   count_launch(), k_new_flags<<<blocks_for(m), kThreads, 0, st_>>>(wo.status, m, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, m, d_tot, scan_ws_, st_);
@@ -607,11 +619,6 @@ int Trie::bucket_and_hash() {
       cudaSuccess)
     return check_cuda(e, "hash cursor");
   count_launch(), k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, (int)nd, cursor, sorted);
-  uint32_t root_ref = 0;
-  if ((e = cudaMemcpyAsync(h_small_, root_, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
-    return check_cuda(e, "root ref");
-  root_ref = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;
   if ((e = cudaMemsetAsync(&ctr_->hashed, 0, 4, st_)) != cudaSuccess ||
@@ -627,8 +634,7 @@ int Trie::bucket_and_hash() {
     uint32_t a = off[2 * d], z = off[2 * d + 2];
     if (z == a) continue;
     ++levels;
-    count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a),
-                                                                               root_ref);
+    count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a));
   }
   if (timing_) {
     cudaEventRecord(kz, st_);
@@ -671,13 +677,16 @@ int Trie::hash() {
   return OK;
 }
 
-int Trie::root(uint8_t out[32], int *len) {
+int Trie::root(uint8_t out[32], int *len, int trie) {
   err_.clear();
+  if (trie < 0 || (uint32_t)trie >= n_tries_) return fail(E_ARG, "trie id outside [0, max_tries)");
   cudaSetDevice(dev_);
   cudaError_t e = cudaSuccess;
   uint8_t *d = wsp<uint8_t>(ws_.misc, 256, e) + 128;
+  int *did = reinterpret_cast<int *>(d + 64);
   if (e != cudaSuccess) return check_cuda(e, "root alloc");
-  count_launch(), k_root<<<1, 32, 0, st_>>>(tv_, d);
+  if ((e = cudaMemcpyAsync(did, &trie, 4, cudaMemcpyHostToDevice, st_)) != cudaSuccess) return check_cuda(e, "root id");
+  count_launch(), k_roots<<<1, 32, 0, st_>>>(tv_, did, 1, d);
   uint8_t h[40];
   if ((e = cudaMemcpyAsync(h_small_, d, 33, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
@@ -688,8 +697,33 @@ int Trie::root(uint8_t out[32], int *len) {
   return OK;
 }
 
+int Trie::roots(const int *ids, int n, uint8_t *out32, int *sizes) {
+  err_.clear();
+  if (n <= 0) return OK;
+  if (ids)
+    for (int i = 0; i < n; ++i)
+      if (ids[i] < 0 || (uint32_t)ids[i] >= n_tries_) return fail(E_ARG, "trie id outside [0, max_tries)");
+  if (!ids && (uint32_t)n > n_tries_) return fail(E_ARG, "more roots than tries");
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  int *did = ids ? wsp<int>(ws_.g_tid, (size_t)n, e) : nullptr;
+  uint8_t *d = wsp<uint8_t>(ws_.g_keys, 33 * (size_t)n, e);
+  if (e == cudaSuccess && ids) e = cudaMemcpyAsync(did, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st_);
+  if (e != cudaSuccess) return check_cuda(e, "roots alloc");
+  count_launch(), k_roots<<<blocks_for(32 * (int64_t)n), kThreads, 0, st_>>>(tv_, did, n, d);
+  std::vector<uint8_t> h(33 * (size_t)n);
+  if ((e = cudaMemcpyAsync(h.data(), d, h.size(), cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "roots");
+  for (int i = 0; i < n; ++i) {
+    std::memcpy(out32 + 32 * (size_t)i, h.data() + 33 * (size_t)i, 32);
+    sizes[i] = h[33 * (size_t)i + 32];
+  }
+  return OK;
+}
+
 int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs, uint64_t *out_hp,
-               int *out_len, int64_t keys_bytes) {
+               int *out_len, int64_t keys_bytes, const int *trie_ids) {
   err_.clear();
   if (n <= 0) return OK;
   cudaSetDevice(dev_);
@@ -703,11 +737,13 @@ int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool dev
   int *di = wsp<int>(ws_.g_idx, 2 * (size_t)n, e);
   uint64_t *dhp = wsp<uint64_t>(ws_.g_hp, (size_t)n, e);
   int *dlen = wsp<int>(ws_.g_len, (size_t)n, e);
+  int *dtid = trie_ids ? wsp<int>(ws_.g_tid, (size_t)n, e) : nullptr;
   if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, kind, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  if (e == cudaSuccess && dtid) e = cudaMemcpyAsync(dtid, trie_ids, sizeof(int) * (size_t)n, kind, st_);
   if (e != cudaSuccess) return check_cuda(e, "gets copy");
-  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr);
+  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr, dtid);
   e = cudaMemcpyAsync(out_hp, dhp, sizeof(uint64_t) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(out_len, dlen, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
@@ -732,7 +768,7 @@ int Trie::get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, st
   if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice, st_);
   if (e != cudaSuccess) return check_cuda(e, "get_values copy");
-  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, dvid);
+  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, dvid, nullptr);
   std::vector<int64_t> vid(n);
   std::vector<int> len(n);
   e = cudaMemcpyAsync(vid.data(), dvid, 8 * (size_t)n, cudaMemcpyDeviceToHost, st_);
@@ -770,7 +806,7 @@ const uint32_t *Trie::pending_dirty(int *n) const {
 int Trie::reset() {
   err_.clear();
   cudaSetDevice(dev_);
-  cudaError_t e = cudaMemsetAsync(root_, 0, 4, st_);
+  cudaError_t e = cudaMemsetAsync(roots_, 0, sizeof(uint32_t) * n_tries_, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctr_, 0, sizeof(Counters), st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "reset");
@@ -805,13 +841,14 @@ int Trie::put_latching(const BatchIn &b) {
   uint64_t *koff;
   uint32_t *klen;
   uint32_t maxlen = 0;
-  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen);
+  const int *tid = nullptr;
+  int rc = stage(b, key_base, vid_base, &koff, &klen, &maxlen, &tid);
   if (rc) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
   count_launch(), k_latch_insert<<<blocks_for((b.n + kLatchWays - 1) / kLatchWays), kThreads, 0, st_>>>(
-      tv_, dl, koff, klen, b.n, vid_base, 1u << 20);
+      tv_, dl, koff, klen, b.n, vid_base, 1u << 20, tid);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) {

@@ -30,6 +30,7 @@ struct BatchIn {
   const uint8_t *values = nullptr;
   const int64_t *values_indexs = nullptr;  // [2n] inclusive
   const uint64_t *values_hps = nullptr;  // [n] caller host pointers, may be null
+  const int *trie_ids = nullptr;         // [n] trie of each key (forest), null = trie 0
   int n = 0;
   int64_t keys_bytes = -1;    // total key stream bytes (derived if < 0, host only)
   int64_t values_bytes = -1;  // total value stream bytes
@@ -60,7 +61,9 @@ enum Status : int {
 
 class Trie {
  public:
-  Trie(int device, int geth_mode);
+  // max_tries > 1 makes a forest: independent tries sharing the node pools
+  // and arenas, addressed by trie id 0..max_tries-1
+  Trie(int device, int geth_mode, int max_tries = 1);
   ~Trie();
   Trie(const Trie &) = delete;
   Trie &operator=(const Trie &) = delete;
@@ -68,10 +71,13 @@ class Trie {
   int put_2phase(const BatchIn &b);
   int put_latching(const BatchIn &b);
   int hash();
-  int root(uint8_t out[32], int *len);
+  int root(uint8_t out[32], int *len, int trie = 0);
+  // roots of tries ids[0..n) (host array; null = tries 0..n-1): out32[32 i..]
+  // zero-padded, sizes[i] = length (0 = empty trie)
+  int roots(const int *ids, int n, uint8_t *out32, int *sizes);
   // out_hp[i] = host pointer given with the value (0 when absent), out_len[i] its size
   int gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs,
-           uint64_t *out_hp, int *out_len, int64_t keys_bytes = -1);
+           uint64_t *out_hp, int *out_len, int64_t keys_bytes = -1, const int *trie_ids = nullptr);
   // value bytes of the stored value for each key (test/export helper)
   int get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &vals,
                  std::vector<int64_t> &offs);
@@ -84,6 +90,7 @@ class Trie {
   const std::string &error() const { return err_; }
   cudaStream_t stream() const { return st_; }
   int device() const { return dev_; }
+  int max_tries() const { return (int)n_tries_; }
   void set_timing(bool on) { timing_ = on; }
   // tuning knobs (names: "local_build", "local_sort")
   int set_option(const std::string &name, int64_t value);
@@ -105,7 +112,8 @@ class Trie {
   uint64_t cap_keys_ = 0, cap_vals_ = 0;
   uint32_t n_full_ = 0, n_short_ = 0, n_value_ = 0;
   uint64_t n_rec_ = 0, key_used_ = 0, val_used_ = 0;
-  uint32_t *root_ = nullptr;
+  uint32_t *roots_ = nullptr;  // [n_tries_] root words
+  uint32_t n_tries_ = 1;
   Counters *ctr_ = nullptr;
   Counters *h_ctr_ = nullptr;  // pinned mirror
   uint32_t epoch_ = 0;         // per put batch (split claims)
@@ -128,7 +136,8 @@ class Trie {
     DevBlock act2, aseg, aseg2, kflags, knib;                   // builder levels
     DevBlock s_start[2], s_end[2], s_depth[2], s_slot[2], s_D[2], s_branch[2];
     DevBlock bins, cursor, sorted_dirty;                        // hash buckets
-    DevBlock g_keys, g_idx, g_hp, g_len;                        // gets
+    DevBlock g_keys, g_idx, g_hp, g_len, g_tid;                 // gets
+    DevBlock tid;                                               // trie ids of the batch
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;
@@ -141,9 +150,9 @@ class Trie {
   int ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
                       uint64_t add_key_bytes, uint64_t add_val_bytes);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
-            uint32_t *maxlen);
-  int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, uint32_t **uord,
-                  int *m);
+            uint32_t *maxlen, const int **tid);
+  int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                  uint32_t **uord, int *m);
   int build_levels(int T);
   int bucket_and_hash();
   uint64_t read_u64(const void *dptr);

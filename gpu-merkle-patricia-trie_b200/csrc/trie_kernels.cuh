@@ -55,8 +55,8 @@ __device__ __forceinline__ void mark_short(const TrieView &tv, DirtyList d, uint
 }
 
 __device__ __forceinline__ void write_slot(const TrieView &tv, uint64_t slot, uint32_t ref) {
-  if (slot == kSlotRoot)
-    *tv.root = ref;
+  if (is_root_slot(slot))
+    tv.roots[slot_trie(slot)] = ref;
   else
     tv.full_child[(slot >> 5) * 17 + (slot & 31)] = ref;
 }
@@ -101,9 +101,10 @@ __device__ __forceinline__ uint32_t new_short(const TrieView &tv, DirtyList d, u
 
 __global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uint64_t *hp, int n,
                         uint64_t key_base, uint64_t val_base, uint64_t vid_base, int64_t kbytes,
-                        int64_t vbytes, uint64_t *koff, uint32_t *klen, uint32_t *maxlen) {
+                        int64_t vbytes, uint64_t *koff, uint32_t *klen, uint32_t *maxlen, const int *tid) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (tid && (uint32_t)tid[i] >= tv.n_tries) set_error(tv.ctr, ERR_BAD_TRIE);
   int ks = ki[2 * i], ke = ki[2 * i + 1];
   bool bad = ks < 0 || ke < ks || (int64_t)ke >= kbytes;  // index pair outside the key stream
   if (bad) ks = ke = 0;
@@ -212,9 +213,10 @@ __global__ void k_sort_flags(const uint8_t *eqprev, int n, unsigned long long *f
   flags[p] = (unsigned long long)active | ((unsigned long long)start << 32);
 }
 
+// c >= 0: key chunk c; c == -1: key length; c == -2: trie id (forest batches)
 __global__ void k_sort_build(TrieView tv, const unsigned long long *flags, const unsigned long long *pos,
                              const uint32_t *order, const uint64_t *koff, const uint32_t *klen, int n, int c,
-                             uint32_t *act, uint64_t *skey, uint32_t *sval) {
+                             uint32_t *act, uint64_t *skey, uint32_t *sval, const int *tid) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   unsigned long long f = flags[p];
@@ -223,7 +225,7 @@ __global__ void k_sort_build(TrieView tv, const unsigned long long *flags, const
   uint32_t k = (uint32_t)q;
   uint32_t seg = (uint32_t)(q >> 32) + (uint32_t)(f >> 32) - 1u;
   uint32_t it = order[p];
-  uint32_t ch = c >= 0 ? key_chunk(tv.keys, koff[it], klen[it], c) : klen[it];
+  uint32_t ch = c >= 0 ? key_chunk(tv.keys, koff[it], klen[it], c) : (c == -1 ? klen[it] : (uint32_t)tid[it]);
   act[k] = (uint32_t)p;
   skey[k] = ((uint64_t)seg << 32) | ch;
   sval[k] = it;
@@ -270,6 +272,11 @@ __device__ __forceinline__ uint64_t code_full(uint32_t f, uint32_t c) {
   return (1ull << 35) | ((uint64_t)f << 5) | c;
 }
 __device__ __forceinline__ uint64_t code_short(uint32_t s) { return (2ull << 35) | ((uint64_t)s << 5) | 31u; }
+// the root word of trie t (kind 0)
+__device__ __forceinline__ uint64_t code_root(uint32_t t) { return (uint64_t)t << 5; }
+__device__ __forceinline__ uint64_t code_slot(uint64_t slot) {
+  return is_root_slot(slot) ? code_root(slot_trie(slot)) : code_full((uint32_t)(slot >> 5), (uint32_t)(slot & 31));
+}
 
 // nibble order used by the sort: terminator (16) sorts before 0
 __device__ __forceinline__ int sym_rank(uint8_t b) { return b == 16 ? -1 : (int)b; }
@@ -295,11 +302,10 @@ constexpr int kWalkWays = 4;
 
 __global__ void __launch_bounds__(256, 2) k_walk(TrieView tv, DirtyList dl, const uint32_t *uord, int m,
                                                  const uint64_t *koff, const uint32_t *klen, uint64_t vid_base,
-                                                 WalkOut wo) {
+                                                 WalkOut wo, const int *tid) {
   const int nthreads = gridDim.x * blockDim.x;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gen = tv.gen;
-  const uint32_t root = *tv.root;
   uint32_t ref[kWalkWays], x[kWalkWays], len[kWalkWays], item[kWalkWays];
   uint64_t slot[kWalkWays];
   bool act[kWalkWays];
@@ -309,9 +315,10 @@ __global__ void __launch_bounds__(256, 2) k_walk(TrieView tv, DirtyList dl, cons
     act[w] = j < m;
     item[w] = act[w] ? uord[j] : 0;
     len[w] = act[w] ? klen[item[w]] : 0;
-    ref[w] = root;
+    const uint32_t tr = (act[w] && tid) ? (uint32_t)tid[item[w]] : 0u;
+    ref[w] = act[w] ? tv.roots[tr] : 0u;
     x[w] = 0;
-    slot[w] = kSlotRoot;
+    slot[w] = root_slot(tr);
   }
   for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
     bool any = false;
@@ -323,8 +330,7 @@ __global__ void __launch_bounds__(256, 2) k_walk(TrieView tv, DirtyList dl, cons
       const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
       if (kind == KIND_NULL) {
         wo.status[j] = W_NEW;
-        wo.code[j] = (slot[w] == kSlotRoot) ? 0ull
-                                            : code_full((uint32_t)(slot[w] >> 5), (uint32_t)(slot[w] & 31));
+        wo.code[j] = code_slot(slot[w]);
         wo.d0[j] = x[w];
         wo.slot[j] = slot[w];
         act[w] = false;
@@ -475,7 +481,8 @@ __global__ void k_items_pseudo(TrieView tv, const WalkOut wo, int n_pseudo, int 
 // in sorted order (no walk, no grouping sort).  Value node j = vbase + j.
 __global__ void k_items_bulk(TrieView tv, const uint32_t *uord, int m, const uint64_t *koff, const uint32_t *klen,
                              uint64_t vid_base, uint32_t vbase, uint64_t *sb_base, uint32_t *sb_len,
-                             uint32_t *sb_ref, uint32_t *sb_d0, uint64_t *sb_slot, uint64_t *sb_code) {
+                             uint32_t *sb_ref, uint32_t *sb_d0, uint64_t *sb_slot, uint64_t *sb_code,
+                             const int *tid) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= m) return;
   if (j == 0) atomicAdd(&tv.ctr->n_value, (uint32_t)m);
@@ -486,8 +493,9 @@ __global__ void k_items_bulk(TrieView tv, const uint32_t *uord, int m, const uin
   sb_len[j] = klen[item];
   sb_ref[j] = make_ref(KIND_VALUE, v);
   sb_d0[j] = 0;
-  sb_slot[j] = kSlotRoot;
-  sb_code[j] = 0;
+  const uint32_t tr = tid ? (uint32_t)tid[item] : 0u;
+  sb_slot[j] = root_slot(tr);
+  sb_code[j] = code_root(tr);
 }
 
 // gather items into sorted order, group starts, and adjacent LCPs
@@ -875,8 +883,7 @@ __device__ __forceinline__ void prefetch_child(const TrieView &tv, uint32_t r) {
 
 // 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
 // lanes in registers without spilling at this bound.
-__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count,
-                                                        uint32_t root_ref) {
+__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
@@ -884,7 +891,9 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
   uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
   bool full = kind == KIND_FULL;
   if (!full && tv.short_dead[idx]) return;
-  bool force = tv.geth_mode && ref == root_ref;
+  // depth 0 holds exactly the roots of the forest's tries; go-ethereum
+  // hashes a root whatever its size
+  bool force = tv.geth_mode && (full ? tv.full_depth[idx] : tv.short_depth[idx]) == 0;
   int nitems = full ? 18 : 3;
   // pass 1: payload size (all child loads issued together, sources prefetched)
   uint64_t payload = 0;
@@ -1023,8 +1032,8 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
 // ---------------------------------------------------------------------------
 // gets (gpu_mpt_kernels.cuh:2267-2340)
 
-__device__ __forceinline__ int64_t lookup(const TrieView &tv, const uint8_t *kb, uint32_t len) {
-  uint32_t ref = *tv.root;
+__device__ __forceinline__ int64_t lookup(const TrieView &tv, uint32_t root, const uint8_t *kb, uint32_t len) {
+  uint32_t ref = root;
   uint32_t x = 0;
   for (uint32_t guard = 0; guard <= len + 1; ++guard) {
     uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
@@ -1048,13 +1057,14 @@ __device__ __forceinline__ int64_t lookup(const TrieView &tv, const uint8_t *kb,
 }
 
 __global__ void k_gets(TrieView tv, const uint8_t *keys, const int *idx, int n, int64_t keys_bytes,
-                       uint64_t *out_hp, int *out_len, int64_t *out_vid) {
+                       uint64_t *out_hp, int *out_len, int64_t *out_vid, const int *tid) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int ks = idx[2 * i], ke = idx[2 * i + 1];
   int len = ke - ks + 1;
-  bool ok = ks >= 0 && len > 0 && (int64_t)ke < keys_bytes;
-  int64_t vid = ok ? lookup(tv, keys + ks, (uint32_t)len) : -1;
+  const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
+  bool ok = ks >= 0 && len > 0 && (int64_t)ke < keys_bytes && tr < tv.n_tries;
+  int64_t vid = ok ? lookup(tv, tv.roots[tr], keys + ks, (uint32_t)len) : -1;
   if (out_vid) out_vid[i] = vid;
   if (vid < 0) {
     out_hp[i] = 0;
@@ -1065,9 +1075,15 @@ __global__ void k_gets(TrieView tv, const uint8_t *keys, const int *idx, int n, 
   }
 }
 
-__global__ void k_root(TrieView tv, uint8_t *out) {
-  int t = threadIdx.x;
-  uint32_t r = *tv.root;
+// Root bytes of trie ids[i] (or trie i when ids is null) into out[33 i ..]:
+// 32 bytes (zero-padded) and the length (0 = empty trie).  Warp per trie.
+__global__ void k_roots(TrieView tv, const int *ids, int n, uint8_t *out) {
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (i >= n) return;
+  const int t = threadIdx.x & 31;
+  const uint32_t tr = ids ? (uint32_t)ids[i] : (uint32_t)i;
+  out += 33 * (size_t)i;
+  uint32_t r = tr < tv.n_tries ? tv.roots[tr] : 0u;
   uint32_t kind = ref_kind(r), idx = ref_idx(r);
   uint32_t len = 0;
   const uint8_t *h = nullptr;
@@ -1082,7 +1098,7 @@ __global__ void k_root(TrieView tv, uint8_t *out) {
     h = tv.vals + tv.rec_off[vid];
     len = min(32u, tv.rec_len[vid]);
   }
-  if (t < 32) out[t] = (h && (uint32_t)t < len) ? h[t] : 0;
+  out[t] = (h && (uint32_t)t < len) ? h[t] : 0;
   if (t == 0) out[32] = (uint8_t)len;
 }
 

@@ -33,6 +33,8 @@ EXPORTS = [
     "gmpt_last_error", "gmpt_last_error_message", "gmpt_free_buffer", "gmpt_stream",
     "gmpt_keccak256_batch", "gmpt_keccak256_batch_device", "gmpt_keccak_peak", "gmpt_launch_count",
     "gmpt_keccak256_batch_noalloc", "gmpt_set_option",
+    "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
+    "gmpt_get_roots", "gmpt_gets_forest",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -84,6 +86,14 @@ def lib():
     L.gmpt_version.restype = i32
     L.gmpt_create.restype = vp
     L.gmpt_create.argtypes = [i32, i32]
+    L.gmpt_create_forest.restype = vp
+    L.gmpt_create_forest.argtypes = [i32, i32, i32]
+    L.gmpt_max_tries.argtypes = [vp]
+    for f in ("gmpt_puts_2phase_forest", "gmpt_puts_latching_forest"):
+        getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, vp, i32]
+        getattr(L, f).restype = i32
+    L.gmpt_get_roots.argtypes = [vp, vp, i32, vp, vp]
+    L.gmpt_gets_forest.argtypes = [vp, vp, vp, vp, i32, vp, vp]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -167,11 +177,15 @@ def launch_count() -> int:
 
 
 class MPT:
-    """A device-resident trie (GpuMPT::Compress::MPT)."""
+    """A device-resident trie (GpuMPT::Compress::MPT).
 
-    def __init__(self, device: int = 0, mode: int = MODE_REF):
+    ``max_tries > 1`` makes a forest of independent tries sharing the node
+    pools; the ``*_forest`` methods take a trie id per key and every other
+    method addresses trie 0."""
+
+    def __init__(self, device: int = 0, mode: int = MODE_REF, max_tries: int = 1):
         self._L = lib()
-        self._h = self._L.gmpt_create(device, mode)
+        self._h = self._L.gmpt_create_forest(device, mode, int(max_tries))
         if not self._h:
             raise GmptError(self._L.gmpt_last_error(), self._L.gmpt_last_error_message().decode())
 
@@ -196,6 +210,32 @@ class MPT:
         kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
         hp = None if values_hps is None else np.ascontiguousarray(values_hps, dtype=np.uint64)
         _check(self._L.gmpt_puts_latching(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), len(ki) // 2))
+
+    def puts_forest(self, two_phase: bool, keys_hexs, keys_indexs, values, values_indexs, trie_ids,
+                    values_hps=None):
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        hp = None if values_hps is None else np.ascontiguousarray(values_hps, dtype=np.uint64)
+        tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
+        f = self._L.gmpt_puts_2phase_forest if two_phase else self._L.gmpt_puts_latching_forest
+        _check(f(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), _p(tid), len(ki) // 2))
+
+    def get_roots(self, trie_ids=None, n: int | None = None) -> list:
+        """Root bytes of each trie in trie_ids (default: tries 0..n-1)."""
+        ids = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        cnt = len(ids) if ids is not None else int(n)
+        out = np.zeros(32 * max(cnt, 1), dtype=np.uint8)
+        sizes = np.zeros(max(cnt, 1), dtype=np.int32)
+        _check(self._L.gmpt_get_roots(self._h, _p(ids), cnt, _p(out), _p(sizes)))
+        return [out[32 * i: 32 * i + sizes[i]].tobytes() for i in range(cnt)]
+
+    def gets_forest(self, keys_hexs, keys_indexs, trie_ids):
+        kh, ki, _, _ = _arrays(keys_hexs, keys_indexs)
+        n = len(ki) // 2
+        tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
+        hps = np.zeros(n, dtype=np.uint64)
+        sizes = np.zeros(n, dtype=np.int32)
+        _check(self._L.gmpt_gets_forest(self._h, _p(kh), _p(ki), _p(tid), n, _p(hps), _p(sizes)))
+        return hps, sizes
 
     def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
                     values_bytes: int, d_hps: int = 0):

@@ -59,6 +59,15 @@ int gmpt_version(void);
 /* MPT::MPT() (gpu_mpt.cuh:162-173): an empty trie on `device`. */
 gmpt_trie *gmpt_create(int device, int encode_mode);
 void gmpt_destroy(gmpt_trie *t);
+
+/* A forest: max_tries independent tries (ids 0 .. max_tries-1) that share
+ * one set of node pools and arenas, so a batch touching many tries (a block's
+ * state trie and its accounts' storage tries) is one insert and one PhaseHC
+ * pass.  No counterpart in the reference, which holds one trie per MPT
+ * object (gpu_mpt.cuh:162-173); trie 0 of a forest is what every
+ * single-trie call below addresses. */
+gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries);
+int gmpt_max_tries(gmpt_trie *t);
 /* drop every node (capacity is kept) */
 int gmpt_reset(gmpt_trie *t);
 
@@ -87,6 +96,16 @@ int gmpt_puts_latching_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const in
                               const uint64_t *d_values_hps, int n, int64_t keys_bytes,
                               int64_t values_bytes);
 
+/* Forest inserts from HOST arrays: key i goes into trie trie_ids[i].  Same
+ * semantics per trie as the single-trie calls above; the tries' roots come
+ * from gmpt_get_roots after gmpt_hash_onepass. */
+int gmpt_puts_2phase_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                            const uint8_t *values_bytes, const int64_t *values_indexs,
+                            const uint8_t *const *values_hps, const int *trie_ids, int n);
+int gmpt_puts_latching_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                              const uint8_t *values_bytes, const int64_t *values_indexs,
+                              const uint8_t *const *values_hps, const int *trie_ids, int n);
+
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
 int gmpt_hash_onepass(gmpt_trie *t);
@@ -99,11 +118,19 @@ int gmpt_pending_targets(gmpt_trie *t, const uint32_t **d_targets, int *n);
  * trie, < 32 for a raw root in GMPT_MODE_REF, else 32. */
 int gmpt_get_root_hash(gmpt_trie *t, uint8_t out[32], int *size);
 
+/* Roots of tries trie_ids[0..n) (NULL: tries 0..n-1), as get_root_hash:
+ * out32[32 i ..] zero-padded, sizes[i] = 0 / < 32 / 32. */
+int gmpt_get_roots(gmpt_trie *t, const int *trie_ids, int n, uint8_t *out32, int *sizes);
+
 /* gets_parallel (gpu_mpt.cuh:139-140, 984-1036): values_hps[i] receives the
  * host pointer given with the stored value (NULL when the key is absent or
  * none was given) and values_sizes[i] its length (0 when absent). */
 int gmpt_gets_parallel(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int n,
                        const uint8_t **values_hps, int *values_sizes);
+
+/* gets_parallel on a forest: key i is looked up in trie trie_ids[i]. */
+int gmpt_gets_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const int *trie_ids, int n,
+                     const uint8_t **values_hps, int *values_sizes);
 
 /* Value bytes stored for each key, concatenated into out (capacity out_cap);
  * out_indexs[2i], out_indexs[2i+1] = inclusive range, or -1, -1 if absent.
