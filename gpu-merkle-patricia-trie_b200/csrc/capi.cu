@@ -147,6 +147,80 @@ int gmpt_gets_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_ind
                      t->t);
 }
 
+static int block_call(gmpt_trie *t, bool device, const uint8_t *keys_hexs, const int *keys_indexs,
+                      const uint8_t *values, const int64_t *values_indexs, const int *trie_ids,
+                      const int *patch_trie, const int *patch_off, int n, int n0, int64_t keys_bytes,
+                      int64_t values_bytes, const int *out_ids, int n_out, uint8_t *out32, int *out_sizes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  gmpt::BlockIn b;
+  b.keys_hexs = keys_hexs;
+  b.keys_indexs = keys_indexs;
+  b.values = values;
+  b.values_indexs = values_indexs;
+  b.trie_ids = trie_ids;
+  b.patch_trie = patch_trie;
+  b.patch_off = patch_off;
+  b.n = n;
+  b.n0 = n0;
+  b.keys_bytes = keys_bytes;
+  b.values_bytes = values_bytes;
+  b.out_ids = out_ids;
+  b.n_out = n_out;
+  b.device = device;
+  return record_trie(t->t->block_update(b, out32, out_sizes), t->t);
+}
+
+int gmpt_block_update(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const uint8_t *values_bytes,
+                      const int64_t *values_indexs, const int *trie_ids, const int *patch_trie, const int *patch_off,
+                      int n, int n0, const int *out_ids, int n_out, uint8_t *out32, int *out_sizes) {
+  return block_call(t, false, keys_hexs, keys_indexs, values_bytes, values_indexs, trie_ids, patch_trie, patch_off, n,
+                    n0, -1, -1, out_ids, n_out, out32, out_sizes);
+}
+
+int gmpt_block_update_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                             const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids,
+                             const int *d_patch_trie, const int *d_patch_off, int n, int n0, int64_t keys_bytes,
+                             int64_t values_bytes, const int *out_ids, int n_out, uint8_t *out32, int *out_sizes) {
+  return block_call(t, true, d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs, d_trie_ids, d_patch_trie,
+                    d_patch_off, n, n0, keys_bytes, values_bytes, out_ids, n_out, out32, out_sizes);
+}
+
+int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_bytes) {
+  if (!t || n_keys < 0 || key_bytes < 0 || value_bytes < 0) return record(GMPT_E_ARG, "bad argument");
+  return record_trie(t->t->reserve((uint64_t)n_keys, (uint64_t)key_bytes, (uint64_t)value_bytes), t->t);
+}
+
+int gmpt_block_times(gmpt_trie *t, float out[3]) {
+  if (!t || !out) return record(GMPT_E_ARG, "null argument");
+  const gmpt::Trie::BlockInfo &bi = t->t->block_info();
+  out[0] = bi.t_inputs_ms;
+  out[1] = bi.t_launch_ms;
+  out[2] = bi.t_total_ms;
+  return record(0, "");
+}
+
+int gmpt_block_timeline(gmpt_trie *t, uint64_t *out_ns, int cap, int *n) {
+  if (!t || !n || (cap > 0 && !out_ns)) return record(GMPT_E_ARG, "null argument");
+  const gmpt::Trie::BlockInfo &bi = t->t->block_info();
+  *n = (int)bi.n_ts;
+  for (int i = 0; i < (int)bi.n_ts && i < cap; ++i) out_ns[i] = bi.ts[i];
+  return record(0, "");
+}
+
+int gmpt_block_info(gmpt_trie *t, uint32_t out[8]) {
+  if (!t || !out) return record(GMPT_E_ARG, "null argument");
+  const gmpt::Trie::BlockInfo &bi = t->t->block_info();
+  out[0] = bi.levels[0];
+  out[1] = bi.levels[1];
+  out[2] = bi.dirty[0];
+  out[3] = bi.dirty[1];
+  out[4] = (uint32_t)bi.grid;
+  out[5] = bi.captures;
+  out[6] = bi.launches;
+  out[7] = 0;
+  return record(0, "");
+}
+
 static gmpt::BatchIn device_batch(const uint8_t *k, const int *ki, const uint8_t *v, const int64_t *vi,
                                   const uint64_t *hps, int n, int64_t kb, int64_t vb) {
   gmpt::BatchIn b;

@@ -127,7 +127,8 @@ __device__ __forceinline__ uint64_t load_u64_unaligned(const uint8_t *p) {
   return (lo >> sh) | (hi << (64 - sh));
 }
 
-// Same, through the coherent path (data written earlier in this kernel).
+// Same with ordinary loads (data written earlier in this kernel, before a
+// grid barrier; never the non-coherent read-only path).
 __device__ __forceinline__ uint64_t load_u64_unaligned_cg(const uint8_t *p) {
   uintptr_t a = reinterpret_cast<uintptr_t>(p);
   const uint64_t *q = reinterpret_cast<const uint64_t *>(a & ~uintptr_t(7));

@@ -181,12 +181,12 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
 // handed to latch_from at the slot where its descent stopped.
 constexpr int kLatchWays = 4;
 
-__global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
-                                                      const uint32_t *klen, int n, uint64_t vid_base,
-                                                      uint32_t retry_limit, const int *tid) {
+// Keys t + w * nthreads (w < kLatchWays) of koff/klen[0..n), record ids
+// vid_base + i, trie ids tid[i] (null: trie 0).
+__device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, const uint64_t *koff,
+                                           const uint32_t *klen, int n, uint64_t vid_base, uint32_t retry_limit,
+                                           const int *tid, int t, int nthreads) {
   const uint32_t gen = tv.gen;
-  const int nthreads = gridDim.x * blockDim.x;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t *sp[kLatchWays];
   uint32_t x[kLatchWays], len[kLatchWays];
   uint64_t ko[kLatchWays];
@@ -305,6 +305,13 @@ __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList 
     if (st[w] != 0)
       latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)(t + w * nthreads),
                  retry_limit);
+}
+
+__global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
+                                                      const uint32_t *klen, int n, uint64_t vid_base,
+                                                      uint32_t retry_limit, const int *tid) {
+  latch_keys(tv, dl, koff, klen, n, vid_base, retry_limit, tid, blockIdx.x * blockDim.x + threadIdx.x,
+             gridDim.x * blockDim.x);
 }
 
 }  // namespace gmpt

@@ -15,6 +15,7 @@
 #include "keccak_batch.cuh"
 #include "local_build.cuh"
 #include "local_sort.cuh"
+#include "block_update.cuh"
 
 namespace gmpt {
 
@@ -104,6 +105,13 @@ Trie::~Trie() {
   }
   sorter_.release();
   scan_ws_.release();
+  DevBlock *bblocks[] = {&blk_.keys, &blk_.kidx, &blk_.vals, &blk_.vidx, &blk_.tid, &blk_.ptrie, &blk_.poff,
+                         &blk_.out_ids, &blk_.out, &blk_.koff, &blk_.klen, &blk_.bins, &blk_.sorted};
+  for (DevBlock *b : bblocks) b->release();
+  if (blk_.exec) cudaGraphExecDestroy(blk_.exec);
+  if (blk_.graph) cudaGraphDestroy(blk_.graph);
+  if (blk_.d_desc) cudaFree(blk_.d_desc);
+  if (blk_.h_desc) cudaFreeHost(blk_.h_desc);
   if (h_ctr_) cudaFreeHost(h_ctr_);
   if (h_small_) cudaFreeHost(h_small_);
   if (st_) cudaStreamDestroy(st_);
@@ -123,6 +131,11 @@ int Trie::sync_counters() {
   cudaError_t e = cudaMemcpyAsync(h_ctr_, ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "sync counters");
+  return apply_counters();
+}
+
+// Node counts and the error word from the pinned copy in h_ctr_.
+int Trie::apply_counters() {
   n_full_ = h_ctr_->n_full;
   n_short_ = h_ctr_->n_short;
   n_value_ = h_ctr_->n_value;
@@ -1090,7 +1103,266 @@ int Trie::set_option(const std::string &name, int64_t value) {
     opt_local_sort_ = value != 0;
     return OK;
   }
+  if (name == "block_grid") {
+    if (value < 0 || value > 1 << 20) return fail(E_ARG, "block_grid must be in [0, 2^20]");
+    opt_block_grid_ = (int)value;
+    return OK;
+  }
+  if (name == "block_graph") {
+    opt_block_graph_ = value != 0;
+    return OK;
+  }
   return fail(E_ARG, "unknown option: " + name);
+}
+
+}  // namespace gmpt
+
+// ---------------------------------------------------------------------------
+// Persistent forest block updates.
+
+namespace gmpt {
+
+namespace {
+
+constexpr int kBlockThreads = 256;
+constexpr size_t kBlockSmem = sizeof(uint64_t) * 17 * kBlockThreads + (kBlockThreads / 32) * kWarpMsgBytes;
+
+// everything a captured graph has baked in
+struct BlockSig {
+  TrieView tv;
+  DirtyList dl;
+  BlockBufs bb;
+  void *h_desc;
+  void *h_ctr;
+  int grid, stage_grid;
+};
+
+}  // namespace
+
+int Trie::block_launch() {
+  cudaError_t e = cudaSuccess;
+  int sms = 0, occ = 0;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_)) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block, kBlockThreads, kBlockSmem)) != cudaSuccess)
+    return check_cuda(e, "block occupancy");
+  const int max_grid = occ * sms;
+  if (max_grid < 1) return fail(E_INTERNAL, "persistent kernel does not fit an SM");
+  const int grid = opt_block_grid_ > 0 ? std::min(opt_block_grid_, max_grid) : sms;
+  const int stage_grid = sms * 4;
+  BlockSig sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.tv = tv_;
+  sig.tv.gen = 0;    // the kernels take the generation from the descriptor
+  sig.tv.epoch = 0;  // (LockNU claims no split epochs)
+  sig.dl = DirtyList{dirty_ref_, dirty_depth_};
+  uint32_t *bins = blk_.bins.as<uint32_t>();
+  sig.bb = BlockBufs{blk_.keys.as<uint8_t>(), blk_.kidx.as<int>(),      blk_.vals.as<uint8_t>(),
+                     blk_.vidx.as<int64_t>(), blk_.tid.as<int>(),       blk_.ptrie.as<int>(),
+                     blk_.poff.as<int>(),     blk_.out_ids.as<int>(),   blk_.out.as<uint8_t>(),
+                     blk_.koff.as<uint64_t>(), blk_.klen.as<uint32_t>(), bins,
+                     bins + 4 * (kDepthBins + 1), blk_.sorted.as<uint32_t>(),
+                     static_cast<BlockDesc *>(blk_.d_desc)};
+  sig.h_desc = blk_.h_desc;
+  sig.h_ctr = h_ctr_;
+  sig.grid = grid;
+  sig.stage_grid = stage_grid;
+  auto issue = [&]() -> cudaError_t {
+    cudaError_t x = cudaMemcpyAsync(blk_.d_desc, blk_.h_desc, sizeof(BlockDesc), cudaMemcpyHostToDevice, st_);
+    if (x != cudaSuccess) return x;
+    count_launch(), k_block_stage<<<stage_grid, kBlockThreads, 0, st_>>>(sig.tv, sig.bb);
+    if ((x = cudaGetLastError()) != cudaSuccess) return x;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBlockThreads);
+    cfg.dynamicSmemBytes = kBlockSmem;
+    cfg.stream = st_;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // all CTAs co-resident, or the launch fails
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    if ((x = cudaLaunchKernelEx(&cfg, k_block, sig.tv, sig.dl, sig.bb, (uint32_t)(1u << 20))) != cudaSuccess) return x;
+    if ((x = cudaMemcpyAsync(blk_.h_desc, blk_.d_desc, sizeof(BlockDesc), cudaMemcpyDeviceToHost, st_)) != cudaSuccess)
+      return x;
+    return cudaMemcpyAsync(h_ctr_, ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, st_);
+  };
+  binfo_.grid = grid;
+  if (!opt_block_graph_) {
+    if ((e = issue()) != cudaSuccess) return check_cuda(e, "block launch");
+    ++binfo_.launches;
+    return OK;
+  }
+  const uint8_t *sb = reinterpret_cast<const uint8_t *>(&sig);
+  if (!blk_.exec || blk_.sig.size() != sizeof(sig) || std::memcmp(blk_.sig.data(), sb, sizeof(sig)) != 0) {
+    if (blk_.exec) cudaGraphExecDestroy(blk_.exec);
+    if (blk_.graph) cudaGraphDestroy(blk_.graph);
+    blk_.exec = nullptr;
+    blk_.graph = nullptr;
+    blk_.sig.clear();
+    if ((e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return check_cuda(e, "block graph capture");
+    cudaError_t ie = issue();
+    e = cudaStreamEndCapture(st_, &blk_.graph);
+    if (ie != cudaSuccess) return check_cuda(ie, "block graph capture");
+    if (e != cudaSuccess) return check_cuda(e, "block graph capture end");
+    if ((e = cudaGraphInstantiate(&blk_.exec, blk_.graph, 0)) != cudaSuccess) {
+      blk_.exec = nullptr;
+      return check_cuda(e, "block graph instantiate");
+    }
+    blk_.sig.assign(sb, sb + sizeof(sig));
+    ++binfo_.captures;
+  }
+  if ((e = cudaGraphLaunch(blk_.exec, st_)) != cudaSuccess) return check_cuda(e, "block graph launch");
+  count_launch();
+  count_launch();
+  ++binfo_.launches;
+  return OK;
+}
+
+int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
+  err_.clear();
+  const int n = b.n;
+  if (n < 0 || n > (1 << 26) || b.n0 < 0 || b.n0 > n || b.n_out < 0 || b.n_out > (1 << 26))
+    return fail(E_ARG, "block sizes out of range");
+  if (n > 0 && (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs || !b.trie_ids))
+    return fail(E_ARG, "null block array");
+  if ((b.patch_trie == nullptr) != (b.patch_off == nullptr)) return fail(E_ARG, "patch_trie and patch_off go together");
+  if (b.n_out > 0 && (!b.out_ids || !out32 || !sizes)) return fail(E_ARG, "null output array");
+  for (int i = 0; i < b.n_out; ++i)
+    if (b.out_ids[i] < 0 || (uint32_t)b.out_ids[i] >= n_tries_) return fail(E_ARG, "trie id outside [0, max_tries)");
+  cudaSetDevice(dev_);
+  cudaEvent_t ev[4] = {};
+  if (timing_) {
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], st_);
+  }
+  struct EvGuard {
+    cudaEvent_t *e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } ev_guard{ev};
+  int64_t kb = b.keys_bytes, vb = b.values_bytes;
+  if (kb < 0 || vb < 0) {
+    if (b.device) return fail(E_ARG, "device blocks need keys_bytes and values_bytes");
+    kb = n ? (int64_t)b.keys_indexs[2 * n - 1] + 1 : 0;
+    vb = n ? (int64_t)b.values_indexs[2 * n - 1] + 1 : 0;
+  }
+  if (kb < 0 || vb < 0 || kb > 0x7FFFFFFFll) return fail(E_ARG, "bad stream lengths");
+  int rc = ensure_capacity((uint64_t)n, 3ull * n, (uint64_t)n, (uint64_t)n, (uint64_t)kb + 64, (uint64_t)vb + 80);
+  if (rc) return rc;
+  cudaError_t e = cudaSuccess;
+  const size_t nn = (size_t)std::max(n, 1), no = (size_t)std::max(b.n_out, 1);
+  if (e == cudaSuccess) e = blk_.keys.ensure((size_t)kb + 128);
+  if (e == cudaSuccess) e = blk_.kidx.ensure(8 * nn);
+  if (e == cudaSuccess) e = blk_.vals.ensure((size_t)vb + 128);
+  if (e == cudaSuccess) e = blk_.vidx.ensure(16 * nn);
+  if (e == cudaSuccess) e = blk_.tid.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.ptrie.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.poff.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.out_ids.ensure(4 * no);
+  if (e == cudaSuccess) e = blk_.out.ensure(33 * no);
+  if (e == cudaSuccess) e = blk_.koff.ensure(8 * nn);
+  if (e == cudaSuccess) e = blk_.klen.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.bins.ensure(sizeof(uint32_t) * (5 * (kDepthBins + 1)));
+  if (e == cudaSuccess) e = blk_.sorted.ensure(sizeof(uint32_t) * (cap_dirty_ + 64));
+  if (e == cudaSuccess && !blk_.d_desc) e = cudaMalloc(&blk_.d_desc, sizeof(BlockDesc));
+  if (e == cudaSuccess && !blk_.h_desc) e = cudaMallocHost(&blk_.h_desc, sizeof(BlockDesc));
+  if (e != cudaSuccess) return check_cuda(e, "block buffers");
+  const cudaMemcpyKind kind = b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (n > 0) {
+    e = cudaMemcpyAsync(blk_.keys.p, b.keys_hexs, (size_t)kb, kind, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.kidx.p, b.keys_indexs, 8 * (size_t)n, kind, st_);
+    if (e == cudaSuccess && vb) e = cudaMemcpyAsync(blk_.vals.p, b.values, (size_t)vb, kind, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.vidx.p, b.values_indexs, 16 * (size_t)n, kind, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.tid.p, b.trie_ids, 4 * (size_t)n, kind, st_);
+    if (b.patch_trie) {
+      if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.ptrie.p, b.patch_trie, 4 * (size_t)n, kind, st_);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.poff.p, b.patch_off, 4 * (size_t)n, kind, st_);
+    } else if (e == cudaSuccess) {
+      e = cudaMemsetAsync(blk_.ptrie.p, 0xFF, 4 * (size_t)n, st_);  // -1: no patch
+    }
+  }
+  if (e == cudaSuccess && b.n_out > 0)
+    e = cudaMemcpyAsync(blk_.out_ids.p, b.out_ids, 4 * (size_t)b.n_out, cudaMemcpyHostToDevice, st_);
+  if (e != cudaSuccess) return check_cuda(e, "block inputs");
+  BlockDesc *h = static_cast<BlockDesc *>(blk_.h_desc);
+  std::memset(h, 0, sizeof(BlockDesc));
+  const uint64_t val_base = (val_used_ + 7) & ~7ull;
+  h->n = n;
+  h->n0 = b.n0;
+  h->n_out = b.n_out;
+  h->kbytes = kb;
+  h->vbytes = vb;
+  h->key_base = key_used_;
+  h->val_base = val_base;
+  h->vid_base = n_rec_;
+  h->gen = gen_;
+  if (timing_) cudaEventRecord(ev[1], st_);
+  if ((rc = block_launch())) return rc;
+  if (timing_) cudaEventRecord(ev[2], st_);
+  if ((e = cudaStreamSynchronize(st_)) != cudaSuccess) return check_cuda(e, "block");
+  binfo_.levels[0] = h->levels[0];
+  binfo_.levels[1] = h->levels[1];
+  binfo_.dirty[0] = h->dirty[0];
+  binfo_.dirty[1] = h->dirty[1];
+  binfo_.n_ts = std::min<uint32_t>(h->n_ts, kBlockMaxTs);
+  std::memcpy(binfo_.ts, h->ts, sizeof(uint64_t) * binfo_.n_ts);
+  if (h->bad || h->noncontig || h->stream_terms != h->key_terms) {
+    cudaMemsetAsync(&ctr_->error, 0, 4, st_);
+    if (h->bad & BLOCK_BAD_TRIE) return fail(E_ARG, "trie id outside [0, max_tries)");
+    if (h->bad & BLOCK_BAD_PATCH)
+      return fail(E_ARG, "patch outside the value, of a stage-0 key, or naming a trie outside [0, max_tries)");
+    if (h->bad & BLOCK_BAD_VALUE) return fail(E_ARG, "value index pair outside the value stream");
+    if (h->noncontig) return fail(E_ARG, "block key index pairs must tile the key stream");
+    return fail(E_BAD_KEY, "malformed key: nibble > 16, terminator not last, or too long");
+  }
+  // the launch got past staging: the arena bytes and records are in use
+  key_used_ += ((uint64_t)kb + 7) & ~7ull;
+  val_used_ = val_base + (uint64_t)vb;
+  n_rec_ += (uint64_t)n;
+  gen_ += 2;
+  tv_.gen = gen_;
+  if (n > 0) empty_ = false;
+  stats_.key_bytes = key_used_;
+  stats_.value_bytes = val_used_;
+  stats_.n_records = n_rec_;
+  if ((rc = apply_counters())) return rc;
+  if (h->status & 1u) return fail(E_INTERNAL, "grid barrier wait gave up");
+  stats_.n_full = n_full_;
+  stats_.n_short = n_short_;
+  stats_.n_value = n_value_;
+  stats_.last_dirty = (uint64_t)h->dirty[0] + h->dirty[1];
+  stats_.last_hash_levels = (uint64_t)h->levels[0] + h->levels[1];
+  if (b.n_out > 0) {
+    std::vector<uint8_t> o(33 * (size_t)b.n_out);
+    if ((e = cudaMemcpyAsync(o.data(), blk_.out.p, o.size(), cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "block roots");
+    for (int i = 0; i < b.n_out; ++i) {
+      std::memcpy(out32 + 32 * (size_t)i, o.data() + 33 * (size_t)i, 32);
+      sizes[i] = o[33 * (size_t)i + 32];
+    }
+  }
+  if (timing_) {
+    cudaEventRecord(ev[3], st_);
+    cudaEventSynchronize(ev[3]);
+    cudaEventElapsedTime(&binfo_.t_inputs_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&binfo_.t_launch_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&binfo_.t_total_ms, ev[0], ev[3]);
+  }
+  return OK;
+}
+
+int Trie::reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes) {
+  err_.clear();
+  if (n_keys > (1ull << 30)) return fail(E_ARG, "reserve: too many keys");
+  cudaSetDevice(dev_);
+  int rc = sync_counters();
+  if (rc) return rc;
+  return ensure_capacity(2 * n_keys, 4 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8);
 }
 
 }  // namespace gmpt

@@ -37,6 +37,26 @@ struct BatchIn {
   bool device = false;        // pointers are device memory
 };
 
+// One persistent two-stage update of a forest (Trie::block_update): keys
+// [0, n0) are stage 0, keys [n0, n) stage 1; stage 1 runs after stage 0 is
+// hashed, and key i of stage 1 with patch_trie[i] >= 0 first gets the 32
+// root bytes of that trie (zero-padded below 32) written into its value at
+// byte patch_off[i].  Index pairs must tile the key and value streams.
+struct BlockIn {
+  const uint8_t *keys_hexs = nullptr;
+  const int *keys_indexs = nullptr;
+  const uint8_t *values = nullptr;
+  const int64_t *values_indexs = nullptr;
+  const int *trie_ids = nullptr;    // [n]
+  const int *patch_trie = nullptr;  // [n] or null (no patches)
+  const int *patch_off = nullptr;   // [n] or null
+  int n = 0, n0 = 0;
+  const int *out_ids = nullptr;     // host array [n_out]: tries whose roots are returned
+  int n_out = 0;
+  int64_t keys_bytes = -1, values_bytes = -1;  // required for device inputs
+  bool device = false;              // key/value/trie/patch arrays are device memory
+};
+
 struct TrieStats {
   uint64_t n_full, n_short, n_value, n_records;
   uint64_t key_bytes, value_bytes;
@@ -92,8 +112,24 @@ class Trie {
   int device() const { return dev_; }
   int max_tries() const { return (int)n_tries_; }
   void set_timing(bool on) { timing_ = on; }
-  // tuning knobs (names: "local_build", "local_sort")
+  // tuning knobs (names: "local_build", "local_sort", "block_grid", "block_graph")
   int set_option(const std::string &name, int64_t value);
+  // persistent graph-replayed forest update; out32[32 i..] / sizes[i] = root
+  // of trie out_ids[i] after the update
+  int block_update(const BlockIn &b, uint8_t *out32, int *sizes);
+  // the last block launch: stage levels / dirty counts, CTAs, graph rebuilds
+  struct BlockInfo {
+    uint32_t levels[2], dirty[2];
+    int grid;
+    uint32_t captures, launches;
+    float t_inputs_ms, t_launch_ms, t_total_ms;  // timing mode: input copies, graph, whole call
+    uint32_t n_ts;
+    uint64_t ts[64];  // device timeline of the last block (ns): stage start, k_block start, each barrier, end
+  };
+  // grow the pools and arenas now for n_keys more keys of the given byte
+  // totals (no growth stalls, and no block graph rebuild, until then)
+  int reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes);
+  const BlockInfo &block_info() const { return binfo_; }
 
  private:
   int dev_ = 0;
@@ -125,6 +161,20 @@ class Trie {
   uint16_t *dirty_depth_ = nullptr;
   uint64_t cap_dirty_ = 0;
 
+  // persistent block launches
+  struct BlockRt {
+    DevBlock keys, kidx, vals, vidx, tid, ptrie, poff, out_ids, out, koff, klen, bins, sorted;
+    void *d_desc = nullptr, *h_desc = nullptr;  // BlockDesc (device / pinned)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint8_t> sig;  // launch arguments the graph was captured with
+    int grid = 0;
+  } blk_;
+  BlockInfo binfo_{};
+  int opt_block_grid_ = 0;      // CTAs of the persistent kernel (0 = one per SM)
+  bool opt_block_graph_ = true;  // replay a captured graph (else plain launches)
+  int block_launch();
+
   // per-batch workspaces
   struct Ws {
     DevBlock koff, klen, ki, vi, hp, kin;          // staged batch
@@ -147,6 +197,7 @@ class Trie {
   int fail(int code, const std::string &msg);
   int check_cuda(cudaError_t e, const char *what);
   int sync_counters();
+  int apply_counters();
   int ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
                       uint64_t add_key_bytes, uint64_t add_val_bytes);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,

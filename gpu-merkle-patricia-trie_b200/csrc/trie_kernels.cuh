@@ -768,8 +768,28 @@ __device__ __forceinline__ void rlp_head(uint64_t size, uint32_t small_tag, uint
   pren = 1 + s;
 }
 
+// Loads of node fields and message bytes.  kCoh = true inside a persistent
+// launch, where the data may have been written earlier in the same launch by
+// another SM, before a grid barrier (fence, arrive, wait, fence): ordinary
+// loads then see those writes, but the non-coherent read-only path
+// (ld.global.nc) is not used for them.  Key nibbles are staged by an earlier
+// launch and stay on the read-only path in both modes.
+template <bool kCoh, typename T>
+__device__ __forceinline__ T ldn(const T *p) {
+  return *p;
+}
+
+template <bool kCoh>
+__device__ __forceinline__ uint64_t ld8(const uint8_t *p) {
+  if constexpr (kCoh)
+    return load_u64_unaligned_cg(p);
+  else
+    return load_u64_unaligned(p);
+}
+
 // the item a parent writes for child `r` (node.cuh:437-450 / 548-557;
 // rlp.cuh:132-155 write_bytes; a value node's "hash" is its raw value)
+template <bool kCoh = false>
 __device__ __forceinline__ EncItem child_item(const TrieView &tv, uint32_t r) {
   EncItem it{0, 0, 0, nullptr, 0};
   uint32_t kind = ref_kind(r), idx = ref_idx(r);
@@ -781,16 +801,16 @@ __device__ __forceinline__ EncItem child_item(const TrieView &tv, uint32_t r) {
   const uint8_t *h;
   uint32_t hl;
   if (kind == KIND_VALUE) {
-    unsigned long long vid = tv.value_vid[idx];
+    unsigned long long vid = ldn<kCoh>(tv.value_vid + idx);
     h = tv.vals + tv.rec_off[vid];
     hl = tv.rec_len[vid];
   } else {
     if (kind == KIND_FULL) {
       h = tv.full_hash + (size_t)idx * 32;
-      hl = tv.full_hlen[idx];
+      hl = ldn<kCoh>(tv.full_hlen + idx);
     } else {
       h = tv.short_hash + (size_t)idx * 32;
-      hl = tv.short_hlen[idx];
+      hl = ldn<kCoh>(tv.short_hlen + idx);
     }
     if (tv.geth_mode && hl < 32) {  // go-ethereum embeds small nodes
       it.body = h;
@@ -800,7 +820,7 @@ __device__ __forceinline__ EncItem child_item(const TrieView &tv, uint32_t r) {
   }
   it.body = h;
   it.blen = hl;
-  if (hl == 1 && h[0] < 0x80) return it;  // single byte is its own encoding
+  if (hl == 1 && ldn<kCoh>(h) < 0x80) return it;  // single byte is its own encoding
   rlp_head(hl, 0x80, 0xb7, it.pre, it.pren);
   return it;
 }
@@ -843,6 +863,7 @@ __device__ __forceinline__ uint64_t pack_pairs8(const uint8_t *p) {
   return r;
 }
 
+template <bool kCoh = false>
 __device__ __forceinline__ EncItem node_item(const TrieView &tv, bool full, uint32_t idx, int item,
                                              uint64_t payload) {
   EncItem it{0, 0, 0, nullptr, 0};
@@ -850,9 +871,9 @@ __device__ __forceinline__ EncItem node_item(const TrieView &tv, bool full, uint
     rlp_head(payload, 0xc0, 0xf7, it.pre, it.pren);
     return it;
   }
-  if (full) return child_item(tv, tv.full_child[(size_t)idx * 17 + (item - 1)]);
-  if (item == 1) return compact_item(tv, tv.short_key[idx], tv.short_klen[idx]);
-  return child_item(tv, tv.short_child[idx]);
+  if (full) return child_item<kCoh>(tv, ldn<kCoh>(tv.full_child + (size_t)idx * 17 + (item - 1)));
+  if (item == 1) return compact_item(tv, ldn<kCoh>(tv.short_key + idx), ldn<kCoh>(tv.short_klen + idx));
+  return child_item<kCoh>(tv, ldn<kCoh>(tv.short_child + idx));
 }
 
 // Thread per dirty node: RLP-encode straight into the sponge, Keccak-256 if
@@ -881,19 +902,16 @@ __device__ __forceinline__ void prefetch_child(const TrieView &tv, uint32_t r) {
     prefetch_l1(tv.short_hash + (size_t)idx * 32);
 }
 
-// 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
-// lanes in registers without spilling at this bound.
-__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
-  extern __shared__ uint64_t stage_all[];
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count) return;
-  uint32_t ref = refs[t];
+// Encode + hash one dirty node; `stage` is this thread's 17-word message
+// block in shared memory (word w at stage[w * stride]).
+template <bool kCoh>
+__device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint64_t *stage, uint32_t stride) {
   uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
   bool full = kind == KIND_FULL;
-  if (!full && tv.short_dead[idx]) return;
+  if (!full && ldn<kCoh>(tv.short_dead + idx)) return;
   // depth 0 holds exactly the roots of the forest's tries; go-ethereum
   // hashes a root whatever its size
-  bool force = tv.geth_mode && (full ? tv.full_depth[idx] : tv.short_depth[idx]) == 0;
+  bool force = tv.geth_mode && (full ? ldn<kCoh>(tv.full_depth + idx) : ldn<kCoh>(tv.short_depth + idx)) == 0;
   int nitems = full ? 18 : 3;
   // pass 1: payload size (all child loads issued together, sources prefetched)
   uint64_t payload = 0;
@@ -902,17 +920,17 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
     const uint32_t *chp = tv.full_child + (size_t)idx * 17;
     uint32_t ch[17];
 #pragma unroll
-    for (int k = 0; k < 17; ++k) ch[k] = chp[k];
+    for (int k = 0; k < 17; ++k) ch[k] = ldn<kCoh>(chp + k);
 #pragma unroll
     for (int k = 0; k < 17; ++k) prefetch_child(tv, ch[k]);
 #pragma unroll
     for (int k = 0; k < 17; ++k) {
-      EncItem it = child_item(tv, ch[k]);
+      EncItem it = child_item<kCoh>(tv, ch[k]);
       payload += it.pren + it.blen;
     }
   } else {
-    uint32_t child = tv.short_child[idx];
-    const uint8_t *kp = tv.keys + tv.short_key[idx];
+    uint32_t child = ldn<kCoh>(tv.short_child + idx);
+    const uint8_t *kp = tv.keys + ldn<kCoh>(tv.short_key + idx);
     prefetch_l1(kp);
     if (ref_kind(child) == KIND_VALUE) {
       unsigned long long vid = tv.value_vid[ref_idx(child)];
@@ -922,8 +940,8 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
     } else {
       prefetch_child(tv, child);
     }
-    it1 = node_item(tv, false, idx, 1, 0);
-    it2 = node_item(tv, false, idx, 2, 0);
+    it1 = node_item<kCoh>(tv, false, idx, 1, 0);
+    it2 = node_item<kCoh>(tv, false, idx, 2, 0);
     payload = it1.pren + it1.blen + it2.pren + it2.blen;
   }
   uint64_t hdr;
@@ -932,7 +950,7 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
   uint64_t total = payload + hn;
   bool raw = total < 32 && !force;
   Sponge sp;
-  sp.reset(stage_all + threadIdx.x, blockDim.x);
+  sp.reset(stage, stride);
   if (!full && total <= 135) {
     // One-block short node (every leaf with a value up to ~100 bytes, every
     // extension): place each segment's 8-byte chunks into the zeroed block
@@ -955,7 +973,7 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
     p += it2.pren;
     for (uint32_t o = 0; o < it2.blen; o += 8) {
       uint32_t nb = min(8u, it2.blen - o);
-      or_bytes(st, S, load_u64_unaligned(it2.body + o) & low_bytes_mask(nb), nb, p + o);
+      or_bytes(st, S, ld8<kCoh>(it2.body + o) & low_bytes_mask(nb), nb, p + o);
     }
     p += it2.blen;
     if (!raw) {
@@ -980,7 +998,7 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
       }
       if (off < cur.blen) {
         uint32_t nb = min(8u, cur.blen - off);
-        uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : load_u64_unaligned(cur.body + off);
+        uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : ld8<kCoh>(cur.body + off);
         sp.push(v & low_bytes_mask(nb), nb);
         off += nb;
         continue;
@@ -990,7 +1008,7 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
         last = true;
         break;
       }
-      cur = node_item(tv, full, idx, item, payload);
+      cur = node_item<kCoh>(tv, full, idx, item, payload);
       off = 0;
       pre_pending = true;
     }
@@ -1027,6 +1045,98 @@ __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32
     o[3] = sp.a[3];
     (full ? tv.full_hlen : tv.short_hlen)[idx] = 32;
   }
+}
+
+// Message buffer of one warp for hash_full_warp (8 Keccak blocks).
+constexpr int kWarpMsgBytes = 8 * 136;
+
+// Warp-cooperative encode + hash of branch node idx, for levels with few
+// nodes where one thread's serial encoding is the latency: lane k < 17 places
+// child k's item into the warp's message at its scanned offset, then lane 0
+// pads and permutes.  All 32 lanes call it with the same idx; returns false
+// (nothing written) when the encoding does not fit kWarpMsgBytes, and the
+// caller hashes the node with hash_node instead.
+template <bool kCoh>
+__device__ __forceinline__ bool hash_full_warp(const TrieView &tv, uint32_t idx, uint8_t *msg, uint64_t *stage,
+                                               uint32_t stride) {
+  const int lane = threadIdx.x & 31;
+  EncItem it{0, 0, 0, nullptr, 0};
+  if (lane < 17) it = child_item<kCoh>(tv, ldn<kCoh>(tv.full_child + (size_t)idx * 17 + lane));
+  const uint32_t sz = lane < 17 ? it.pren + it.blen : 0u;
+  uint32_t incl = sz;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t payload = __shfl_sync(0xffffffffu, incl, 31);
+  uint64_t hdr;
+  uint32_t hn;
+  rlp_head(payload, 0xc0, 0xf7, hdr, hn);
+  const uint32_t total = payload + hn;
+  if (total + 1 > (uint32_t)kWarpMsgBytes) return false;
+  const bool force = tv.geth_mode && ldn<kCoh>(tv.full_depth + idx) == 0;
+  const bool raw = total < 32 && !force;
+  const uint32_t nblk = raw ? 1u : (total + 1 + 135) / 136;
+  const uint32_t padded = nblk * 136;
+  // zero the blocks, then place the header and the items
+  uint64_t *m64 = reinterpret_cast<uint64_t *>(msg);
+  for (uint32_t w = lane; w < padded / 8; w += 32) m64[w] = 0;
+  __syncwarp();
+  if (lane == 0)
+    for (uint32_t b = 0; b < hn; ++b) msg[b] = (uint8_t)(hdr >> (8 * b));
+  if (lane < 17) {
+    uint32_t p = hn + incl - sz;
+    for (uint32_t b = 0; b < it.pren; ++b) msg[p + b] = (uint8_t)(it.pre >> (8 * b));
+    p += it.pren;
+    for (uint32_t o = 0; o < it.blen; o += 8) {
+      const uint64_t v = ld8<kCoh>(it.body + o);
+      const uint32_t nb = min(8u, it.blen - o);
+      for (uint32_t b = 0; b < nb; ++b) msg[p + o + b] = (uint8_t)(v >> (8 * b));
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    uint8_t *hout = tv.full_hash + (size_t)idx * 32;
+    uint64_t *o = reinterpret_cast<uint64_t *>(hout);
+    if (raw) {
+#pragma unroll
+      for (int w = 0; w < 4; ++w) o[w] = m64[w];  // zero beyond total
+      tv.full_hlen[idx] = (uint8_t)total;
+    } else {
+      msg[total] ^= 0x01;
+      msg[padded - 1] ^= 0x80;
+      uint64_t a[25];
+#pragma unroll
+      for (int w = 0; w < 25; ++w) a[w] = 0;
+      for (uint32_t b = 0; b < nblk; ++b) {
+#pragma unroll
+        for (int w = 0; w < 17; ++w) a[w] ^= m64[b * 17 + w];
+        keccak_f1600(a);
+      }
+      o[0] = a[0];
+      o[1] = a[1];
+      o[2] = a[2];
+      o[3] = a[3];
+      tv.full_hlen[idx] = 32;
+    }
+    atomicAdd(&tv.ctr->enc_bytes, (unsigned long long)total);
+    atomicAdd(&tv.ctr->keccak_blocks, (unsigned long long)(raw ? 0u : nblk));
+    atomicAdd(&tv.ctr->hashed, 1u);
+  }
+  __syncwarp();
+  (void)stage;
+  (void)stride;
+  return true;
+}
+
+// 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
+// lanes in registers without spilling at this bound.
+__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
+  extern __shared__ uint64_t stage_all[];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  hash_node<false>(tv, refs[t], stage_all + threadIdx.x, blockDim.x);
 }
 
 // ---------------------------------------------------------------------------

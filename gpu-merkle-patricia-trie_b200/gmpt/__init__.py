@@ -34,7 +34,8 @@ EXPORTS = [
     "gmpt_keccak256_batch", "gmpt_keccak256_batch_device", "gmpt_keccak_peak", "gmpt_launch_count",
     "gmpt_keccak256_batch_noalloc", "gmpt_set_option",
     "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
-    "gmpt_get_roots", "gmpt_gets_forest",
+    "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
+    "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -94,6 +95,14 @@ def lib():
         getattr(L, f).restype = i32
     L.gmpt_get_roots.argtypes = [vp, vp, i32, vp, vp]
     L.gmpt_gets_forest.argtypes = [vp, vp, vp, vp, i32, vp, vp]
+    L.gmpt_block_update.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp]
+    L.gmpt_block_update.restype = i32
+    L.gmpt_block_update_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, i64, i64, vp, i32, vp, vp]
+    L.gmpt_block_update_device.restype = i32
+    L.gmpt_block_info.argtypes = [vp, vp]
+    L.gmpt_block_times.argtypes = [vp, vp]
+    L.gmpt_block_timeline.argtypes = [vp, vp, i32, vp]
+    L.gmpt_reserve.argtypes = [vp, i64, i64, i64]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -166,6 +175,26 @@ def keccak256_batch(messages) -> list:
     return [out[32 * i: 32 * i + 32].tobytes() for i in range(len(msgs))]
 
 
+def keccak256_rows(msgs: np.ndarray, chunk: int = 1 << 22) -> np.ndarray:
+    """Keccak-256 of every row of a 2-D uint8 array (fixed-length messages)
+    on the GPU -> [rows, 32] uint8."""
+    msgs = np.ascontiguousarray(msgs, dtype=np.uint8)
+    rows, width = msgs.shape
+    out = np.empty((rows, 32), dtype=np.uint8)
+    for a in range(0, rows, chunk):
+        m = msgs[a: a + chunk]
+        k = len(m)
+        idx = np.empty(2 * k, dtype=np.int64)
+        starts = np.arange(k, dtype=np.int64) * width
+        idx[0::2] = starts
+        idx[1::2] = starts + width - 1
+        data = np.concatenate([m.reshape(-1), np.zeros(8, np.uint8)])
+        o = np.empty(32 * k, dtype=np.uint8)
+        _check(lib().gmpt_keccak256_batch(_p(data), _p(idx), k, _p(o)))
+        out[a: a + k] = o.reshape(k, 32)
+    return out
+
+
 def keccak_peak(device: int = 0) -> float:
     v = C.c_double()
     _check(lib().gmpt_keccak_peak(device, C.byref(v)))
@@ -236,6 +265,55 @@ class MPT:
         sizes = np.zeros(n, dtype=np.int32)
         _check(self._L.gmpt_gets_forest(self._h, _p(kh), _p(ki), _p(tid), n, _p(hps), _p(sizes)))
         return hps, sizes
+
+    def block_update(self, keys_hexs, keys_indexs, values, values_indexs, trie_ids, n0: int, out_ids,
+                     patch_trie=None, patch_off=None) -> list:
+        """One persistent launch: stage 0 = keys [0, n0), stage 1 = the rest
+        (values patched with stage-0 roots); returns the roots of out_ids."""
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
+        pt = None if patch_trie is None else np.ascontiguousarray(patch_trie, dtype=np.int32)
+        po = None if patch_off is None else np.ascontiguousarray(patch_off, dtype=np.int32)
+        oid = np.ascontiguousarray(out_ids, dtype=np.int32)
+        out = np.zeros(32 * max(len(oid), 1), dtype=np.uint8)
+        sizes = np.zeros(max(len(oid), 1), dtype=np.int32)
+        _check(self._L.gmpt_block_update(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(tid), _p(pt), _p(po),
+                                         len(ki) // 2, int(n0), _p(oid), len(oid), _p(out), _p(sizes)))
+        return [out[32 * i: 32 * i + sizes[i]].tobytes() for i in range(len(oid))]
+
+    def block_update_device(self, d_keys, d_kidx, d_vals, d_vidx, d_tid, d_ptrie, d_poff, n: int, n0: int,
+                            keys_bytes: int, values_bytes: int, out_ids, out=None, sizes=None) -> list:
+        """block_update with device-resident inputs (raw addresses; d_ptrie / d_poff may be 0)."""
+        oid = np.ascontiguousarray(out_ids, dtype=np.int32)
+        if out is None:
+            out = np.zeros(32 * max(len(oid), 1), dtype=np.uint8)
+        if sizes is None:
+            sizes = np.zeros(max(len(oid), 1), dtype=np.int32)
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_block_update_device(self._h, v(d_keys), v(d_kidx), v(d_vals), v(d_vidx), v(d_tid),
+                                                v(d_ptrie), v(d_poff), int(n), int(n0), int(keys_bytes),
+                                                int(values_bytes), _p(oid), len(oid), _p(out), _p(sizes)))
+        return [out[32 * i: 32 * i + sizes[i]].tobytes() for i in range(len(oid))]
+
+    def block_info(self) -> dict:
+        a = np.zeros(8, dtype=np.uint32)
+        _check(self._L.gmpt_block_info(self._h, _p(a)))
+        tm = np.zeros(3, dtype=np.float32)
+        _check(self._L.gmpt_block_times(self._h, _p(tm)))
+        return {"levels": (int(a[0]), int(a[1])), "dirty": (int(a[2]), int(a[3])), "grid": int(a[4]),
+                "captures": int(a[5]), "launches": int(a[6]), "t_inputs_ms": float(tm[0]),
+                "t_launch_ms": float(tm[1]), "t_total_ms": float(tm[2])}
+
+    def block_timeline(self) -> np.ndarray:
+        """Device timestamps (ns) of the last block's phases, relative to its start."""
+        a = np.zeros(64, dtype=np.uint64)
+        n = C.c_int()
+        _check(self._L.gmpt_block_timeline(self._h, _p(a), 64, C.byref(n)))
+        a = a[: n.value].astype(np.int64)
+        return a - a[0] if len(a) else a
+
+    def reserve(self, n_keys: int, key_bytes: int, value_bytes: int):
+        _check(self._L.gmpt_reserve(self._h, int(n_keys), int(key_bytes), int(value_bytes)))
 
     def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
                     values_bytes: int, d_hps: int = 0):

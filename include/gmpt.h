@@ -106,6 +106,49 @@ int gmpt_puts_latching_forest(gmpt_trie *t, const uint8_t *keys_hexs, const int 
                               const uint8_t *values_bytes, const int64_t *values_indexs,
                               const uint8_t *const *values_hps, const int *trie_ids, int n);
 
+/* One block of a forest in ONE persistent launch (no counterpart in the
+ * reference, whose per-trie puts_latching_with_valuehp_v2 + hash_onepass_v2
+ * pairs this replaces for a whole set of tries, gpu_mpt.cuh:554-615 and
+ * 1162-1191):
+ *   stage 0 = keys [0, n0): LockNU insert into tries trie_ids[i], PhaseHC;
+ *   stage 1 = keys [n0, n): key i with patch_trie[i] >= 0 first gets the 32
+ *     root bytes of trie patch_trie[i] (after stage 0; zero-padded when the
+ *     root is shorter or the trie empty) written into its value at byte
+ *     offset patch_off[i]; then LockNU insert and PhaseHC.
+ * This is the Ethereum block shape: storage tries in stage 0, the state trie
+ * in stage 1 with storageRoot patched into each account's RLP.  Key and
+ * value index pairs must tile their streams (keys back to back).  patch_trie
+ * and patch_off may both be NULL.  On return out32[32 j..] / out_sizes[j]
+ * hold the root of trie out_ids[j] (host array) after the block.  The
+ * staging copy and the persistent kernel are replayed from one captured CUDA
+ * graph, rebuilt only when a buffer or node pool grows.  Stage semantics per
+ * trie equal gmpt_puts_latching_forest + gmpt_hash_onepass. */
+int gmpt_block_update(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const uint8_t *values_bytes,
+                      const int64_t *values_indexs, const int *trie_ids, const int *patch_trie, const int *patch_off,
+                      int n, int n0, const int *out_ids, int n_out, uint8_t *out32, int *out_sizes);
+/* Same with device-resident key/value/trie/patch arrays (out_ids stays a
+ * host array). */
+int gmpt_block_update_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                             const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids,
+                             const int *d_patch_trie, const int *d_patch_off, int n, int n0, int64_t keys_bytes,
+                             int64_t values_bytes, const int *out_ids, int n_out, uint8_t *out32, int *out_sizes);
+/* The last block: hash levels of stage 0 / 1, dirty nodes of stage 0 / 1,
+ * CTAs of the persistent kernel, graph captures so far, block launches so
+ * far, 0. */
+int gmpt_block_info(gmpt_trie *t, uint32_t out[8]);
+/* With gmpt_set_timing on: the last block's input copies, graph replay and
+ * whole call, in ms (CUDA events on the trie's stream). */
+int gmpt_block_times(gmpt_trie *t, float out[3]);
+/* Device timeline of the last block (globaltimer ns, up to cap entries):
+ * staging start, persistent kernel start, each grid barrier, end.  *n =
+ * entries recorded. */
+int gmpt_block_timeline(gmpt_trie *t, uint64_t *out_ns, int cap, int *n);
+/* Grow the node pools and arenas now for n_keys more keys carrying
+ * key_bytes / value_bytes stream bytes, so later inserts (and block graphs)
+ * do not stall on growth.  No counterpart in the reference, whose arenas are
+ * fixed at construction (util/allocator.cuh:152-157). */
+int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_bytes);
+
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
 int gmpt_hash_onepass(gmpt_trie *t);
@@ -142,7 +185,11 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
 /* Tuning knobs of the batch pipeline (results never depend on them):
  *   "local_build" 1/0: finish build segments of <= 2048 keys inside one CTA
  *                      each (default 1) or keep every level device-wide;
- *   "local_sort"  1/0: same for the still-tied runs of the batch sort. */
+ *   "local_sort"  1/0: same for the still-tied runs of the batch sort;
+ *   "block_grid"  N:   CTAs of the persistent block kernel (0 = one per SM,
+ *                      capped at what can be co-resident);
+ *   "block_graph" 1/0: replay block launches from a captured CUDA graph
+ *                      (default 1) or issue them one by one. */
 int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value);
 /* per-phase CUDA-event timing into gmpt_stats (adds synchronisation) */
 int gmpt_set_timing(gmpt_trie *t, int on);

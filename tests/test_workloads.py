@@ -38,3 +38,86 @@ def test_vocab_keys_lengths():
     assert lens.min() >= 8 and lens.max() <= 96
     vl = b.values_indexs[1::2] - b.values_indexs[0::2] + 1
     assert vl.min() >= 128 and vl.max() <= 4096
+
+
+# -- Ethereum-shaped forest workload -------------------------------------------
+
+def _oracle_keccak_rows(msgs):
+    import oracle as O
+
+    return np.array([np.frombuffer(O.keccak256(m.tobytes()), np.uint8) for m in msgs]).reshape(-1, 32)
+
+
+def _rlp_items(buf: bytes):
+    """Decode one RLP list of short strings (enough for accounts)."""
+    assert buf[0] == 0xF8 and buf[1] == len(buf) - 2
+    items, p = [], 2
+    while p < len(buf):
+        h = buf[p]
+        assert 0x80 <= h <= 0xB7
+        items.append(buf[p + 1: p + 1 + h - 0x80])
+        p += 1 + h - 0x80
+    assert p == len(buf)
+    return items
+
+
+def test_empty_root_constant_is_keccak_of_empty_rlp():
+    import oracle as O
+    from gmpt import eth
+
+    assert eth.EMPTY_ROOT == O.keccak256(b"\x80")
+
+
+def test_account_values_are_rlp_accounts():
+    from gmpt import eth
+
+    rng = W.Xoshiro256ss(3)
+    roots = rng.bytes(32 * 500).reshape(500, 32)
+    vb, vi, roff = eth.account_values(rng, 500, roots)
+    for i in range(500):
+        v = vb[vi[2 * i]: vi[2 * i + 1] + 1].tobytes()
+        assert 71 <= len(v) <= 110
+        nonce, balance, sroot, code = _rlp_items(v)
+        assert len(sroot) == 32 and len(code) == 32 and 1 <= len(balance) <= 32 and len(nonce) <= 8
+        assert v[roff[i]: roff[i] + 32] == roots[i].tobytes() == sroot
+        if len(balance) == 1:
+            assert balance[0] >= 0x80
+        elif balance:
+            assert balance[0] != 0
+
+
+def test_power_law_sizes_range_and_skew():
+    from gmpt import eth
+
+    s = eth.power_law_sizes(W.Xoshiro256ss(4), 200000)
+    assert s.min() >= 1 and s.max() <= 5000
+    # density ~ s^-1.5 on [1, 5000]: mean ~ 70, median ~ 3.9
+    assert 55 < s.mean() < 90 and 2 <= np.median(s) <= 6
+
+
+def test_eth_block_layout():
+    from gmpt import eth
+
+    st = eth.make_state(500, _oracle_keccak_rows)
+    gen = eth.EthBlocks(st, _oracle_keccak_rows, min_updates=5, max_updates=12, max_storage=40)
+    seen = set()
+    for _ in range(3):
+        blk = gen.next()
+        b = blk.batch
+        assert blk.n0 == int(blk.spans[-1]) and blk.n == blk.n0 + len(blk.accounts)
+        assert np.all(blk.patch_trie[: blk.n0] == -1) and np.all(blk.trie_ids[blk.n0:] == 0)
+        assert np.all(blk.patch_trie[blk.n0:] == blk.storage_ids)
+        assert len(set(blk.storage_ids.tolist())) == len(blk.storage_ids) and 0 not in set(blk.storage_ids.tolist())
+        for j in range(len(blk.accounts)):
+            a, z = blk.spans[j], blk.spans[j + 1]
+            assert np.all(blk.trie_ids[a:z] == blk.storage_ids[j])
+        # index pairs tile both streams
+        assert b.keys_indexs[0] == 0 and np.all(b.keys_indexs[2::2] == b.keys_indexs[1:-1:2] + 1)
+        assert b.values_indexs[0] == 0 and np.all(b.values_indexs[2::2] == b.values_indexs[1:-1:2] + 1)
+        for j in range(blk.n0, blk.n):
+            ln = b.values_indexs[2 * j + 1] - b.values_indexs[2 * j] + 1
+            assert blk.patch_off[j] == ln - 65
+        # an account keeps its storage trie id across blocks
+        for a, s in zip(blk.accounts.tolist(), blk.storage_ids.tolist()):
+            assert gen.sid_of[a] == s
+            seen.add(a)
