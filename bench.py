@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=1 << 20)
+    p.add_argument("--eth-accounts", type=int, default=30_000_000, help="state trie accounts (0 = skip)")
+    p.add_argument("--eth-blocks", type=int, default=512)
+    p.add_argument("--eth-compare-blocks", type=int, default=32,
+                   help="blocks also run through the per-trie and forest multi-launch paths")
     return p.parse_args()
 
 
@@ -212,6 +216,145 @@ def cpu_baseline(args, batches):
         kind, cores, desc = "port", 1, "C restatement of the reference CPU MPT, one thread"
     return {"value": round(2 * n / dt / 1e6, 4), "unit": "Mkeys/s", "cores": cores, "kind": kind,
             "sample": f"first {n} keys of the load and of the update batch; {desc}"}
+
+
+def run_eth(args, local, dev):
+    """Ethereum-shaped forest: state trie + per-account storage tries, block by
+    block, through the persistent graph-replayed launch (device-resident and
+    pinned-host inputs) and, for the first blocks, through one-call-per-trie
+    and forest multi-launch paths on replicas of the same state."""
+    import torch
+
+    import gmpt
+    from gmpt import eth
+
+    t0 = time.time()
+    st = eth.make_state(args.eth_accounts, gmpt.keccak256_rows)
+    gen = eth.EthBlocks(st, gmpt.keccak256_rows)
+    blks = [gen.next() for _ in range(args.eth_blocks)]
+    setup_gen_s = time.time() - t0
+    tot_keys = sum(b.n for b in blks)
+    kb = sum(b.batch.key_bytes() for b in blks)
+    vb = sum(b.batch.value_bytes() for b in blks)
+    ncmp = min(args.eth_compare_blocks, len(blks))
+
+    def fresh():
+        f = gmpt.MPT(device=local, mode=gmpt.MODE_GETH, max_tries=gen.next_sid + 1)
+        b = st.batch
+        f.reserve(b.n + tot_keys, b.key_bytes() + kb, b.value_bytes() + vb)
+        f.puts_2phase_with_valuehp(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+        f.hash_onepass_v2()
+        f.reserve_block(max(x.n for x in blks), max(x.batch.key_bytes() for x in blks),
+                        max(x.batch.value_bytes() for x in blks), max(len(x.out_ids) for x in blks))
+        return f
+
+    t1 = time.time()
+    fb = fresh()
+    state_root = fb.get_root_hash()
+    setup_load_s = time.time() - t1
+    # device-resident block inputs
+    dblk = []
+    for b in blks:
+        arrs = [b.batch.keys_hexs, b.batch.keys_indexs, b.batch.values, b.batch.values_indexs, b.trie_ids,
+                b.patch_trie, b.patch_off]
+        dblk.append([torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in arrs])
+    stream = torch.cuda.ExternalStream(fb.stream_ptr(), device=dev)
+    torch.cuda.synchronize(dev)
+    # the largest block first sizes the block buffers (one graph capture)
+    roots_block, ms_block = [], []
+    launches0 = gmpt.launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    for b, d in zip(blks, dblk):
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fb.block_update_device(*[x.data_ptr() for x in d], b.n, b.n0, b.batch.key_bytes(),
+                                   b.batch.value_bytes(), b.out_ids)
+        z.record(stream)
+        z.synchronize()
+        roots_block.append(r)
+        ms_block.append(a.elapsed_time(z))
+    clocks = sampler.stop()
+    launches = gmpt.launch_count() - launches0
+    info = fb.block_info()
+    tl = fb.block_timeline()
+    fb.close()
+    del dblk
+    # e2e: pinned host inputs through the host C ABI, block by block
+    fe = fresh()
+    pinned = []
+    for b in blks:
+        arrs = [b.batch.keys_hexs, b.batch.keys_indexs, b.batch.values, b.batch.values_indexs, b.trie_ids,
+                b.patch_trie, b.patch_off]
+        pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in arrs])
+    L = gmpt.lib()
+    import ctypes
+    ms_e2e, h2d = [], 0
+    out = np.zeros(32 * 4096, np.uint8)
+    sizes = np.zeros(4096, np.int32)
+    for b, pa in zip(blks, pinned):
+        oid = b.out_ids
+        tt = time.perf_counter()
+        rc = L.gmpt_block_update(fe._h, *[ctypes.c_void_p(x.data_ptr()) for x in pa], b.n, b.n0,
+                                 oid.ctypes.data_as(ctypes.c_void_p), len(oid),
+                                 out.ctypes.data_as(ctypes.c_void_p), sizes.ctypes.data_as(ctypes.c_void_p))
+        ms_e2e.append((time.perf_counter() - tt) * 1e3)
+        if rc:
+            raise RuntimeError(L.gmpt_last_error_message().decode())
+        h2d += sum(x.numel() * x.element_size() for x in pa) + 4 * len(oid)
+    e2e_root = out[:32].tobytes()
+    assert e2e_root == roots_block[-1][0], "pinned-host and device block paths disagree"
+    fe.close()
+    del pinned
+    # the same first blocks one trie at a time, and as forest multi-launch batches
+    fp = fresh()
+    ms_plain = []
+    for k in range(ncmp):
+        tt = time.perf_counter()
+        r = eth.apply_plain(fp, blks[k])
+        ms_plain.append((time.perf_counter() - tt) * 1e3)
+        assert r == roots_block[k], f"per-trie path disagrees at block {k}"
+    fp.close()
+    ff = fresh()
+    ms_forest = []
+    for k in range(ncmp):
+        tt = time.perf_counter()
+        r = eth.apply_forest(ff, blks[k])
+        ms_forest.append((time.perf_counter() - tt) * 1e3)
+        assert r == roots_block[k], f"forest path disagrees at block {k}"
+    ff.close()
+    keys_cmp = sum(b.n for b in blks[:ncmp])
+
+    def rate(keys, ms):
+        return round(keys / (sum(ms) / 1e3) / 1e6, 3)
+
+    blk_rate = rate(tot_keys, ms_block)
+    plain_rate = rate(keys_cmp, ms_plain)
+    return {
+        "workload": f"ethereum-shaped forest: state trie of {args.eth_accounts} accounts (key = Keccak-256 of a random "
+                    f"20 B address, 71-110 B RLP account); {len(blks)} blocks of U[150,400] account updates, each "
+                    "touched account's storage trie gets p(s)~s^-1.5 on [1,5000] entries (Keccak slot keys, "
+                    "1-32 B values); storage roots written into the account values; go-ethereum encoding",
+        "keys": tot_keys, "tries_touched_per_block": round(float(np.mean([len(b.storage_ids) + 1 for b in blks])), 1),
+        "keys_per_block": round(tot_keys / len(blks), 1),
+        "block_mkeys_s": blk_rate, "block_p50_ms": round(float(np.percentile(ms_block, 50)), 3),
+        "block_p99_ms": round(float(np.percentile(ms_block, 99)), 3),
+        "e2e_mkeys_s": rate(tot_keys, ms_e2e), "e2e_p50_ms": round(float(np.percentile(ms_e2e, 50)), 3),
+        "e2e_p99_ms": round(float(np.percentile(ms_e2e, 99)), 3), "e2e_h2d_bytes": int(h2d),
+        "compare_blocks": ncmp,
+        "plain_per_trie_mkeys_s": plain_rate, "plain_p50_ms": round(float(np.percentile(ms_plain, 50)), 3),
+        "forest_multilaunch_mkeys_s": rate(keys_cmp, ms_forest),
+        "forest_p50_ms": round(float(np.percentile(ms_forest, 50)), 3),
+        "block_vs_plain": round(blk_rate / plain_rate, 2) if plain_rate else None,
+        "block_vs_forest": round(blk_rate / rate(keys_cmp, ms_forest), 2),
+        "roots_agree": True, "state_root_before": state_root.hex(), "state_root_after": roots_block[-1][0].hex(),
+        "persistent_grid": info["grid"], "graph_captures": info["captures"], "gpu_launches": int(launches),
+        "last_block_levels": info["levels"], "last_block_dirty": info["dirty"],
+        "last_block_timeline_us": [round(x / 1e3, 1) for x in np.diff(tl).tolist()],
+        "setup_s": {"generate": round(setup_gen_s, 1), "load_state": round(setup_load_s, 1)},
+        "clocks": clocks,
+    }
 
 
 def run_ours(args, world, rank, local):
@@ -401,9 +544,15 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, batches)
+    if world == 1 and args.eth_accounts > 0:
+        t.close()
+        del dbat
+        torch.cuda.empty_cache()
+        line["batched"] = run_eth(args, local, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    t.close()
+    if not (world == 1 and args.eth_accounts > 0):
+        t.close()
     if world > 1:
         import torch.distributed as dist
 

@@ -190,6 +190,12 @@ int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_
   return record_trie(t->t->reserve((uint64_t)n_keys, (uint64_t)key_bytes, (uint64_t)value_bytes), t->t);
 }
 
+int gmpt_reserve_block(gmpt_trie *t, int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes,
+                       int64_t max_out) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->reserve_block(max_keys, max_key_bytes, max_value_bytes, max_out), t->t);
+}
+
 int gmpt_block_times(gmpt_trie *t, float out[3]) {
   if (!t || !out) return record(GMPT_E_ARG, "null argument");
   const gmpt::Trie::BlockInfo &bi = t->t->block_info();

@@ -1139,7 +1139,7 @@ struct BlockSig {
 
 }  // namespace
 
-int Trie::block_launch() {
+int Trie::block_launch(bool launch) {
   cudaError_t e = cudaSuccess;
   int sms = 0, occ = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_)) != cudaSuccess ||
@@ -1189,6 +1189,7 @@ int Trie::block_launch() {
   };
   binfo_.grid = grid;
   if (!opt_block_graph_) {
+    if (!launch) return OK;
     if ((e = issue()) != cudaSuccess) return check_cuda(e, "block launch");
     ++binfo_.launches;
     return OK;
@@ -1213,6 +1214,7 @@ int Trie::block_launch() {
     blk_.sig.assign(sb, sb + sizeof(sig));
     ++binfo_.captures;
   }
+  if (!launch) return OK;
   if ((e = cudaGraphLaunch(blk_.exec, st_)) != cudaSuccess) return check_cuda(e, "block graph launch");
   count_launch();
   count_launch();
@@ -1253,24 +1255,8 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   if (kb < 0 || vb < 0 || kb > 0x7FFFFFFFll) return fail(E_ARG, "bad stream lengths");
   int rc = ensure_capacity((uint64_t)n, 3ull * n, (uint64_t)n, (uint64_t)n, (uint64_t)kb + 64, (uint64_t)vb + 80);
   if (rc) return rc;
+  if ((rc = block_buffers(n, kb, vb, b.n_out))) return rc;
   cudaError_t e = cudaSuccess;
-  const size_t nn = (size_t)std::max(n, 1), no = (size_t)std::max(b.n_out, 1);
-  if (e == cudaSuccess) e = blk_.keys.ensure((size_t)kb + 128);
-  if (e == cudaSuccess) e = blk_.kidx.ensure(8 * nn);
-  if (e == cudaSuccess) e = blk_.vals.ensure((size_t)vb + 128);
-  if (e == cudaSuccess) e = blk_.vidx.ensure(16 * nn);
-  if (e == cudaSuccess) e = blk_.tid.ensure(4 * nn);
-  if (e == cudaSuccess) e = blk_.ptrie.ensure(4 * nn);
-  if (e == cudaSuccess) e = blk_.poff.ensure(4 * nn);
-  if (e == cudaSuccess) e = blk_.out_ids.ensure(4 * no);
-  if (e == cudaSuccess) e = blk_.out.ensure(33 * no);
-  if (e == cudaSuccess) e = blk_.koff.ensure(8 * nn);
-  if (e == cudaSuccess) e = blk_.klen.ensure(4 * nn);
-  if (e == cudaSuccess) e = blk_.bins.ensure(sizeof(uint32_t) * (5 * (kDepthBins + 1)));
-  if (e == cudaSuccess) e = blk_.sorted.ensure(sizeof(uint32_t) * (cap_dirty_ + 64));
-  if (e == cudaSuccess && !blk_.d_desc) e = cudaMalloc(&blk_.d_desc, sizeof(BlockDesc));
-  if (e == cudaSuccess && !blk_.h_desc) e = cudaMallocHost(&blk_.h_desc, sizeof(BlockDesc));
-  if (e != cudaSuccess) return check_cuda(e, "block buffers");
   const cudaMemcpyKind kind = b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (n > 0) {
     e = cudaMemcpyAsync(blk_.keys.p, b.keys_hexs, (size_t)kb, kind, st_);
@@ -1356,13 +1342,49 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   return OK;
 }
 
+// Block input / scratch buffers for a block of n keys (grown, never shrunk).
+int Trie::block_buffers(int64_t n, int64_t kb, int64_t vb, int64_t n_out) {
+  cudaError_t e = cudaSuccess;
+  const size_t nn = (size_t)std::max<int64_t>(n, 1), no = (size_t)std::max<int64_t>(n_out, 1);
+  if (e == cudaSuccess) e = blk_.keys.ensure((size_t)kb + 128);
+  if (e == cudaSuccess) e = blk_.kidx.ensure(8 * nn);
+  if (e == cudaSuccess) e = blk_.vals.ensure((size_t)vb + 128);
+  if (e == cudaSuccess) e = blk_.vidx.ensure(16 * nn);
+  if (e == cudaSuccess) e = blk_.tid.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.ptrie.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.poff.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.out_ids.ensure(4 * no);
+  if (e == cudaSuccess) e = blk_.out.ensure(33 * no);
+  if (e == cudaSuccess) e = blk_.koff.ensure(8 * nn);
+  if (e == cudaSuccess) e = blk_.klen.ensure(4 * nn);
+  if (e == cudaSuccess) e = blk_.bins.ensure(sizeof(uint32_t) * (5 * (kDepthBins + 1)));
+  if (e == cudaSuccess) e = blk_.sorted.ensure(sizeof(uint32_t) * (cap_dirty_ + 64));
+  if (e == cudaSuccess && !blk_.d_desc) e = cudaMalloc(&blk_.d_desc, sizeof(BlockDesc));
+  if (e == cudaSuccess && !blk_.h_desc) e = cudaMallocHost(&blk_.h_desc, sizeof(BlockDesc));
+  return check_cuda(e, "block buffers");
+}
+
+int Trie::reserve_block(int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes, int64_t max_out) {
+  err_.clear();
+  if (max_keys < 0 || max_keys > (1 << 26) || max_key_bytes < 0 || max_value_bytes < 0 || max_out < 0)
+    return fail(E_ARG, "reserve_block: bad sizes");
+  cudaSetDevice(dev_);
+  int rc = sync_counters();
+  if (!rc) rc = ensure_capacity((uint64_t)max_keys, 3ull * max_keys, (uint64_t)max_keys, (uint64_t)max_keys,
+                                (uint64_t)max_key_bytes + 64, (uint64_t)max_value_bytes + 80);
+  if (!rc) rc = block_buffers(max_keys, max_key_bytes, max_value_bytes, max_out);
+  if (!rc) rc = block_launch(false);
+  return rc;
+}
+
 int Trie::reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes) {
   err_.clear();
   if (n_keys > (1ull << 30)) return fail(E_ARG, "reserve: too many keys");
   cudaSetDevice(dev_);
   int rc = sync_counters();
   if (rc) return rc;
-  return ensure_capacity(2 * n_keys, 4 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8);
+  // LockNU / block bound per key: one branch, three short nodes, one value
+  return ensure_capacity(n_keys, 3 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8);
 }
 
 }  // namespace gmpt

@@ -129,6 +129,9 @@ class Trie {
   // grow the pools and arenas now for n_keys more keys of the given byte
   // totals (no growth stalls, and no block graph rebuild, until then)
   int reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes);
+  // size the block buffers for blocks up to these sizes and capture the
+  // block graph now (so the first blocks do not pay for it)
+  int reserve_block(int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes, int64_t max_out);
   const BlockInfo &block_info() const { return binfo_; }
 
  private:
@@ -173,7 +176,8 @@ class Trie {
   BlockInfo binfo_{};
   int opt_block_grid_ = 0;      // CTAs of the persistent kernel (0 = one per SM)
   bool opt_block_graph_ = true;  // replay a captured graph (else plain launches)
-  int block_launch();
+  int block_launch(bool launch = true);
+  int block_buffers(int64_t n, int64_t kb, int64_t vb, int64_t n_out);
 
   // per-batch workspaces
   struct Ws {

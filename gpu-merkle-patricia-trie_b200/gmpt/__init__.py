@@ -35,7 +35,7 @@ EXPORTS = [
     "gmpt_keccak256_batch_noalloc", "gmpt_set_option",
     "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
     "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
-    "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline",
+    "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -103,6 +103,7 @@ def lib():
     L.gmpt_block_times.argtypes = [vp, vp]
     L.gmpt_block_timeline.argtypes = [vp, vp, i32, vp]
     L.gmpt_reserve.argtypes = [vp, i64, i64, i64]
+    L.gmpt_reserve_block.argtypes = [vp, i64, i64, i64, i64]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -311,6 +312,10 @@ class MPT:
         _check(self._L.gmpt_block_timeline(self._h, _p(a), 64, C.byref(n)))
         a = a[: n.value].astype(np.int64)
         return a - a[0] if len(a) else a
+
+    def reserve_block(self, max_keys: int, max_key_bytes: int, max_value_bytes: int, max_out: int):
+        _check(self._L.gmpt_reserve_block(self._h, int(max_keys), int(max_key_bytes), int(max_value_bytes),
+                                          int(max_out)))
 
     def reserve(self, n_keys: int, key_bytes: int, value_bytes: int):
         _check(self._L.gmpt_reserve(self._h, int(n_keys), int(key_bytes), int(value_bytes)))

@@ -53,34 +53,30 @@ def account_values(rng: W.Xoshiro256ss, n: int, storage_roots: np.ndarray | None
     """RLP accounts [nonce, balance, storageRoot, codeHash].
 
     Returns (values, values_indexs, root_off): root_off[i] is the byte offset
-    of storageRoot inside value i (always len - 65)."""
+    of storageRoot inside value i (always len - 65).  Every field sits at its
+    largest offset in a 110-column row and one mask keeps the bytes in use,
+    so the row-major compaction is the concatenated encodings."""
     ln, nb = _rlp_uint_bytes(rng, n, 8, 0)
     lb, bb = _rlp_uint_bytes(rng, n, 32, 1)
     code = rng.bytes(32 * n).reshape(n, 32)
     if storage_roots is None:
         storage_roots = np.tile(np.frombuffer(EMPTY_ROOT, np.uint8), (n, 1))
     total = 70 + ln + lb
-    arr = np.zeros((n, MAX_ACCOUNT_BYTES), dtype=np.uint8)
-    rows = np.arange(n)
+    arr = np.empty((n, MAX_ACCOUNT_BYTES), dtype=np.uint8)
     arr[:, 0] = 0xF8
     arr[:, 1] = (total - 2).astype(np.uint8)
     arr[:, 2] = (0x80 + ln).astype(np.uint8)
-    for j in range(8):
-        m = ln > j
-        arr[rows[m], 3 + j] = nb[m, j]
-    sb = 3 + ln
-    arr[rows, sb] = (0x80 + lb).astype(np.uint8)
-    for j in range(32):
-        m = lb > j
-        arr[rows[m], sb[m] + 1 + j] = bb[m, j]
-    sr = sb + 1 + lb
-    arr[rows, sr] = 0xA0
-    for j in range(32):
-        arr[rows, sr + 1 + j] = storage_roots[:, j]
-    arr[rows, sr + 33] = 0xA0
-    for j in range(32):
-        arr[rows, sr + 34 + j] = code[:, j]
-    mask = np.arange(MAX_ACCOUNT_BYTES)[None, :] < total[:, None]
+    arr[:, 3:11] = nb
+    arr[:, 11] = (0x80 + lb).astype(np.uint8)
+    arr[:, 12:44] = bb
+    arr[:, 44] = 0xA0
+    arr[:, 45:77] = storage_roots
+    arr[:, 77] = 0xA0
+    arr[:, 78:110] = code
+    col = np.arange(MAX_ACCOUNT_BYTES)
+    mask = np.ones((n, MAX_ACCOUNT_BYTES), dtype=bool)
+    mask[:, 3:11] = col[None, 3:11] - 3 < ln[:, None]
+    mask[:, 12:44] = col[None, 12:44] - 12 < lb[:, None]
     vb = arr[mask]
     offs = np.zeros(n + 1, dtype=np.int64)
     np.cumsum(total, out=offs[1:])

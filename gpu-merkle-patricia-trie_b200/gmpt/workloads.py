@@ -138,6 +138,21 @@ def keys_to_hexs(key_bytes: np.ndarray, key_lens: np.ndarray):
     (util/utils.cuh:340-349 applied per key)."""
     key_lens = key_lens.astype(np.int64)
     n = len(key_lens)
+    if n and np.all(key_lens == key_lens[0]):
+        # fixed length: one (n, 2L+1) array, nibbles interleaved + terminator
+        L = int(key_lens[0])
+        kb = np.asarray(key_bytes, dtype=np.uint8).reshape(n, L)
+        rows = np.empty((n, 2 * L + 1), dtype=np.uint8)
+        rows[:, 0:2 * L:2] = kb >> 4
+        rows[:, 1:2 * L:2] = kb & 15
+        rows[:, 2 * L] = 16
+        if n * (2 * L + 1) >= 2 ** 31:
+            raise ValueError("key stream exceeds the int32 index range")
+        starts = np.arange(n, dtype=np.int64) * (2 * L + 1)
+        idx = np.empty(2 * n, dtype=np.int32)
+        idx[0::2] = starts
+        idx[1::2] = starts + 2 * L
+        return rows.reshape(-1), idx
     hex_lens = 2 * key_lens + 1
     hoffs = np.zeros(n + 1, dtype=np.int64)
     np.cumsum(hex_lens, out=hoffs[1:])

@@ -148,6 +148,13 @@ int gmpt_block_timeline(gmpt_trie *t, uint64_t *out_ns, int cap, int *n);
  * do not stall on growth.  No counterpart in the reference, whose arenas are
  * fixed at construction (util/allocator.cuh:152-157). */
 int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_bytes);
+/* Size the gmpt_block_update buffers for blocks of up to max_keys keys,
+ * max_key_bytes / max_value_bytes stream bytes and max_out reported roots,
+ * and capture the block graph now, so that no block of that size pays for
+ * buffer growth or a capture.  Also reserves the node pools for one such
+ * block. */
+int gmpt_reserve_block(gmpt_trie *t, int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes,
+                       int64_t max_out);
 
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */

@@ -121,3 +121,17 @@ def test_eth_block_layout():
         for a, s in zip(blk.accounts.tolist(), blk.storage_ids.tolist()):
             assert gen.sid_of[a] == s
             seen.add(a)
+
+
+def test_keys_to_hexs_fixed_and_ragged_paths_agree_with_per_key_expansion():
+    from conftest import nib
+
+    rng = W.Xoshiro256ss(11)
+    for lens in (np.full(50, 7), np.array([3, 1, 9, 9, 2, 16, 5] * 5)):
+        kb = rng.bytes(int(lens.sum()))
+        kh, ki = W.keys_to_hexs(kb, lens)
+        pos = 0
+        for i, ln in enumerate(lens.tolist()):
+            want = nib(kb[pos: pos + ln].tobytes())
+            pos += ln
+            assert kh[ki[2 * i]: ki[2 * i + 1] + 1].tolist() == want
