@@ -10,10 +10,15 @@
 
 #include "../../include/gmpt.h"
 #include "../../include/libgmpt.h"
+#include "mlp.h"
 #include "trie.h"
 
 struct gmpt_trie {
   gmpt::Trie *t;
+};
+
+struct gmpt_mlp {
+  gmpt::Mlp *m;
 };
 
 namespace {
@@ -367,6 +372,61 @@ int gmpt_keccak_peak(int device, double *perm_per_s) {
 }
 
 void *gmpt_stream(gmpt_trie *t) { return t ? static_cast<void *>(t->t->stream()) : nullptr; }
+
+gmpt_mlp *gmpt_mlp_create(int device, int n_in, int n_hidden, int n_out, uint64_t seed) {
+  gmpt_mlp *h = new (std::nothrow) gmpt_mlp{nullptr};
+  if (!h) {
+    record(GMPT_E_CAPACITY, "out of host memory");
+    return nullptr;
+  }
+  h->m = new (std::nothrow) gmpt::Mlp(device, n_in, n_hidden, n_out, seed);
+  if (!h->m || !h->m->error().empty()) {
+    record(GMPT_E_ARG, h->m ? h->m->error() : "out of host memory");
+    delete h->m;
+    delete h;
+    return nullptr;
+  }
+  record(0, "");
+  return h;
+}
+
+void gmpt_mlp_destroy(gmpt_mlp *m) {
+  if (!m) return;
+  delete m->m;
+  delete m;
+}
+
+int gmpt_mlp_num_params(gmpt_mlp *m) { return m ? m->m->n_params() : 0; }
+
+static int record_mlp(int rc, gmpt::Mlp *m) { return record(rc ? GMPT_E_CUDA : 0, rc ? m->error() : std::string()); }
+
+int gmpt_mlp_get_params(gmpt_mlp *m, float *out) {
+  if (!m || !out) return record(GMPT_E_ARG, "null argument");
+  return record_mlp(m->m->get_params(out), m->m);
+}
+
+int gmpt_mlp_set_params(gmpt_mlp *m, const float *in) {
+  if (!m || !in) return record(GMPT_E_ARG, "null argument");
+  return record_mlp(m->m->set_params(in), m->m);
+}
+
+int gmpt_mlp_forward(gmpt_mlp *m, const float *x, int n, float *y) {
+  if (!m || n < 0 || (n > 0 && (!x || !y))) return record(GMPT_E_ARG, "null argument");
+  return record_mlp(m->m->forward(x, n, y), m->m);
+}
+
+int gmpt_mlp_loss_grad(gmpt_mlp *m, const float *x, const float *t, const float *mask, int n, float *loss,
+                       float *grad) {
+  if (!m || n < 1 || !x || !t || !mask || !loss || !grad) return record(GMPT_E_ARG, "null argument");
+  return record_mlp(m->m->loss_grad(x, t, mask, n, loss, grad), m->m);
+}
+
+int gmpt_mlp_train(gmpt_mlp *m, const float *x, const float *t, const float *mask, int n, int epochs, int batch,
+                   float lr, uint64_t seed, float *loss) {
+  if (!m || n < 0 || epochs < 0 || !loss || (n > 0 && (!x || !t || !mask))) return record(GMPT_E_ARG, "null argument");
+  if (batch < 1 || batch > 64) return record(GMPT_E_ARG, "batch must be in [1, 64]");
+  return record_mlp(m->m->train(x, t, mask, n, epochs, batch, lr, seed, loss), m->m);
+}
 
 int gmpt_last_error(void) { return g_last; }
 const char *gmpt_last_error_message(void) { return g_msg.c_str(); }

@@ -36,6 +36,8 @@ EXPORTS = [
     "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
     "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
+    "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
+    "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -104,6 +106,15 @@ def lib():
     L.gmpt_block_timeline.argtypes = [vp, vp, i32, vp]
     L.gmpt_reserve.argtypes = [vp, i64, i64, i64]
     L.gmpt_reserve_block.argtypes = [vp, i64, i64, i64, i64]
+    L.gmpt_mlp_create.restype = vp
+    L.gmpt_mlp_create.argtypes = [i32, i32, i32, i32, C.c_uint64]
+    L.gmpt_mlp_destroy.argtypes = [vp]
+    L.gmpt_mlp_num_params.argtypes = [vp]
+    L.gmpt_mlp_get_params.argtypes = [vp, vp]
+    L.gmpt_mlp_set_params.argtypes = [vp, vp]
+    L.gmpt_mlp_forward.argtypes = [vp, vp, i32, vp]
+    L.gmpt_mlp_loss_grad.argtypes = [vp, vp, vp, vp, i32, vp, vp]
+    L.gmpt_mlp_train.argtypes = [vp, vp, vp, vp, i32, i32, i32, C.c_float, C.c_uint64, vp]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -204,6 +215,61 @@ def keccak_peak(device: int = 0) -> float:
 
 def launch_count() -> int:
     return int(lib().gmpt_launch_count())
+
+
+class Net:
+    """The selector's MLP on the GPU (gmpt_mlp_*): hand-written CUDA forward,
+    gradient and Adam training kernels."""
+
+    def __init__(self, n_in: int, n_hidden: int, n_out: int, seed: int = 1, device: int = 0):
+        self._L = lib()
+        self.dims = (n_in, n_hidden, n_out)
+        self._h = self._L.gmpt_mlp_create(device, n_in, n_hidden, n_out, seed)
+        if not self._h:
+            raise GmptError(self._L.gmpt_last_error(), self._L.gmpt_last_error_message().decode())
+        self.n_params = self._L.gmpt_mlp_num_params(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gmpt_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        _check(self._L.gmpt_mlp_get_params(self._h, _p(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        _check(self._L.gmpt_mlp_set_params(self._h, _p(p)))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.dims[0])
+        y = np.zeros((len(x), self.dims[2]), dtype=np.float32)
+        _check(self._L.gmpt_mlp_forward(self._h, _p(x), len(x), _p(y)))
+        return y
+
+    def loss_grad(self, x, t, m):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        _check(self._L.gmpt_mlp_loss_grad(self._h, _p(x), _p(t), _p(m), len(x), _p(loss), _p(g)))
+        return float(loss[0]), g
+
+    def train(self, x, t, m, epochs: int, batch: int = 64, lr: float = 1e-3, seed: int = 7) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        _check(self._L.gmpt_mlp_train(self._h, _p(x), _p(t), _p(m), len(x), int(epochs), int(batch), float(lr),
+                                      int(seed), _p(loss)))
+        return float(loss[0])
 
 
 class MPT:

@@ -237,6 +237,35 @@ int gmpt_keccak_peak(int device, double *perm_per_s);
 /* Number of kernels this library has launched in this process. */
 uint64_t gmpt_launch_count(void);
 
+/* ---- schedule selector network --------------------------------------
+ * A two-hidden-layer ReLU MLP (n_in <= 16, n_hidden <= 64, n_out <= 8, fp32)
+ * with hand-written CUDA inference, gradient and Adam training kernels; the
+ * library's schedule selector predicts per-configuration batch times with it.
+ * No counterpart in the reference, whose insert strategy is fixed
+ * (libgmpt.cu:107-111) and whose model fitting happens offline
+ * (experiments.cu:3250-3348).  Parameters, flat: W1[H][I] b1[H] W2[H][H]
+ * b2[H] W3[O][H] b3[O]; He-uniform weights from `seed`, zero biases.
+ * Loss: sum of mask * (y - target)^2 over all outputs / sum of mask. */
+typedef struct gmpt_mlp gmpt_mlp;
+gmpt_mlp *gmpt_mlp_create(int device, int n_in, int n_hidden, int n_out, uint64_t seed);
+void gmpt_mlp_destroy(gmpt_mlp *m);
+int gmpt_mlp_num_params(gmpt_mlp *m);
+int gmpt_mlp_get_params(gmpt_mlp *m, float *out);
+/* also clears the Adam moments and step count */
+int gmpt_mlp_set_params(gmpt_mlp *m, const float *in);
+/* y[n][n_out] for x[n][n_in] (host arrays) */
+int gmpt_mlp_forward(gmpt_mlp *m, const float *x, int n, float *y);
+/* loss and gradient (n_params floats) over all n samples */
+int gmpt_mlp_loss_grad(gmpt_mlp *m, const float *x, const float *t, const float *mask, int n, float *loss,
+                       float *grad);
+/* Adam (0.9, 0.999, 1e-8) over `epochs` passes in mini-batches of `batch`
+ * (1..64) samples, one launch; epoch e visits positions j of [0, P), P the
+ * next power of two >= n, as sample (a_e j + b_e) mod P, skipping images >= n,
+ * with a_e odd and b_e from splitmix64 of seed and e.  *loss = mean
+ * mini-batch loss of the last epoch. */
+int gmpt_mlp_train(gmpt_mlp *m, const float *x, const float *t, const float *mask, int n, int epochs, int batch,
+                   float lr, uint64_t seed, float *loss);
+
 /* Status of the last failed call on this thread, and its message. */
 int gmpt_last_error(void);
 const char *gmpt_last_error_message(void);
