@@ -265,6 +265,47 @@ int gmpt_puts_latching_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const in
                      t->t);
 }
 
+int gmpt_puts_forest_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                            const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const uint64_t *d_values_hps,
+                            const int *d_trie_ids, int n, int64_t keys_bytes, int64_t values_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  gmpt::BatchIn b = device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs, d_values_hps, n,
+                                 keys_bytes, values_bytes);
+  b.trie_ids = d_trie_ids;
+  return record_trie(two_phase ? t->t->put_2phase(b) : t->t->put_latching(b), t->t);
+}
+
+int gmpt_gets_forest_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
+                            int n, int64_t keys_bytes, const uint8_t **values_hps, int *values_sizes) {
+  if (!t || (n > 0 && (!d_keys_hexs || !d_keys_indexs || !values_hps || !values_sizes)) || keys_bytes < 0)
+    return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->gets(d_keys_hexs, d_keys_indexs, n, true, reinterpret_cast<uint64_t *>(values_hps),
+                                values_sizes, keys_bytes, d_trie_ids),
+                     t->t);
+}
+
+int gmpt_gen_ids(uint64_t seed, int64_t n, int64_t n_existing, int64_t next_new, double p_new, double theta,
+                 int64_t *d_ids, int64_t *n_new, void *stream) {
+  std::string err;
+  int rc = gmpt::gen_ids(seed, n, n_existing, next_new, p_new, theta, d_ids, n_new, static_cast<cudaStream_t>(stream),
+                         err);
+  return record(rc, err);
+}
+
+int gmpt_gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes, uint8_t *d_keys_hexs,
+                  int *d_keys_indexs, void *stream) {
+  std::string err;
+  int rc = gmpt::gen_keys(seed, d_ids, n, key_bytes, d_keys_hexs, d_keys_indexs, static_cast<cudaStream_t>(stream), err);
+  return record(rc, err);
+}
+
+int gmpt_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_values, int64_t *d_values_indexs,
+                    void *stream) {
+  std::string err;
+  int rc = gmpt::gen_values(seed, n, value_bytes, d_values, d_values_indexs, static_cast<cudaStream_t>(stream), err);
+  return record(rc, err);
+}
+
 int gmpt_hash_onepass(gmpt_trie *t) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(t->t->hash(), t->t);

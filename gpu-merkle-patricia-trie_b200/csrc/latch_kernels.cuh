@@ -181,18 +181,19 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
 // handed to latch_from at the slot where its descent stopped.
 constexpr int kLatchWays = 4;
 
-// Keys t + w * nthreads (w < kLatchWays) of koff/klen[0..n), record ids
+// Keys t + w * nthreads (w < kWays) of koff/klen[0..n), record ids
 // vid_base + i, trie ids tid[i] (null: trie 0).
+template <int kWays = kLatchWays>
 __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, const uint64_t *koff,
                                            const uint32_t *klen, int n, uint64_t vid_base, uint32_t retry_limit,
                                            const int *tid, int t, int nthreads) {
   const uint32_t gen = tv.gen;
-  uint32_t *sp[kLatchWays];
-  uint32_t x[kLatchWays], len[kLatchWays];
-  uint64_t ko[kLatchWays];
-  uint8_t st[kLatchWays];  // 0 done, 1 walking, 2 hand off to latch_from
+  uint32_t *sp[kWays];
+  uint32_t x[kWays], len[kWays];
+  uint64_t ko[kWays];
+  uint8_t st[kWays];  // 0 done, 1 walking, 2 hand off to latch_from
 #pragma unroll
-  for (int w = 0; w < kLatchWays; ++w) {
+  for (int w = 0; w < kWays; ++w) {
     const int i = t + w * nthreads;
     st[w] = i < n ? 1 : 0;
     sp[w] = tv.roots + ((i < n && tid) ? tid[i] : 0);
@@ -205,12 +206,12 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
   // epoch, (2) key comparison chunks of short nodes, (3) advance / resolve,
   // (4) dirty marks (their atomics are off the descent's critical path).
   for (int round = 0; round < kMaxKeyNibbles + 2; ++round) {
-    uint32_t ref[kLatchWays], ep[kLatchWays], nib[kLatchWays], sl[kLatchWays];
-    uint64_t sko[kLatchWays];
+    uint32_t ref[kWays], ep[kWays], nib[kWays], sl[kWays];
+    uint64_t sko[kWays];
 #pragma unroll
-    for (int w = 0; w < kLatchWays; ++w) ref[w] = st[w] == 1 ? __ldcg(sp[w]) : 0u;
+    for (int w = 0; w < kWays; ++w) ref[w] = st[w] == 1 ? __ldcg(sp[w]) : 0u;
 #pragma unroll
-    for (int w = 0; w < kLatchWays; ++w) {
+    for (int w = 0; w < kWays; ++w) {
       const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
       ep[w] = gen;
       nib[w] = 0;
@@ -227,10 +228,10 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
       }
     }
     // short nodes: compare the key chunk by chunk, all ways together
-    uint32_t lim[kLatchWays], mm[kLatchWays];
-    bool cmp[kLatchWays];
+    uint32_t lim[kWays], mm[kWays];
+    bool cmp[kWays];
 #pragma unroll
-    for (int w = 0; w < kLatchWays; ++w) {
+    for (int w = 0; w < kWays; ++w) {
       cmp[w] = st[w] == 1 && ref_kind(ref[w]) == KIND_SHORT;
       lim[w] = cmp[w] ? min(sl[w], len[w] - x[w]) : 0u;
       mm[w] = 0;
@@ -238,7 +239,7 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
     for (int c = 0; c < kMaxKeyNibbles / 8 + 1; ++c) {
       bool more = false;
 #pragma unroll
-      for (int w = 0; w < kLatchWays; ++w) {
+      for (int w = 0; w < kWays; ++w) {
         if (!cmp[w]) continue;
         const uint32_t o = 8u * c;
         if (o >= lim[w]) {
@@ -259,7 +260,7 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
     }
     bool any = false;
 #pragma unroll
-    for (int w = 0; w < kLatchWays; ++w) {
+    for (int w = 0; w < kWays; ++w) {
       if (st[w] != 1) continue;
       const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
       if (kind == KIND_FULL) {
@@ -287,7 +288,7 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
       }
     }
 #pragma unroll
-    for (int w = 0; w < kLatchWays; ++w) {
+    for (int w = 0; w < kWays; ++w) {
       if (ep[w] == gen) continue;
       const uint32_t kind = ref_kind(ref[w]), idx = ref_idx(ref[w]);
       if (kind == KIND_FULL) {
@@ -301,17 +302,18 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
     if (!any) break;
   }
 #pragma unroll
-  for (int w = 0; w < kLatchWays; ++w)
+  for (int w = 0; w < kWays; ++w)
     if (st[w] != 0)
       latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)(t + w * nthreads),
                  retry_limit);
 }
 
+template <int kWays>
 __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
                                                       const uint32_t *klen, int n, uint64_t vid_base,
                                                       uint32_t retry_limit, const int *tid) {
-  latch_keys(tv, dl, koff, klen, n, vid_base, retry_limit, tid, blockIdx.x * blockDim.x + threadIdx.x,
-             gridDim.x * blockDim.x);
+  latch_keys<kWays>(tv, dl, koff, klen, n, vid_base, retry_limit, tid, blockIdx.x * blockDim.x + threadIdx.x,
+                    gridDim.x * blockDim.x);
 }
 
 }  // namespace gmpt

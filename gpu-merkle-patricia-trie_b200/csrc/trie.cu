@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -16,6 +18,7 @@
 #include "local_build.cuh"
 #include "local_sort.cuh"
 #include "block_update.cuh"
+#include "gen_kernels.cuh"
 
 namespace gmpt {
 
@@ -860,8 +863,10 @@ int Trie::put_latching(const BatchIn &b) {
   if ((rc = sync_counters())) return rc;
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
-  count_launch(), k_latch_insert<<<blocks_for((b.n + kLatchWays - 1) / kLatchWays), kThreads, 0, st_>>>(
-      tv_, dl, koff, klen, b.n, vid_base, 1u << 20, tid);
+  const int ways = opt_latch_ways_;
+  auto kern = ways == 1 ? k_latch_insert<1> : (ways == 2 ? k_latch_insert<2> : k_latch_insert<4>);
+  count_launch(), kern<<<blocks_for((b.n + ways - 1) / ways), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base,
+                                                                                 1u << 20, tid);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) {
@@ -1106,6 +1111,11 @@ int Trie::set_option(const std::string &name, int64_t value) {
   if (name == "block_grid") {
     if (value < 0 || value > 1 << 20) return fail(E_ARG, "block_grid must be in [0, 2^20]");
     opt_block_grid_ = (int)value;
+    return OK;
+  }
+  if (name == "latch_ways") {
+    if (value != 1 && value != 2 && value != 4) return fail(E_ARG, "latch_ways must be 1, 2 or 4");
+    opt_latch_ways_ = (int)value;
     return OK;
   }
   if (name == "block_graph") {
@@ -1385,6 +1395,113 @@ int Trie::reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes) {
   if (rc) return rc;
   // LockNU / block bound per key: one branch, three short nodes, one value
   return ensure_capacity(n_keys, 3 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8);
+}
+
+}  // namespace gmpt
+
+// ---------------------------------------------------------------------------
+// Synthetic request batches generated on the device.
+
+namespace gmpt {
+
+namespace {
+
+std::mutex g_gen_mu;
+DevBlock g_gen_flags, g_gen_rank, g_gen_scan, g_gen_tot;
+
+ZipfParams zipf_params(int64_t items, double theta) {
+  ZipfParams z{};
+  z.items = items;
+  if (std::fabs(theta - 1.0) < 1e-3) theta = 0.999;  // Gray's constants are singular at 1
+  z.theta = theta;
+  if (items <= 0 || theta <= 0.0) return z;
+  // zeta(items, theta): exact head, midpoint-integral tail
+  const int64_t K = std::min<int64_t>(items, 100000);
+  double zs = 0;
+  for (int64_t i = 1; i <= K; ++i) zs += std::pow((double)i, -theta);
+  if (items > K) {
+    const double a = (double)K + 0.5, b = (double)items + 0.5;
+    zs += (std::pow(b, 1.0 - theta) - std::pow(a, 1.0 - theta)) / (1.0 - theta);
+  }
+  z.zetan = zs;
+  z.alpha = 1.0 / (1.0 - theta);
+  z.half_pow = std::pow(0.5, theta);
+  const double zeta2 = 1.0 + z.half_pow;
+  z.eta = (1.0 - std::pow(2.0 / (double)items, 1.0 - theta)) / (1.0 - zeta2 / zs);
+  return z;
+}
+
+}  // namespace
+
+int gen_ids(uint64_t seed, int64_t n, int64_t n_existing, int64_t next_new, double p_new, double theta, int64_t *d_ids,
+            int64_t *n_new, cudaStream_t st, std::string &err) {
+  if (n < 0 || n > (1ll << 30) || n_existing < 0 || next_new < 0 || !d_ids || !n_new) {
+    err = "gen_ids: bad arguments";
+    return E_ARG;
+  }
+  *n_new = 0;
+  if (n == 0) return OK;
+  std::lock_guard<std::mutex> g(g_gen_mu);
+  cudaError_t e = g_gen_flags.ensure(sizeof(uint32_t) * n + 64);
+  if (e == cudaSuccess) e = g_gen_rank.ensure(sizeof(unsigned long long) * 2 * n + 64);
+  if (e == cudaSuccess) e = g_gen_scan.ensure(scan_ws_bytes<unsigned long long>(n));
+  if (e == cudaSuccess) e = g_gen_tot.ensure(64);
+  if (e != cudaSuccess) {
+    err = std::string("gen_ids: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  const ZipfParams z = zipf_params(n_existing, theta);
+  uint32_t *flags = g_gen_flags.as<uint32_t>();
+  unsigned long long *f64 = g_gen_rank.as<unsigned long long>(), *rank = f64 + n;
+  count_launch(), k_gen_ids<<<blocks_for(n), kThreads, 0, st>>>(seed, n, p_new, z, d_ids, flags);
+  count_launch(), k_gen_widen<<<blocks_for(n), kThreads, 0, st>>>(flags, n, f64);
+  unsigned long long *tot = g_gen_tot.as<unsigned long long>();
+  e = exclusive_scan<unsigned long long>(f64, rank, n, tot, g_gen_scan, st);
+  if (e == cudaSuccess) count_launch(), k_gen_new_ids<<<blocks_for(n), kThreads, 0, st>>>(flags, rank, n, next_new, d_ids);
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, tot, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("gen_ids: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  *n_new = (int64_t)(h & 0xFFFFFFFFull);
+  return OK;
+}
+
+int gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes, uint8_t *d_hexs, int *d_idx, cudaStream_t st,
+             std::string &err) {
+  if (n < 0 || key_bytes < 1 || key_bytes > kMaxKeyNibbles / 2 || (n > 0 && (!d_ids || !d_hexs || !d_idx)) ||
+      n * (2 * (int64_t)key_bytes + 1) >= (1ll << 31)) {
+    err = "gen_keys: bad arguments";
+    return E_ARG;
+  }
+  if (n == 0) return OK;
+  count_launch(), k_gen_keys<<<blocks_for(n), kThreads, 0, st>>>(seed, d_ids, n, key_bytes, d_hexs, d_idx);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("gen_keys: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  return OK;
+}
+
+int gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_vals, int64_t *d_idx, cudaStream_t st,
+               std::string &err) {
+  if (n < 0 || value_bytes < 1 || (n > 0 && (!d_vals || !d_idx))) {
+    err = "gen_values: bad arguments";
+    return E_ARG;
+  }
+  if (n == 0) return OK;
+  count_launch(), k_gen_values<<<blocks_for(n), kThreads, 0, st>>>(seed, n, value_bytes, d_vals, d_idx);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("gen_values: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  return OK;
 }
 
 }  // namespace gmpt

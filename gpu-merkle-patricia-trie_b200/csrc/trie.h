@@ -112,7 +112,7 @@ class Trie {
   int device() const { return dev_; }
   int max_tries() const { return (int)n_tries_; }
   void set_timing(bool on) { timing_ = on; }
-  // tuning knobs (names: "local_build", "local_sort", "block_grid", "block_graph")
+  // tuning knobs (names: "local_build", "local_sort", "latch_ways", "block_grid", "block_graph")
   int set_option(const std::string &name, int64_t value);
   // persistent graph-replayed forest update; out32[32 i..] / sizes[i] = root
   // of trie out_ids[i] after the update
@@ -143,6 +143,7 @@ class Trie {
   bool timing_ = false;
   bool opt_local_build_ = true;  // finish small build segments in one CTA each
   bool opt_local_sort_ = true;   // finish small tied sort runs in one CTA each
+  int opt_latch_ways_ = 4;       // LockNU keys per thread (1, 2, 4)
 
   // node pools (capacities in elements)
   TrieView tv_{};
@@ -216,5 +217,11 @@ class Trie {
 int keccak256_batch_device(const uint8_t *d_data, const int64_t *d_idx, int n, uint8_t *d_out, cudaStream_t st);
 int keccak_peak(int device, double *perm_per_s);
 int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32, std::string &err);
+int gen_ids(uint64_t seed, int64_t n, int64_t n_existing, int64_t next_new, double p_new, double theta, int64_t *d_ids,
+            int64_t *n_new, cudaStream_t st, std::string &err);
+int gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes, uint8_t *d_hexs, int *d_idx, cudaStream_t st,
+             std::string &err);
+int gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_vals, int64_t *d_idx, cudaStream_t st,
+               std::string &err);
 
 }  // namespace gmpt

@@ -38,6 +38,7 @@ EXPORTS = [
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
+    "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -115,6 +116,11 @@ def lib():
     L.gmpt_mlp_forward.argtypes = [vp, vp, i32, vp]
     L.gmpt_mlp_loss_grad.argtypes = [vp, vp, vp, vp, i32, vp, vp]
     L.gmpt_mlp_train.argtypes = [vp, vp, vp, vp, i32, i32, i32, C.c_float, C.c_uint64, vp]
+    L.gmpt_puts_forest_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32, i64, i64]
+    L.gmpt_gets_forest_device.argtypes = [vp, vp, vp, vp, i32, i64, vp, vp]
+    L.gmpt_gen_ids.argtypes = [C.c_uint64, i64, i64, i64, C.c_double, C.c_double, vp, vp, vp]
+    L.gmpt_gen_keys.argtypes = [C.c_uint64, vp, i64, i32, vp, vp, vp]
+    L.gmpt_gen_values.argtypes = [C.c_uint64, i64, i32, vp, vp, vp]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -205,6 +211,25 @@ def keccak256_rows(msgs: np.ndarray, chunk: int = 1 << 22) -> np.ndarray:
         _check(lib().gmpt_keccak256_batch(_p(data), _p(idx), k, _p(o)))
         out[a: a + k] = o.reshape(k, 32)
     return out
+
+
+def gen_ids(seed: int, n: int, n_existing: int, next_new: int, p_new: float, theta: float, d_ids: int,
+            stream: int = 0) -> int:
+    """Fill d_ids (device int64[n]); returns how many fresh ids were used."""
+    nn = C.c_int64()
+    _check(lib().gmpt_gen_ids(int(seed) & ((1 << 64) - 1), int(n), int(n_existing), int(next_new), float(p_new),
+                              float(theta), C.c_void_p(d_ids), C.byref(nn), C.c_void_p(stream) if stream else None))
+    return nn.value
+
+
+def gen_keys(seed: int, d_ids: int, n: int, key_bytes: int, d_hexs: int, d_idx: int, stream: int = 0):
+    _check(lib().gmpt_gen_keys(int(seed) & ((1 << 64) - 1), C.c_void_p(d_ids), int(n), int(key_bytes),
+                               C.c_void_p(d_hexs), C.c_void_p(d_idx), C.c_void_p(stream) if stream else None))
+
+
+def gen_values(seed: int, n: int, value_bytes: int, d_vals: int, d_idx: int, stream: int = 0):
+    _check(lib().gmpt_gen_values(int(seed) & ((1 << 64) - 1), int(n), int(value_bytes), C.c_void_p(d_vals),
+                                 C.c_void_p(d_idx), C.c_void_p(stream) if stream else None))
 
 
 def keccak_peak(device: int = 0) -> float:
@@ -385,6 +410,21 @@ class MPT:
 
     def reserve(self, n_keys: int, key_bytes: int, value_bytes: int):
         _check(self._L.gmpt_reserve(self._h, int(n_keys), int(key_bytes), int(value_bytes)))
+
+    def puts_forest_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, d_tids, n: int, keys_bytes: int,
+                           values_bytes: int):
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_puts_forest_device(self._h, 1 if two_phase else 0, v(d_keys), v(d_kidx), v(d_vals),
+                                               v(d_vidx), None, v(d_tids), int(n), int(keys_bytes),
+                                               int(values_bytes)))
+
+    def gets_forest_device(self, d_keys, d_kidx, d_tids, n: int, keys_bytes: int):
+        hps = np.zeros(max(n, 1), dtype=np.uint64)
+        sizes = np.zeros(max(n, 1), dtype=np.int32)
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_gets_forest_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes),
+                                               _p(hps), _p(sizes)))
+        return hps[:n], sizes[:n]
 
     def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
                     values_bytes: int, d_hps: int = 0):

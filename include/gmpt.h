@@ -156,6 +156,31 @@ int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_
 int gmpt_reserve_block(gmpt_trie *t, int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes,
                        int64_t max_out);
 
+/* Forest inserts from DEVICE arrays (two_phase: PhaseNU, else LockNU);
+ * d_trie_ids may be NULL (trie 0). */
+int gmpt_puts_forest_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                            const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const uint64_t *d_values_hps,
+                            const int *d_trie_ids, int n, int64_t keys_bytes, int64_t values_bytes);
+/* gets_parallel with DEVICE keys (and trie ids, or NULL for trie 0); the
+ * results land in the host arrays as for gmpt_gets_parallel. */
+int gmpt_gets_forest_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
+                            int n, int64_t keys_bytes, const uint8_t **values_hps, int *values_sizes);
+
+/* ---- synthetic request batches in device memory (bench and tests) ----
+ * gmpt_gen_ids: n ids; each is fresh (next_new, next_new + 1, ... in batch
+ * order) with probability p_new, else zipf(theta) over [0, n_existing)
+ * (Gray et al.'s generator, ranks scrambled by FNV-1a-64); *n_new = fresh
+ * ids used.  gmpt_gen_keys: key_bytes bytes per id from a splitmix64 stream
+ * of (seed, id), as hex nibbles + terminator back to back with int32 index
+ * pairs.  gmpt_gen_values: value_bytes random bytes per batch position.
+ * Synchronous on `stream` (a cudaStream_t or NULL). */
+int gmpt_gen_ids(uint64_t seed, int64_t n, int64_t n_existing, int64_t next_new, double p_new, double theta,
+                 int64_t *d_ids, int64_t *n_new, void *stream);
+int gmpt_gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes, uint8_t *d_keys_hexs,
+                  int *d_keys_indexs, void *stream);
+int gmpt_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_values, int64_t *d_values_indexs,
+                    void *stream);
+
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
 int gmpt_hash_onepass(gmpt_trie *t);
@@ -193,6 +218,8 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
  *   "local_build" 1/0: finish build segments of <= 2048 keys inside one CTA
  *                      each (default 1) or keep every level device-wide;
  *   "local_sort"  1/0: same for the still-tied runs of the batch sort;
+ *   "latch_ways"  1/2/4: keys each LockNU thread walks together (default 4:
+ *                      more loads in flight; 1: more threads for small batches);
  *   "block_grid"  N:   CTAs of the persistent block kernel (0 = one per SM,
  *                      capped at what can be co-resident);
  *   "block_graph" 1/0: replay block launches from a captured CUDA graph

@@ -1,0 +1,118 @@
+"""Request loop over a forest of tenant tries: results never depend on the
+schedule (configuration, merging of queued requests), and equal the
+oracle's; the learned selector trains on measured times and picks
+configurations; device-generated batches have the promised shape."""
+import numpy as np
+import pytest
+
+import oracle as O
+from gmpt import serve as S
+from gmpt import tuner as TU
+from gmpt import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev(gpu_lib):
+    import torch
+
+    return torch.device("cuda", 0)
+
+
+def _oracle_roots(record, tenants):
+    ts = {t.tid: O.OracleTrie(O.MODE_REF) for t in tenants}
+    for batch, tids in record:
+        for t in sorted(set(tids.tolist())):
+            sel = np.nonzero(tids == t)[0]
+            sub = batch.subset(sel)
+            ts[t].puts(sub.keys_hexs, sub.keys_indexs, sub.values, sub.values_indexs)
+    out = []
+    for t in tenants:
+        ts[t.tid].hash()
+        out.append(ts[t.tid].root())
+    return out
+
+
+def test_served_stream_matches_oracle_under_every_schedule(gpu_lib, dev):
+    tenants = S.make_tenants([0, 1500, 6000])
+    reqs = S.make_stream(7, 40, len(tenants), 0.4, 50, 3000)
+    S.poisson_arrivals(reqs, 5000.0)  # dense arrivals: the batched server merges
+    rng = np.random.default_rng(0)
+    runs = []
+    for batching in (False, True):
+        r = S.Runner(gpu_lib, tenants, 0, dev, record=True)
+        picks = []
+
+        def policy(runner, run, n, kb, vb):
+            k = int(rng.integers(len(TU.CONFIGS)))
+            picks.append(k)
+            return k
+
+        res = S.serve(r, reqs, policy, batching)
+        runs.append((r.roots(), res, r.record, picks))
+        r.close()
+    (roots_a, res_a, rec_a, picks_a), (roots_b, res_b, rec_b, _) = runs
+    assert roots_a == roots_b
+    assert roots_a == _oracle_roots(rec_a, tenants)
+    assert len(set(picks_a)) > 3  # many configurations exercised
+    assert res_b.groups < res_a.groups  # merging happened
+    # lookups answer the same whichever way they were grouped
+    assert np.array_equal(np.concatenate(res_a.get_sizes), np.concatenate(res_b.get_sizes))
+
+
+def test_time_matrix_replicas_agree_and_selector_trains(gpu_lib, dev):
+    tenants = S.make_tenants([0, 4000, 20000])
+    reqs = S.make_stream(11, 30, len(tenants), 0.2, 100, 20000)
+    reps = [S.Runner(gpu_lib, tenants, 0, dev) for _ in TU.CONFIGS]
+    T, G, F = S.time_matrix(reps, reqs)  # raises if any configuration changes a root
+    roots = [r.roots() for r in reps]
+    assert all(x == roots[0] for x in roots)
+    puts = np.array([r.kind == "put" for r in reqs])
+    assert np.all(np.isfinite(T[puts])) and np.all(np.isnan(T[~puts]))
+    assert np.all(np.isfinite(G[~puts]))
+    rule = TU.Autotuner().fit(F[puts], T[puts])
+    sel = TU.Selector(gpu_lib.Net(len(TU.FEATURES), 32, len(TU.CONFIGS), seed=3), rule)
+    loss0 = None
+    for _ in range(3):
+        loss = sel.fit(F[puts], T[puts], epochs=100)
+        loss0 = loss if loss0 is None else loss0
+    assert loss <= loss0
+    for f in F[puts]:
+        assert 0 <= sel.choose(f) < len(TU.CONFIGS)
+    for r in reps:
+        r.close()
+
+
+def test_generated_ids_keys_and_values(gpu_lib, dev):
+    import torch
+
+    n = 50000
+    ids = torch.empty(n, dtype=torch.int64, device=dev)
+    nn = gpu_lib.gen_ids(5, n, 1000, 1000, 0.3, 0.99, ids.data_ptr())
+    h = ids.cpu().numpy()
+    fresh = h >= 1000
+    assert nn == fresh.sum() and abs(nn / n - 0.3) < 0.02
+    assert np.array_equal(np.sort(h[fresh]), np.arange(1000, 1000 + nn))  # dense fresh ids
+    old = h[~fresh]
+    assert old.min() >= 0 and old.max() < 1000
+    cnt = np.bincount(old, minlength=1000)
+    assert cnt.max() > 20 * np.median(cnt[cnt > 0])  # skewed
+    # same seed, same ids
+    ids2 = torch.empty(n, dtype=torch.int64, device=dev)
+    gpu_lib.gen_ids(5, n, 1000, 1000, 0.3, 0.99, ids2.data_ptr())
+    assert torch.equal(ids, ids2)
+    keys = torch.empty(n * 41 + 64, dtype=torch.uint8, device=dev)
+    kidx = torch.empty(2 * n, dtype=torch.int32, device=dev)
+    gpu_lib.gen_keys(9, ids.data_ptr(), n, 20, keys.data_ptr(), kidx.data_ptr())
+    k = keys[: n * 41].cpu().numpy().reshape(n, 41)
+    assert np.all(k[:, 40] == 16) and k[:, :40].max() <= 15
+    # equal ids give equal keys
+    for a in np.nonzero(~fresh)[0][:200]:
+        b = np.nonzero(h == h[a])[0]
+        assert all(np.array_equal(k[a], k[j]) for j in b[:5])
+    assert np.array_equal(kidx.cpu().numpy()[0::2], np.arange(n) * 41)
+    vals = torch.empty(n * 7 + 64, dtype=torch.uint8, device=dev)
+    vidx = torch.empty(2 * n, dtype=torch.int64, device=dev)
+    gpu_lib.gen_values(3, n, 7, vals.data_ptr(), vidx.data_ptr())
+    assert np.array_equal(vidx.cpu().numpy()[1::2], np.arange(n) * 7 + 6)
