@@ -51,6 +51,15 @@ def parse():
     p.add_argument("--eth-blocks", type=int, default=512)
     p.add_argument("--eth-compare-blocks", type=int, default=32,
                    help="blocks also run through the per-trie and forest multi-launch paths")
+    p.add_argument("--req-tenants", default="0,262144,1048576,4194304",
+                   help="pre-existing keys of each tenant trie of the request loop (empty = skip)")
+    p.add_argument("--req-train", type=int, default=1200, help="requests of the selector's training streams")
+    p.add_argument("--req-train-episode", type=int, default=300, help="requests per training episode")
+    p.add_argument("--req-eval", type=int, default=300, help="requests of each evaluation stream")
+    p.add_argument("--req-min", type=int, default=1000)
+    p.add_argument("--req-max", type=int, default=1 << 20)
+    p.add_argument("--req-util", type=float, default=0.85, help="load of the plain server (arrival rate)")
+    p.add_argument("--req-load", type=float, default=0.25, help="share of puts that fill a new empty tenant trie")
     return p.parse_args()
 
 
@@ -357,6 +366,145 @@ def run_eth(args, local, dev):
     }
 
 
+MERGE_KEYS = 1 << 22  # largest merged batch of the queue-draining server
+
+
+def run_requests(args, local, dev):
+    """Request loop: streams of put / get batches over tenant tries, served by
+    the plain fixed-LockNU one-at-a-time server, by the selectors, and by the
+    learned + batched server (selector-chosen schedule, queued requests
+    drained and merged into forest calls).  Every put of a training stream
+    is timed under every configuration on its own replica; the MLP selector
+    trains on those times with the library's CUDA kernels."""
+    import torch
+
+    import gmpt
+    from gmpt import serve as S
+    from gmpt import tuner as TU
+
+    sizes = [int(x) for x in args.req_tenants.split(",") if x]
+    t0 = time.time()
+
+    def stream(seed, count, ratio):
+        tenants = S.make_tenants(sizes)
+        return tenants, S.make_stream(seed, count, tenants, ratio, args.req_min, args.req_max, load_frac=args.req_load)
+
+    # training data: episodes of fresh tenant sets, every configuration timed
+    tenants, st = stream(0x5EED0C60, args.req_train_episode, 0.2)
+    reps = [S.Runner(gmpt, tenants, local, dev, max_tries=4096) for _ in TU.CONFIGS]
+    Fs, Ts = [], []
+    episodes = max(1, args.req_train // args.req_train_episode)
+    for e in range(episodes):
+        if e:
+            tenants, st = stream(0x5EED0C60 + e, args.req_train_episode, 0.2)
+            for r in reps:
+                r.reset(tenants)
+        for r in reps:
+            r.reserve_for(st)
+        if e == 0:  # first feature call initialises the sampling kernel
+            n0, kb0, vb0 = reps[0].build([x for x in st if x.kind == "put"][:1])
+            reps[0].features([x for x in st if x.kind == "put"][:1], n0, kb0, vb0)
+            reps[0].reset(tenants)
+        T, _, F = S.time_matrix(reps, st)
+        puts = np.array([r.kind == "put" for r in st])
+        Fs.append(F[puts])
+        Ts.append(T[puts])
+    Ftr, Ttr = np.concatenate(Fs), np.concatenate(Ts)
+    net = gmpt.Net(len(TU.FEATURES), 32, len(TU.CONFIGS), seed=5, device=local)
+    sel = TU.Selector(net, TU.Autotuner())
+    tt = time.time()
+    loss = sel.fit(Ftr, Ttr, max_epochs=600, lr=3e-3)
+    train_s = time.time() - tt
+    rule = sel.rule
+    out = {"workload": f"request loop over tenant tries (pre-existing keys {sizes}, plus a new empty tenant per "
+                       f"load request = {args.req_load:.2f} of puts; keys 20-96 B, values 16-128 B per tenant); "
+                       f"batches log-uniform [{args.req_min}, {args.req_max}] keys, zipf theta U[0,1.2], puts mix "
+                       "fresh keys (share U[0,1]) and zipf updates; Poisson arrivals at "
+                       f"{args.req_util:.2f} load of the plain server",
+           "configs": [c["name"] for c in TU.CONFIGS],
+           "train": {"requests": episodes * args.req_train_episode, "episodes": episodes, "puts": int(len(Ftr)),
+                     "mlp": f"{len(TU.FEATURES)}-32-32-{len(TU.CONFIGS)}", "final_loss": round(loss, 4),
+                     "train_kernel_s": round(train_s, 3), "validation": sel.validation,
+                     "rule_buckets": len(rule.table),
+                     "best_config_share": np.bincount(np.nanargmin(Ttr, 1), minlength=len(TU.CONFIGS)).tolist()},
+           "streams": {}}
+    for label, ratio, seed in (("50/50", 0.5, 0x5EED0C61), ("95/5", 0.95, 0x5EED0C62)):
+        tenants, ev = stream(seed, args.req_eval, ratio)
+        for r in reps:
+            r.reset(tenants)
+            r.reserve_for(ev)
+        T, G, F = S.time_matrix(reps, ev)
+        final = reps[0].roots()
+        isput = np.array([r.kind == "put" for r in ev])
+        keys = sum(r.n for r in ev)
+        rn = reps[0]
+        res = {}
+
+        def live(name, policy, batching):
+            rn.reset(tenants)
+            if batching:
+                rn.reserve_for(ev, merged_keys=MERGE_KEYS)
+            fb0 = sel.fallbacks
+            r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS)
+            assert rn.roots() == final, f"{name}: roots differ from the fixed-schedule replicas"
+            res[name] = {"mkeys_s": round(r.keys / (r.busy_ms / 1e3) / 1e6, 3),
+                         "p50_ms": round(float(np.percentile(r.latency_ms, 50)), 3),
+                         "p99_ms": round(float(np.percentile(r.latency_ms, 99)), 3),
+                         "groups": r.groups, "rule_fallbacks": sel.fallbacks - fb0,
+                         "choices": {TU.CONFIGS[k]["name"]: v for k, v in sorted(r.choices.items())}}
+            return r
+
+        def plain_policy(runner, run, n, kb, vb):
+            return TU.FIXED_LOCKNU
+
+        def learned_policy(runner, run, n, kb, vb):
+            return sel.choose(runner.features(run, n, kb, vb))
+
+        # the plain server (fixed LockNU, one request at a time): its service
+        # times do not depend on arrivals, so it sets the arrival rate
+        for r in ev:
+            r.arrival = 0.0
+        plain = live("plain_live", plain_policy, False)
+        rate = args.req_util / (plain.service_ms.mean() / 1e3)
+        S.poisson_arrivals(ev, rate)
+        lat = S.fifo_latency(ev, plain.service_ms)
+        res["plain_live"]["p50_ms"] = round(float(np.percentile(lat, 50)), 3)
+        res["plain_live"]["p99_ms"] = round(float(np.percentile(lat, 99)), 3)
+        live("learned_live", learned_policy, False)
+        live("learned_batched_live", learned_policy, True)
+        # the same arrivals against per-request times of the timing matrix
+        choice = {"matrix_fixed_locknu": np.full(len(ev), TU.FIXED_LOCKNU),
+                  "matrix_fixed_phasenu": np.full(len(ev), TU.FIXED_PHASENU),
+                  "matrix_rule": np.array([rule.choose(f) if p else 0 for f, p in zip(F, isput)]),
+                  "matrix_mlp": np.array([sel._net_choice(f) if p else 0 for f, p in zip(F, isput)]),
+                  "matrix_selector": np.array([sel.choose(f) if p else 0 for f, p in zip(F, isput)])}
+        best = np.where(isput, np.nanmin(np.where(isput[:, None], T, np.inf), 1), G)
+        for name, c in choice.items():
+            svc = np.where(isput, T[np.arange(len(ev)), c], G)
+            lat = S.fifo_latency(ev, svc)
+            res[name] = {"mkeys_s": round(keys / (svc.sum() / 1e3) / 1e6, 3),
+                         "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                         "regret": round(float(svc[isput].sum() / best[isput].sum() - 1.0), 4)}
+        lat = S.fifo_latency(ev, best)
+        res["matrix_best"] = {"mkeys_s": round(keys / (best.sum() / 1e3) / 1e6, 3),
+                              "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                              "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+        res["requests"] = len(ev)
+        res["keys"] = int(keys)
+        res["arrival_rate_per_s"] = round(rate, 2)
+        res["learned_batched_vs_plain"] = round(res["learned_batched_live"]["mkeys_s"] /
+                                                res["plain_live"]["mkeys_s"], 3)
+        res["p99_learned_batched_vs_plain"] = round(res["learned_batched_live"]["p99_ms"] /
+                                                    res["plain_live"]["p99_ms"], 3)
+        res["roots_bit_exact"] = True
+        out["streams"][label] = res
+    for r in reps:
+        r.close()
+    out["wall_s"] = round(time.time() - t0, 1)
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -544,14 +692,18 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, batches)
-    if world == 1 and args.eth_accounts > 0:
+    if world == 1 and (args.eth_accounts > 0 or args.req_tenants):
         t.close()
         del dbat
         torch.cuda.empty_cache()
+    if world == 1 and args.eth_accounts > 0:
         line["batched"] = run_eth(args, local, dev)
+        torch.cuda.empty_cache()
+    if world == 1 and args.req_tenants:
+        line["learned"] = run_requests(args, local, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if not (world == 1 and args.eth_accounts > 0):
+    if not (world == 1 and (args.eth_accounts > 0 or args.req_tenants)):
         t.close()
     if world > 1:
         import torch.distributed as dist

@@ -195,6 +195,15 @@ int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_
   return record_trie(t->t->reserve((uint64_t)n_keys, (uint64_t)key_bytes, (uint64_t)value_bytes), t->t);
 }
 
+int gmpt_reserve_nodes(gmpt_trie *t, int64_t full, int64_t shorts, int64_t values, int64_t records, int64_t key_bytes,
+                       int64_t value_bytes) {
+  if (!t || full < 0 || shorts < 0 || values < 0 || records < 0 || key_bytes < 0 || value_bytes < 0)
+    return record(GMPT_E_ARG, "bad argument");
+  return record_trie(t->t->reserve_nodes((uint64_t)full, (uint64_t)shorts, (uint64_t)values, (uint64_t)records,
+                                         (uint64_t)key_bytes, (uint64_t)value_bytes),
+                     t->t);
+}
+
 int gmpt_reserve_block(gmpt_trie *t, int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes,
                        int64_t max_out) {
   if (!t) return record(GMPT_E_ARG, "null trie");
@@ -303,6 +312,14 @@ int gmpt_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_values
                     void *stream) {
   std::string err;
   int rc = gmpt::gen_values(seed, n, value_bytes, d_values, d_values_indexs, static_cast<cudaStream_t>(stream), err);
+  return record(rc, err);
+}
+
+int gmpt_batch_features_device(const uint8_t *d_keys_hexs, const int *d_keys_indexs, int n, int64_t keys_bytes,
+                               float out[4], void *stream) {
+  std::string err;
+  int rc = gmpt::batch_features_device(d_keys_hexs, d_keys_indexs, n, keys_bytes, out,
+                                       static_cast<cudaStream_t>(stream), err);
   return record(rc, err);
 }
 

@@ -116,3 +116,78 @@ __global__ void k_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t 
 }
 
 }  // namespace gmpt
+
+namespace gmpt {
+
+// Selector features of a staged key batch from 64 evenly spaced keys, one
+// CTA: mean and spread of key length (nibbles), share of sampled keys equal
+// to an earlier sample, and mean over samples of the longest common prefix
+// with any other sample (= with its neighbour in sorted order) over the mean
+// length.  out[4].
+// Reads only bytes [0, keys_bytes) of `keys` (ranges outside count as empty
+// keys) and compares byte by byte, so the caller's buffer needs no padding.
+__global__ void __launch_bounds__(64) k_sample_features(const uint8_t *keys, const int *kidx, int n,
+                                                        int64_t keys_bytes, float *out) {
+  __shared__ int s_off[64], s_len[64];
+  __shared__ float red[4][64];
+  const int j = threadIdx.x;
+  const int s = n < 64 ? n : 64;
+  if (j < s) {
+    const int64_t i = (int64_t)j * n / s;
+    const int a = kidx[2 * i], z = kidx[2 * i + 1];
+    const bool ok = a >= 0 && z >= a && (int64_t)z < keys_bytes;
+    s_off[j] = ok ? a : 0;
+    s_len[j] = ok ? z - a + 1 : 0;
+  }
+  __syncthreads();
+  float len = 0.f, dup = 0.f, lcp = 0.f;
+  if (j < s) {
+    const uint8_t *a = keys + s_off[j];
+    const int la = s_len[j];
+    int best = 0;
+    bool earlier = false;
+    for (int k = 0; k < s; ++k) {
+      if (k == j) continue;
+      const int lb = s_len[k];
+      const int m = la < lb ? la : lb;
+      const uint8_t *b = keys + s_off[k];
+      int l = 0;
+      while (l < m && a[l] == b[l]) ++l;
+      if (l == m && la == lb && k < j) earlier = true;
+      best = l > best ? l : best;
+    }
+    len = (float)la;
+    dup = earlier ? 1.f : 0.f;
+    lcp = (float)best;
+  }
+  __shared__ float s_mean;
+  red[0][j] = len;
+  red[2][j] = dup;
+  red[3][j] = lcp;
+  __syncthreads();
+  if (j == 0) {
+    float t = 0.f;
+    for (int k = 0; k < s; ++k) t += red[0][k];
+    s_mean = s > 0 ? t / (float)s : 0.f;
+  }
+  __syncthreads();
+  const float d = len - s_mean;  // two-pass variance (no cancellation)
+  red[1][j] = j < s ? d * d : 0.f;
+  __syncthreads();
+  if (j < 4 && j > 0) {
+    float t = 0.f;
+    for (int k = 0; k < s; ++k) t += red[j][k];
+    red[j][0] = t;  // row j's slot 0 is read only by thread j
+  }
+  __syncthreads();
+  if (j == 0) {
+    const float inv = s > 0 ? 1.f / (float)s : 0.f;
+    const float mean = s_mean;
+    out[0] = mean;
+    out[1] = sqrtf(red[1][0] * inv);
+    out[2] = red[2][0] * inv;
+    out[3] = mean > 0.f ? red[3][0] * inv / mean : 0.f;
+  }
+}
+
+}  // namespace gmpt

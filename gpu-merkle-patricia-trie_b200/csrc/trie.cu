@@ -27,6 +27,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kHashThreads = 128;
 constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);
+// levels with at most this many branch nodes hash them one warp each
+constexpr int kWarpFullMax = 4096;
 
 inline unsigned blocks_for(int64_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
@@ -111,8 +113,10 @@ Trie::~Trie() {
   DevBlock *bblocks[] = {&blk_.keys, &blk_.kidx, &blk_.vals, &blk_.vidx, &blk_.tid, &blk_.ptrie, &blk_.poff,
                          &blk_.out_ids, &blk_.out, &blk_.koff, &blk_.klen, &blk_.bins, &blk_.sorted};
   for (DevBlock *b : bblocks) b->release();
-  if (blk_.exec) cudaGraphExecDestroy(blk_.exec);
-  if (blk_.graph) cudaGraphDestroy(blk_.graph);
+  for (auto &c : blk_.graphs) {
+    if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+  }
   if (blk_.d_desc) cudaFree(blk_.d_desc);
   if (blk_.h_desc) cudaFreeHost(blk_.h_desc);
   if (h_ctr_) cudaFreeHost(h_ctr_);
@@ -164,9 +168,10 @@ uint64_t Trie::read_u64(const void *dptr) {
 }
 
 int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
-                          uint64_t add_key_bytes, uint64_t add_val_bytes) {
+                          uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact) {
   cudaError_t e = cudaSuccess;
-  auto grow_to = [](uint64_t need, uint64_t cap) {
+  auto grow_to = [exact](uint64_t need, uint64_t cap) {
+    if (exact) return std::max<uint64_t>(need, 1024);
     uint64_t c = cap ? cap : 1024;
     while (c < need) c = c + c / 2 + 1024;
     return c;
@@ -646,11 +651,21 @@ int Trie::bucket_and_hash() {
     cudaEventCreate(&kz);
     cudaEventRecord(ka, st_);
   }
+  const size_t smem_warp = smem + 4 * kWarpMsgBytes;
   for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
-    uint32_t a = off[2 * d], z = off[2 * d + 2];
+    uint32_t a = off[2 * d], m = off[2 * d + 1], z = off[2 * d + 2];
     if (z == a) continue;
     ++levels;
-    count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a, (int)(z - a));
+    if (z - m > 0 && z - m <= (uint32_t)kWarpFullMax) {
+      // few branches: short nodes thread-wise, branches one warp each
+      if (m > a)
+        count_launch(), k_hash_level<<<blocks_for(m - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a,
+                                                                                                  (int)(m - a));
+      count_launch(), k_hash_full_warp<<<(z - m + 3) / 4, 128, smem_warp, st_>>>(tv_, sorted + m, (int)(z - m));
+    } else {
+      count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a,
+                                                                                                (int)(z - a));
+    }
   }
   if (timing_) {
     cudaEventRecord(kz, st_);
@@ -1157,7 +1172,7 @@ int Trie::block_launch(bool launch) {
     return check_cuda(e, "block occupancy");
   const int max_grid = occ * sms;
   if (max_grid < 1) return fail(E_INTERNAL, "persistent kernel does not fit an SM");
-  const int grid = opt_block_grid_ > 0 ? std::min(opt_block_grid_, max_grid) : sms;
+  const int grid = opt_block_grid_ > 0 ? std::min(opt_block_grid_, max_grid) : max_grid;
   const int stage_grid = sms * 4;
   BlockSig sig;
   std::memset(&sig, 0, sizeof(sig));
@@ -1205,27 +1220,40 @@ int Trie::block_launch(bool launch) {
     return OK;
   }
   const uint8_t *sb = reinterpret_cast<const uint8_t *>(&sig);
-  if (!blk_.exec || blk_.sig.size() != sizeof(sig) || std::memcmp(blk_.sig.data(), sb, sizeof(sig)) != 0) {
-    if (blk_.exec) cudaGraphExecDestroy(blk_.exec);
-    if (blk_.graph) cudaGraphDestroy(blk_.graph);
-    blk_.exec = nullptr;
-    blk_.graph = nullptr;
-    blk_.sig.clear();
+  BlockRt::Captured *hit = nullptr;
+  for (auto &c : blk_.graphs)
+    if (c.sig.size() == sizeof(sig) && std::memcmp(c.sig.data(), sb, sizeof(sig)) == 0) hit = &c;
+  if (!hit) {
+    constexpr size_t kKeep = 4;
+    if (blk_.graphs.size() >= kKeep) {  // drop the least recently used capture
+      auto lru = std::min_element(blk_.graphs.begin(), blk_.graphs.end(),
+                                  [](const BlockRt::Captured &a, const BlockRt::Captured &b) { return a.used < b.used; });
+      if (lru->exec) cudaGraphExecDestroy(lru->exec);
+      if (lru->graph) cudaGraphDestroy(lru->graph);
+      blk_.graphs.erase(lru);
+    }
+    BlockRt::Captured c;
     if ((e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return check_cuda(e, "block graph capture");
     cudaError_t ie = issue();
-    e = cudaStreamEndCapture(st_, &blk_.graph);
-    if (ie != cudaSuccess) return check_cuda(ie, "block graph capture");
+    e = cudaStreamEndCapture(st_, &c.graph);
+    if (ie != cudaSuccess) {
+      if (c.graph) cudaGraphDestroy(c.graph);
+      return check_cuda(ie, "block graph capture");
+    }
     if (e != cudaSuccess) return check_cuda(e, "block graph capture end");
-    if ((e = cudaGraphInstantiate(&blk_.exec, blk_.graph, 0)) != cudaSuccess) {
-      blk_.exec = nullptr;
+    if ((e = cudaGraphInstantiate(&c.exec, c.graph, 0)) != cudaSuccess) {
+      cudaGraphDestroy(c.graph);
       return check_cuda(e, "block graph instantiate");
     }
-    blk_.sig.assign(sb, sb + sizeof(sig));
+    c.sig.assign(sb, sb + sizeof(sig));
+    blk_.graphs.push_back(std::move(c));
+    hit = &blk_.graphs.back();
     ++binfo_.captures;
   }
+  hit->used = ++blk_.tick;
   if (!launch) return OK;
-  if ((e = cudaGraphLaunch(blk_.exec, st_)) != cudaSuccess) return check_cuda(e, "block graph launch");
+  if ((e = cudaGraphLaunch(hit->exec, st_)) != cudaSuccess) return check_cuda(e, "block graph launch");
   count_launch();
   count_launch();
   ++binfo_.launches;
@@ -1387,6 +1415,15 @@ int Trie::reserve_block(int64_t max_keys, int64_t max_key_bytes, int64_t max_val
   return rc;
 }
 
+int Trie::reserve_nodes(uint64_t full, uint64_t shorts, uint64_t values, uint64_t records, uint64_t key_bytes,
+                        uint64_t value_bytes) {
+  err_.clear();
+  cudaSetDevice(dev_);
+  int rc = sync_counters();
+  if (rc) return rc;
+  return ensure_capacity(full, shorts, values, records, key_bytes + 64 * 8, value_bytes + 80 * 8, true);
+}
+
 int Trie::reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes) {
   err_.clear();
   if (n_keys > (1ull << 30)) return fail(E_ARG, "reserve: too many keys");
@@ -1394,7 +1431,7 @@ int Trie::reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes) {
   int rc = sync_counters();
   if (rc) return rc;
   // LockNU / block bound per key: one branch, three short nodes, one value
-  return ensure_capacity(n_keys, 3 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8);
+  return ensure_capacity(n_keys, 3 * n_keys, n_keys, n_keys, key_bytes + 64 * 8, value_bytes + 80 * 8, true);
 }
 
 }  // namespace gmpt
@@ -1499,6 +1536,49 @@ int gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_vals, int64
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("gen_values: ") + cudaGetErrorString(e);
+    return E_CUDA;
+  }
+  return OK;
+}
+
+}  // namespace gmpt
+
+namespace gmpt {
+
+namespace {
+static __device__ float g_feat_out[4 * 64];
+std::mutex g_feat_mu;
+float *g_feat_ptr[64] = {};
+}  // namespace
+
+// Sampled key features of a device-resident batch (k_sample_features); no
+// allocation per call: a small static device array per device.
+int batch_features_device(const uint8_t *d_keys, const int *d_kidx, int n, int64_t keys_bytes, float out[4],
+                          cudaStream_t st, std::string &err) {
+  if (n <= 0 || keys_bytes <= 0 || !d_keys || !d_kidx || !out) {
+    err = "batch_features: bad arguments";
+    return E_ARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    err = "batch_features: no usable device";
+    return E_CUDA;
+  }
+  std::lock_guard<std::mutex> g(g_feat_mu);
+  if (!g_feat_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_feat_out) != cudaSuccess) {
+      err = "batch_features: symbol address";
+      return E_CUDA;
+    }
+    g_feat_ptr[dev] = static_cast<float *>(p);
+  }
+  count_launch(), k_sample_features<<<1, 64, 0, st>>>(d_keys, d_kidx, n, keys_bytes, g_feat_ptr[dev]);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, g_feat_ptr[dev], 16, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("batch_features: ") + cudaGetErrorString(e);
     return E_CUDA;
   }
   return OK;

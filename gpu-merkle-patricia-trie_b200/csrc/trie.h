@@ -129,6 +129,9 @@ class Trie {
   // grow the pools and arenas now for n_keys more keys of the given byte
   // totals (no growth stalls, and no block graph rebuild, until then)
   int reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes);
+  // the same with explicit headroom per pool
+  int reserve_nodes(uint64_t full, uint64_t shorts, uint64_t values, uint64_t records, uint64_t key_bytes,
+                    uint64_t value_bytes);
   // size the block buffers for blocks up to these sizes and capture the
   // block graph now (so the first blocks do not pay for it)
   int reserve_block(int64_t max_keys, int64_t max_key_bytes, int64_t max_value_bytes, int64_t max_out);
@@ -169,13 +172,17 @@ class Trie {
   struct BlockRt {
     DevBlock keys, kidx, vals, vidx, tid, ptrie, poff, out_ids, out, koff, klen, bins, sorted;
     void *d_desc = nullptr, *h_desc = nullptr;  // BlockDesc (device / pinned)
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    std::vector<uint8_t> sig;  // launch arguments the graph was captured with
-    int grid = 0;
+    struct Captured {
+      std::vector<uint8_t> sig;  // launch arguments the graph was captured with
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      uint64_t used = 0;
+    };
+    std::vector<Captured> graphs;  // a few recent captures (e.g. one per grid size)
+    uint64_t tick = 0;
   } blk_;
   BlockInfo binfo_{};
-  int opt_block_grid_ = 0;      // CTAs of the persistent kernel (0 = one per SM)
+  int opt_block_grid_ = 0;      // CTAs of the persistent kernel (0 = all that fit co-resident)
   bool opt_block_graph_ = true;  // replay a captured graph (else plain launches)
   int block_launch(bool launch = true);
   int block_buffers(int64_t n, int64_t kb, int64_t vb, int64_t n_out);
@@ -203,8 +210,9 @@ class Trie {
   int check_cuda(cudaError_t e, const char *what);
   int sync_counters();
   int apply_counters();
+  // exact: grow to exactly what is asked (reservations) instead of by 1.5x steps
   int ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_value, uint64_t add_rec,
-                      uint64_t add_key_bytes, uint64_t add_val_bytes);
+                      uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact = false);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
   int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
@@ -223,5 +231,7 @@ int gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes, uint
              std::string &err);
 int gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_vals, int64_t *d_idx, cudaStream_t st,
                std::string &err);
+int batch_features_device(const uint8_t *d_keys, const int *d_kidx, int n, int64_t keys_bytes, float out[4],
+                          cudaStream_t st, std::string &err);
 
 }  // namespace gmpt

@@ -1130,6 +1130,18 @@ __device__ __forceinline__ bool hash_full_warp(const TrieView &tv, uint32_t idx,
   return true;
 }
 
+// A level's branch nodes, one warp each (levels with few branches, where a
+// node's serial encoding is the latency): 4 warps per CTA.
+__global__ void __launch_bounds__(128) k_hash_full_warp(TrieView tv, const uint32_t *refs, int count) {
+  extern __shared__ uint64_t stage_all[];  // 17 words per thread, then 4 messages
+  const int j = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (j >= count) return;  // whole warps leave together
+  uint8_t *msg = reinterpret_cast<uint8_t *>(stage_all + 17 * blockDim.x) + (threadIdx.x >> 5) * kWarpMsgBytes;
+  const uint32_t r = refs[j];
+  if (!hash_full_warp<false>(tv, ref_idx(r), msg, stage_all + threadIdx.x, blockDim.x) && (threadIdx.x & 31) == 0)
+    hash_node<false>(tv, r, stage_all + threadIdx.x, blockDim.x);
+}
+
 // 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
 // lanes in registers without spilling at this bound.
 __global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count) {

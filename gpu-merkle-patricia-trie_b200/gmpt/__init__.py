@@ -36,6 +36,7 @@ EXPORTS = [
     "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
     "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
+    "gmpt_reserve_nodes", "gmpt_batch_features_device",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
@@ -107,6 +108,7 @@ def lib():
     L.gmpt_block_timeline.argtypes = [vp, vp, i32, vp]
     L.gmpt_reserve.argtypes = [vp, i64, i64, i64]
     L.gmpt_reserve_block.argtypes = [vp, i64, i64, i64, i64]
+    L.gmpt_reserve_nodes.argtypes = [vp, i64, i64, i64, i64, i64, i64]
     L.gmpt_mlp_create.restype = vp
     L.gmpt_mlp_create.argtypes = [i32, i32, i32, i32, C.c_uint64]
     L.gmpt_mlp_destroy.argtypes = [vp]
@@ -121,6 +123,7 @@ def lib():
     L.gmpt_gen_ids.argtypes = [C.c_uint64, i64, i64, i64, C.c_double, C.c_double, vp, vp, vp]
     L.gmpt_gen_keys.argtypes = [C.c_uint64, vp, i64, i32, vp, vp, vp]
     L.gmpt_gen_values.argtypes = [C.c_uint64, i64, i32, vp, vp, vp]
+    L.gmpt_batch_features_device.argtypes = [vp, vp, i32, i64, vp, vp]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -230,6 +233,15 @@ def gen_keys(seed: int, d_ids: int, n: int, key_bytes: int, d_hexs: int, d_idx: 
 def gen_values(seed: int, n: int, value_bytes: int, d_vals: int, d_idx: int, stream: int = 0):
     _check(lib().gmpt_gen_values(int(seed) & ((1 << 64) - 1), int(n), int(value_bytes), C.c_void_p(d_vals),
                                  C.c_void_p(d_idx), C.c_void_p(stream) if stream else None))
+
+
+def batch_features_device(d_keys: int, d_kidx: int, n: int, keys_bytes: int, stream: int = 0) -> np.ndarray:
+    """[mean key nibbles, their std, repeated-sample share, common-prefix share]
+    of a device-resident batch (one kernel over 64 sampled keys)."""
+    out = np.zeros(4, dtype=np.float32)
+    _check(lib().gmpt_batch_features_device(C.c_void_p(d_keys), C.c_void_p(d_kidx), int(n), int(keys_bytes), _p(out),
+                                            C.c_void_p(stream) if stream else None))
+    return out
 
 
 def keccak_peak(device: int = 0) -> float:
@@ -408,6 +420,10 @@ class MPT:
         _check(self._L.gmpt_reserve_block(self._h, int(max_keys), int(max_key_bytes), int(max_value_bytes),
                                           int(max_out)))
 
+    def reserve_nodes(self, full: int, shorts: int, values: int, records: int, key_bytes: int, value_bytes: int):
+        _check(self._L.gmpt_reserve_nodes(self._h, int(full), int(shorts), int(values), int(records), int(key_bytes),
+                                          int(value_bytes)))
+
     def reserve(self, n_keys: int, key_bytes: int, value_bytes: int):
         _check(self._L.gmpt_reserve(self._h, int(n_keys), int(key_bytes), int(value_bytes)))
 
@@ -418,9 +434,11 @@ class MPT:
                                                v(d_vidx), None, v(d_tids), int(n), int(keys_bytes),
                                                int(values_bytes)))
 
-    def gets_forest_device(self, d_keys, d_kidx, d_tids, n: int, keys_bytes: int):
-        hps = np.zeros(max(n, 1), dtype=np.uint64)
-        sizes = np.zeros(max(n, 1), dtype=np.int32)
+    def gets_forest_device(self, d_keys, d_kidx, d_tids, n: int, keys_bytes: int, hps=None, sizes=None):
+        """Lookups of device-resident keys; results into hps / sizes (host
+        arrays of >= n entries, pinned for speed) or fresh arrays."""
+        hps = np.zeros(max(n, 1), dtype=np.uint64) if hps is None else hps
+        sizes = np.zeros(max(n, 1), dtype=np.int32) if sizes is None else sizes
         v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
         _check(self._L.gmpt_gets_forest_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes),
                                                _p(hps), _p(sizes)))

@@ -6,7 +6,8 @@ as a Poisson stream, served one at a time or drained and merged.
   expanded on the device (gmpt.gen_keys), so replicas regenerate identical
   batches without host copies.
 * A put request inserts n keys: fresh ids with probability p_new, else
-  zipf(theta) over the tenant's existing ids (updates).  A get request
+  zipf(theta) over the tenant's existing ids (updates).  A load request
+  fills a tenant trie created for it (empty, all keys fresh).  A get request
   looks up n zipf(theta) existing ids.
 * ``Runner`` applies requests to one forest replica: a run of same-kind
   requests (several tenants) becomes one forest put + PhaseHC + root read,
@@ -42,7 +43,7 @@ class Tenant:
 @dataclass
 class Request:
     i: int
-    kind: str             # "put" | "get"
+    kind: str             # "put" | "get" (a load is a put with p_new 1 into a new tenant)
     tenant: int
     n: int
     theta: float
@@ -58,16 +59,34 @@ def make_tenants(sizes, seed: int = 0x5EED0C50):
     return [Tenant(t, int(kb[t]), int(vb[t]), int(s)) for t, s in enumerate(sizes)]
 
 
-def make_stream(seed: int, count: int, n_tenants: int, read_ratio: float, n_min: int, n_max: int,
-                theta_max: float = 1.2):
+def make_stream(seed: int, count: int, tenants: list, read_ratio: float, n_min: int, n_max: int,
+                theta_max: float = 1.2, load_frac: float = 0.0):
+    """count requests; a put is a load into a new tenant (appended to
+    `tenants`, empty) with probability load_frac.  Requests target tenants
+    that exist by then; gets only non-empty ones."""
     rng = W.Xoshiro256ss(seed, lanes=256)
-    u = rng.uniform(5 * count).reshape(count, 5)
+    u = rng.uniform(7 * count).reshape(count, 7)
+    live = [t.tid for t in tenants]
+    filled = {t.tid for t in tenants if t.initial > 0}
     reqs = []
     for i in range(count):
-        n = int(round(math.exp(math.log(n_min) + u[i, 0] * (math.log(n_max) - math.log(n_min)))))
-        kind = "get" if u[i, 1] < read_ratio else "put"
-        reqs.append(Request(i, kind, int(u[i, 2] * n_tenants) % n_tenants, max(n, 1), float(u[i, 3] * theta_max),
-                            float(u[i, 4]), int(rng.words(1)[0])))
+        n = max(1, int(round(math.exp(math.log(n_min) + u[i, 0] * (math.log(n_max) - math.log(n_min))))))
+        seed_i = int(rng.words(1)[0])
+        if u[i, 1] < read_ratio and filled:
+            pool = sorted(filled)
+            reqs.append(Request(i, "get", pool[int(u[i, 2] * len(pool)) % len(pool)], n,
+                                float(u[i, 3] * theta_max), 0.0, seed_i))
+        elif u[i, 5] < load_frac:
+            t = make_tenants([0], seed=seed_i)[0]
+            t.tid = len(tenants)
+            tenants.append(t)
+            live.append(t.tid)
+            filled.add(t.tid)
+            reqs.append(Request(i, "put", t.tid, n, 0.0, 1.0, seed_i))
+        else:
+            tid = live[int(u[i, 2] * len(live)) % len(live)]
+            filled.add(tid)
+            reqs.append(Request(i, "put", tid, n, float(u[i, 3] * theta_max), float(u[i, 4]), seed_i))
     return reqs
 
 
@@ -114,21 +133,37 @@ class Stage:
 class Runner:
     """One forest replica holding every tenant, plus its id counters."""
 
-    def __init__(self, gmpt, tenants, device: int, dev, mode: int = 0, chunk: int = 1 << 22, record: bool = False):
+    def __init__(self, gmpt, tenants, device: int, dev, mode: int = 0, chunk: int = 1 << 22, record: bool = False,
+                 max_tries: int = 0):
         self.g = gmpt
-        self.tenants = tenants
-        self.mpt = gmpt.MPT(device=device, mode=mode, max_tries=len(tenants))
+        self.mpt = gmpt.MPT(device=device, mode=mode, max_tries=max(max_tries, len(tenants)))
         self.stage = Stage(dev)
-        self.count = {t.tid: 0 for t in tenants}
         self.stream = self.mpt.stream_ptr()
         self.record = [] if record else None  # host copies of every applied put (tests)
+        self.get_cap = 0
+        self.chunk = chunk
+        self._fill(tenants)
+
+    def _fill(self, tenants):
+        self.tenants = tenants
+        self.count = {t.tid: 0 for t in tenants}
         for t in tenants:  # initial contents, PhaseNU bulk loads
             left = t.initial
             while left > 0:
-                n = min(chunk, left)
+                n = min(self.chunk, left)
                 self._load_fresh(t, n)
                 left -= n
         self.mpt.hash_onepass_v2()
+
+    def reset(self, tenants):
+        """Empty the forest (capacity kept) and load a new tenant set."""
+        if len(tenants) > self.mpt_max_tries():
+            raise ValueError("more tenants than the forest holds")
+        self.mpt.reset()
+        self._fill(tenants)
+
+    def mpt_max_tries(self) -> int:
+        return int(self.mpt._L.gmpt_max_tries(self.mpt._h))
 
     def _load_fresh(self, t, n):
         s = self.stage
@@ -145,6 +180,33 @@ class Runner:
         self.mpt.puts_forest_device(True, s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(), s.vidx.data_ptr(),
                                     s.tids.data_ptr(), n, n * (2 * t.key_bytes + 1), n * t.value_bytes)
         self.count[t.tid] += n
+
+    def reserve_for(self, reqs, merged_keys: int = 0):
+        """Grow pools, arenas and block buffers now for every put of the
+        stream (no growth, no graph capture inside a timed request)."""
+        kmax = max(2 * t.key_bytes + 1 for t in self.tenants)
+        vmax = max(t.value_bytes for t in self.tenants)
+        puts = [r for r in reqs if r.kind == "put"]
+        total = sum(r.n for r in puts)
+        kbytes = sum(r.n * (2 * self.tenants[r.tenant].key_bytes + 1 + 8) for r in puts)
+        vbytes = sum(r.n * self.tenants[r.tenant].value_bytes for r in puts)
+        big = max([r.n for r in reqs] + [merged_keys, 1])
+        # growth of the stream (a new key adds about one short node and a
+        # fraction of a branch) plus the per-batch headroom the inserts check
+        # for (PhaseNU: 2 branches and 4 short nodes per key of the batch)
+        self.mpt.reserve_nodes(total // 2 + 2 * big, total + total // 4 + 4 * big, total + big, total + big,
+                               kbytes + big * kmax, vbytes + big * vmax)
+        gets = [r for r in reqs if r.kind == "get"]
+        if gets:  # grow the lookup workspaces and result buffers now (read only)
+            g = max(gets, key=lambda r: r.n)
+            warm = Request(-1, "get", g.tenant, max(g.n, merged_keys if merged_keys else 0), 0.0, 0.0, 1)
+            n, kb, _ = self.build([warm])
+            self.get(n, kb)
+        for c in TU.CONFIGS:  # capture the block graph of every persistent grid
+            if c.get("persistent"):
+                self.mpt.set_option("block_grid", c.get("block_grid", 0))
+                self.mpt.reserve_block(big, big * kmax, big * vmax, len(self.tenants))
+        self.stage.ensure(big, big * kmax, big * vmax)
 
     def build(self, reqs):
         """Generate the merged batch of same-kind requests into the stage."""
@@ -181,38 +243,14 @@ class Runner:
         torch.cuda.synchronize(s.dev)
         return n, kb, voff
 
-    def features(self, reqs, n, kb, vb, sample: int = 512, probe: int = 256):
-        """Selector features from a sample of the staged batch (keys copied
-        to the host) and a lookup of a few sampled keys (new-key share)."""
+    def features(self, reqs, n, kb, vb):
+        """Selector features: exact totals plus one sampling kernel over the
+        staged keys (gmpt_batch_features_device)."""
         s = self.stage
-        torch = s.torch
-        rng = np.random.default_rng(reqs[0].seed & 0xFFFFFFFF)
-        pos = np.sort(rng.choice(n, size=min(n, sample), replace=False)) if n > sample else np.arange(n)
-        dpos = torch.from_numpy(pos).to(s.dev)
-        kid = s.kidx[: 2 * n].view(-1, 2)[dpos].long()
-        lens = kid[:, 1] - kid[:, 0] + 1
-        starts = torch.repeat_interleave(kid[:, 0], lens)
-        within = torch.arange(int(lens.sum().item()), device=s.dev) - torch.repeat_interleave(
-            torch.cumsum(lens, 0) - lens, lens)
-        flat = s.keys[starts + within].cpu().numpy()
-        lh = lens.cpu().numpy()
-        keys, at = [], 0
-        for ln in lh.tolist():
-            keys.append(flat[at: at + ln].tobytes())
-            at += ln
-        # new-key share of a few sampled keys (lookups on the live forest)
-        pk = min(len(pos), probe)
-        pidx = np.zeros(2 * pk, np.int32)
-        buf = b"".join(keys[:pk])
-        at = 0
-        for j in range(pk):
-            pidx[2 * j], pidx[2 * j + 1] = at, at + len(keys[j]) - 1
-            at += len(keys[j])
-        tids = s.tids[: n][torch.from_numpy(pos[:pk]).to(s.dev)].cpu().numpy().astype(np.int32)
-        _, sizes = self.mpt.gets_forest(np.frombuffer(buf, np.uint8), pidx, tids)
-        new_frac = float(np.mean(sizes == 0)) if pk else 0.0
-        trie_keys = sum(self.count[t] for t in set(r.tenant for r in reqs))
-        return TU.batch_features(n, keys, vb / max(n, 1), trie_keys, new_frac)
+        st = self.g.batch_features_device(s.keys.data_ptr(), s.kidx.data_ptr(), n, kb)
+        touched = set(r.tenant for r in reqs)
+        trie_keys = sum(self.count[t] for t in touched)
+        return TU.features_from_stats(n, kb, st, vb / max(n, 1), trie_keys, len(touched))
 
     def snapshot(self, n, kb, vb):
         """Host copy of the staged batch (keys, values, trie ids)."""
@@ -225,15 +263,25 @@ class Runner:
             self.record.append(self.snapshot(n, kb, vb))
         two = TU.apply_config(self.mpt, k)
         s = self.stage
+        touched = sorted(set(r.tenant for r in reqs))
+        if TU.CONFIGS[k].get("persistent"):
+            return self.mpt.block_update_device(s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(),
+                                                s.vidx.data_ptr(), s.tids.data_ptr(), 0, 0, n, n, kb, vb, touched)
         self.mpt.puts_forest_device(two, s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(), s.vidx.data_ptr(),
                                     s.tids.data_ptr(), n, kb, vb)
         self.mpt.hash_onepass_v2()
-        return self.mpt.get_roots(sorted(set(r.tenant for r in reqs)))
+        return self.mpt.get_roots(touched)
 
     def get(self, n, kb):
         s = self.stage
-        _, sizes = self.mpt.gets_forest_device(s.keys.data_ptr(), s.kidx.data_ptr(), s.tids.data_ptr(), n, kb)
-        return sizes
+        if n > self.get_cap:  # pinned result buffers, reused
+            torch = s.torch
+            self.get_cap = int(n * 1.25) + 1024
+            self.h_hps = torch.empty(self.get_cap, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+            self.h_sizes = torch.empty(self.get_cap, dtype=torch.int32).pin_memory().numpy()
+        _, sizes = self.mpt.gets_forest_device(s.keys.data_ptr(), s.kidx.data_ptr(), s.tids.data_ptr(), n, kb,
+                                               self.h_hps, self.h_sizes)
+        return sizes.copy()
 
     def roots(self):
         return self.mpt.get_roots(n=len(self.tenants))
@@ -248,20 +296,22 @@ def _timed(fn):
     return out, (time.perf_counter() - t0) * 1e3
 
 
-def time_matrix(replicas, reqs, with_features=True):
-    """Every put under every configuration (replica k runs configuration k).
-    Returns times [N, K] (ms; nan for gets), get times [N] (nan for puts),
+def time_matrix(replicas, reqs, with_features=True, configs=None):
+    """Every put under every configuration (replica j runs configuration
+    configs[j], default j).  Returns times [N, len(CONFIGS)] (ms; nan for
+    gets and for configurations not run), get times [N] (nan for puts),
     features [N, F] of the puts (zeros for gets)."""
-    K = len(replicas)
-    T = np.full((len(reqs), K), np.nan)
+    configs = list(range(len(replicas))) if configs is None else list(configs)
+    T = np.full((len(reqs), len(TU.CONFIGS)), np.nan)
     G = np.full(len(reqs), np.nan)
     F = np.zeros((len(reqs), len(TU.FEATURES)), dtype=np.float32)
     for i, r in enumerate(reqs):
         if r.kind == "put":
             roots = None
-            for k, rep in enumerate(replicas):
+            for j, rep in enumerate(replicas):
+                k = configs[j]
                 n, kb, vb = rep.build([r])
-                if k == 0 and with_features:
+                if j == 0 and with_features:
                     F[i] = rep.features([r], n, kb, vb)
                 out, ms = _timed(lambda: rep.put([r], k, n, kb, vb))
                 T[i, k] = ms
@@ -297,12 +347,14 @@ class ServeResult:
     groups: int
     choices: dict = field(default_factory=dict)
     get_sizes: list = field(default_factory=list)
+    service_ms: np.ndarray | None = None  # per request (one-at-a-time server)
 
 
 def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> ServeResult:
     """Live server on a virtual clock.  policy(runner, reqs, n, kb, vb) ->
     configuration index (its own time is part of the service time)."""
     lat = np.zeros(len(reqs))
+    svc = np.zeros(len(reqs))
     free = 0.0
     busy = 0.0
     groups = 0
@@ -339,7 +391,8 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> Serv
             groups += 1
             for r in run:
                 lat[r.i - reqs[0].i] = (t - r.arrival) * 1e3
+                svc[r.i - reqs[0].i] = ms / len(run)
             a = b
         free = t
         i = j
-    return ServeResult(lat, busy, sum(r.n for r in reqs), 0, groups, choices, gets)
+    return ServeResult(lat, busy, sum(r.n for r in reqs), 0, groups, choices, gets, svc)

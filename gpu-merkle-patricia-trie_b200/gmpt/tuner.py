@@ -28,16 +28,20 @@ import numpy as np
 CONFIGS = [
     {"name": "phasenu", "two_phase": True, "local_build": 1, "local_sort": 1},
     {"name": "phasenu-global-build", "two_phase": True, "local_build": 0, "local_sort": 1},
-    {"name": "phasenu-global-sort", "two_phase": True, "local_build": 1, "local_sort": 0},
     {"name": "locknu-4", "two_phase": False, "latch_ways": 4},
     {"name": "locknu-2", "two_phase": False, "latch_ways": 2},
     {"name": "locknu-1", "two_phase": False, "latch_ways": 1},
+    # LockNU insert + PhaseHC + root read in one graph-replayed persistent
+    # launch (gmpt_block_update with every key in stage 0), with two or one
+    # co-resident CTAs per SM (block_grid 0 = the device's maximum)
+    {"name": "persistent-2cta", "two_phase": False, "persistent": True, "block_grid": 0},
+    {"name": "persistent-1cta", "two_phase": False, "persistent": True, "block_grid": 148},
 ]
 FIXED_PHASENU = 0
-FIXED_LOCKNU = 3  # the reference's fixed choice
+FIXED_LOCKNU = 2  # the reference's fixed choice
 
 FEATURES = ["log2_n", "key_nibbles", "key_nibbles_std", "dup_frac", "log2_trie_keys", "log2_value_bytes",
-            "lcp_frac", "new_frac_hint"]
+            "lcp_frac", "log2_tries"]
 
 
 def apply_config(mpt, k: int) -> bool:
@@ -46,29 +50,57 @@ def apply_config(mpt, k: int) -> bool:
     mpt.set_option("local_build", c.get("local_build", 1))
     mpt.set_option("local_sort", c.get("local_sort", 1))
     mpt.set_option("latch_ways", c.get("latch_ways", 4))
+    if c.get("persistent"):
+        mpt.set_option("block_grid", c.get("block_grid", 0))
     return bool(c["two_phase"])
 
 
-def batch_features(n: int, sample_keys: list, value_bytes: float, trie_keys: int, new_frac_hint: float = 0.0):
-    """Features of a put batch from a sample of its keys (bytes objects, hex
-    nibble form) and the trie's current key count."""
-    s = max(len(sample_keys), 1)
-    lens = np.array([len(k) for k in sample_keys] or [0], dtype=np.float64)
-    distinct = len(set(sample_keys))
-    dup = 1.0 - distinct / s
-    ks = sorted(set(sample_keys))
-    lcp = 0.0
-    if len(ks) > 1:
-        tot = 0
-        for a, b in zip(ks, ks[1:]):
-            m = min(len(a), len(b))
-            j = 0
-            while j < m and a[j] == b[j]:
-                j += 1
-            tot += j
-        lcp = tot / (len(ks) - 1) / max(lens.mean(), 1.0)
-    return np.array([math.log2(n + 1), lens.mean() / 64.0, lens.std() / 64.0, dup, math.log2(trie_keys + 1),
-                     math.log2(value_bytes + 1), lcp, new_frac_hint], dtype=np.float32)
+def sample_stats(keys_hexs: np.ndarray, keys_indexs: np.ndarray, samples: int = 64) -> np.ndarray:
+    """Host restatement of gmpt_batch_features_device (k_sample_features):
+    over `samples` evenly spaced keys (j * n // s), mean and spread of key
+    length in nibbles, share of samples equal to an earlier sample, and the
+    mean longest common prefix of a sample with any other sample (= with
+    its neighbours in sorted order) over the mean length."""
+    ki = np.asarray(keys_indexs).reshape(-1, 2)
+    n = len(ki)
+    s = min(n, samples)
+    if s == 0:
+        return np.zeros(4, dtype=np.float32)
+    pos = (np.arange(s, dtype=np.int64) * n) // s
+    keys = [bytes(keys_hexs[ki[i, 0]: ki[i, 1] + 1]) for i in pos]
+    lens = np.array([len(k) for k in keys], dtype=np.float64)
+    seen, dup = set(), 0
+    for k in keys:
+        dup += k in seen
+        seen.add(k)
+    order = sorted(range(s), key=lambda j: keys[j])
+    best = np.zeros(s)
+
+    def lcp(a, b):
+        m = min(len(a), len(b))
+        i = 0
+        while i < m and a[i] == b[i]:
+            i += 1
+        return i
+
+    for r in range(1, s):
+        a, b = order[r - 1], order[r]
+        v = lcp(keys[a], keys[b])
+        best[a] = max(best[a], v)
+        best[b] = max(best[b], v)
+    mean = lens.mean()
+    return np.array([mean, lens.std(), dup / s, best.mean() / mean if mean > 0 else 0.0], dtype=np.float32)
+
+
+def features_from_stats(n: int, key_bytes_total: int, stats, value_bytes: float, trie_keys: int,
+                        n_tries: int = 1) -> np.ndarray:
+    """Selector features of a put batch: exact size and key bytes, sampled
+    key statistics (sample_stats / gmpt_batch_features_device), the mean
+    value size, the key count of the tries it touches and how many."""
+    st = np.asarray(stats, dtype=np.float64)
+    return np.array([math.log2(n + 1), key_bytes_total / max(n, 1) / 64.0, st[1] / 64.0, st[2],
+                     math.log2(trie_keys + 1), math.log2(value_bytes + 1), st[3], math.log2(max(n_tries, 1))],
+                    dtype=np.float32)
 
 
 # -- the plain autotuned rule --------------------------------------------------
@@ -115,35 +147,92 @@ class Autotuner:
 
 # -- the MLP selector ----------------------------------------------------------
 
+def regret(times_ms: np.ndarray, choice) -> float:
+    """Total time of the chosen configurations over the per-batch best, - 1."""
+    t = np.asarray(times_ms, dtype=np.float64)
+    best = np.nanmin(t, 1)
+    got = t[np.arange(len(t)), np.asarray(choice)]
+    return float(np.nansum(got) / np.nansum(best) - 1.0)
+
+
 @dataclass
 class Selector:
+    """MLP schedule selector with the autotuned rule as fallback and judge:
+    fit() holds out a quarter of the measured batches, and the network is
+    used only if its regret there is no worse than the rule's (fit on the
+    same three quarters); either way both are then refit on all batches."""
+
     net: object                 # gmpt.Net(len(FEATURES), hidden, len(CONFIGS))
     rule: Autotuner
     mean: np.ndarray | None = None
     std: np.ndarray | None = None
     lo: np.ndarray | None = None
     hi: np.ndarray | None = None
+    cols: list | None = None    # configurations with measurements
     ood_margin: float = 0.5     # fallback outside [lo - m*range, hi + m*range]
+    use_net: bool = False
+    validation: dict = field(default_factory=dict)
     fallbacks: int = 0
     choices: int = 0
 
-    def fit(self, feats: np.ndarray, times_ms: np.ndarray, epochs: int = 300, lr: float = 3e-3, seed: int = 17,
-            batch: int = 64) -> float:
-        """Train on measured times: target log(ms) per configuration, masked
-        where a configuration was not measured.  Uses the GPU kernels."""
+    def _train(self, feats, times_ms, epochs, lr, seed, batch):
         x = np.asarray(feats, dtype=np.float64)
         self.mean = x.mean(0)
         self.std = np.where(x.std(0) > 1e-6, x.std(0), 1.0)
         self.lo, self.hi = x.min(0), x.max(0)
         z = ((x - self.mean) / self.std).astype(np.float32)
         t = np.asarray(times_ms, dtype=np.float64)
-        m = (~np.isnan(t)).astype(np.float32)
-        tgt = np.where(np.isnan(t), 0.0, np.log(np.maximum(t, 1e-6))).astype(np.float32)
+        self.cols = [k for k in range(t.shape[1]) if np.any(~np.isnan(t[:, k]))]
+        tgt, m = self._targets(t)
         return self.net.train(z, tgt, m, epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+    def fit(self, feats: np.ndarray, times_ms: np.ndarray, max_epochs: int = 600, lr: float = 3e-3, seed: int = 17,
+            batch: int = 64, holdout: float = 0.25, step: int = 50) -> float:
+        """Train on measured times (target log(ms) per configuration, masked
+        where a configuration was not measured) with the GPU kernels.  The
+        epoch count is the one with the least regret on the held-out
+        quarter (checked every `step` epochs); the network is enabled only
+        if that regret is no worse than the rule's."""
+        feats = np.asarray(feats, dtype=np.float64)
+        times_ms = np.asarray(times_ms, dtype=np.float64)
+        n = len(feats)
+        init = self.net.params()
+        epochs = max_epochs
+        if n >= 8:
+            hold = np.zeros(n, dtype=bool)
+            hold[np.random.default_rng(seed).permutation(n)[: max(2, int(n * holdout))]] = True
+            rule = Autotuner().fit(feats[~hold], times_ms[~hold])
+            rule_r = regret(times_ms[hold], [rule.choose(f) for f in feats[hold]])
+            self._train(feats[~hold], times_ms[~hold], step, lr, seed, batch)
+            curve = []
+            for e in range(step, max_epochs + 1, step):
+                if e > step:
+                    self.net.train(((feats[~hold] - self.mean) / self.std).astype(np.float32),
+                                   *self._targets(times_ms[~hold]), epochs=step, batch=batch, lr=lr, seed=seed + e)
+                curve.append((regret(times_ms[hold], [self._net_choice(f) for f in feats[hold]]), e))
+            net_r, epochs = min(curve)
+            self.use_net = net_r <= rule_r
+            self.validation = {"held_out": int(hold.sum()), "net_regret": round(net_r, 4), "epochs": epochs,
+                               "rule_regret": round(rule_r, 4), "use_net": self.use_net}
+            self.net.set_params(init)
+        else:
+            self.use_net = True
+        self.rule.fit(feats, times_ms)
+        return self._train(feats, times_ms, epochs, lr, seed, batch)
+
+    def _targets(self, times_ms):
+        t = np.asarray(times_ms, dtype=np.float64)
+        m = (~np.isnan(t)).astype(np.float32)
+        tgt = np.where(np.isnan(t), 0.0, np.log(np.maximum(np.nan_to_num(t, nan=1.0), 1e-6))).astype(np.float32)
+        return tgt, m
 
     def predict(self, feats) -> np.ndarray:
         z = ((np.atleast_2d(feats) - self.mean) / self.std).astype(np.float32)
         return self.net.forward(z)
+
+    def _net_choice(self, f) -> int:
+        y = self.predict(f)[0]
+        return int(self.cols[int(np.argmin(y[self.cols]))])
 
     def in_range(self, f) -> bool:
         span = np.maximum(self.hi - self.lo, 1e-6)
@@ -151,7 +240,7 @@ class Selector:
 
     def choose(self, f) -> int:
         self.choices += 1
-        if self.mean is None or not self.in_range(f):
+        if self.mean is None or not self.use_net or not self.in_range(f):
             self.fallbacks += 1
             return self.rule.choose(f)
-        return int(np.argmin(self.predict(f)[0]))
+        return self._net_choice(f)

@@ -148,6 +148,11 @@ int gmpt_block_timeline(gmpt_trie *t, uint64_t *out_ns, int cap, int *n);
  * do not stall on growth.  No counterpart in the reference, whose arenas are
  * fixed at construction (util/allocator.cuh:152-157). */
 int gmpt_reserve(gmpt_trie *t, int64_t n_keys, int64_t key_bytes, int64_t value_bytes);
+/* gmpt_reserve with explicit headroom: free slots for `full` branch nodes,
+ * `shorts` short nodes, `values` value nodes and `records` value records,
+ * and key_bytes / value_bytes more arena bytes, beyond what is in use. */
+int gmpt_reserve_nodes(gmpt_trie *t, int64_t full, int64_t shorts, int64_t values, int64_t records, int64_t key_bytes,
+                       int64_t value_bytes);
 /* Size the gmpt_block_update buffers for blocks of up to max_keys keys,
  * max_key_bytes / max_value_bytes stream bytes and max_out reported roots,
  * and capture the block graph now, so that no block of that size pays for
@@ -180,6 +185,15 @@ int gmpt_gen_keys(uint64_t seed, const int64_t *d_ids, int64_t n, int key_bytes,
                   int *d_keys_indexs, void *stream);
 int gmpt_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_values, int64_t *d_values_indexs,
                     void *stream);
+
+/* Schedule-selector features of a device-resident key batch, from 64 evenly
+ * spaced keys: out[0] mean key length (nibbles), out[1] its standard
+ * deviation, out[2] share of sampled keys repeating an earlier sample,
+ * out[3] mean longest common prefix of a sample with any other sample over
+ * the mean length.  Reads only bytes [0, keys_bytes) of the key stream.
+ * One kernel, no allocation; synchronous on `stream`. */
+int gmpt_batch_features_device(const uint8_t *d_keys_hexs, const int *d_keys_indexs, int n, int64_t keys_bytes,
+                               float out[4], void *stream);
 
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
