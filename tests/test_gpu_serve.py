@@ -136,3 +136,35 @@ def test_device_feature_sampler_matches_host_restatement(gpu_lib, dev):
         got = gpu_lib.batch_features_device(dk.data_ptr(), di.data_ptr(), n, len(b.keys_hexs))
         want = TU.sample_stats(b.keys_hexs, b.keys_indexs)
         assert np.allclose(got, want, rtol=1e-5, atol=1e-5), (n, got, want)
+
+
+def test_trained_network_gains_over_fixed_schedules(gpu_lib, dev):
+    """Train the selector on times measured for one stream; on a second
+    stream's times, the network's picks must cost less than running every
+    put with the fixed LockNU schedule (what the reference does) or the fixed
+    PhaseNU one, and the gated selector must be no worse than the rule."""
+    def matrix(seed, count):
+        tenants = S.make_tenants([0, 20000, 100000])
+        reqs = S.make_stream(seed, count, tenants, 0.1, 500, 200000, load_frac=0.25)
+        reps = [S.Runner(gpu_lib, tenants, 0, dev) for _ in TU.CONFIGS]
+        for r in reps:
+            r.reserve_for(reqs)
+        T, _, F = S.time_matrix(reps, reqs)
+        for r in reps:
+            r.close()
+        puts = np.array([r.kind == "put" for r in reqs])
+        return F[puts], T[puts]
+
+    Ftr, Ttr = matrix(0x7E57, 160)
+    Fev, Tev = matrix(0x7E58, 100)
+    sel = TU.Selector(gpu_lib.Net(len(TU.FEATURES), 32, len(TU.CONFIGS), seed=2), TU.Autotuner())
+    sel.fit(Ftr, Ttr, max_epochs=400)
+    net = TU.regret(Tev, [sel._net_choice(f) for f in Fev])
+    chosen = TU.regret(Tev, [sel.choose(f) for f in Fev])
+    locknu = TU.regret(Tev, [TU.FIXED_LOCKNU] * len(Fev))
+    phasenu = TU.regret(Tev, [TU.FIXED_PHASENU] * len(Fev))
+    rule = TU.regret(Tev, [sel.rule.choose(f) for f in Fev])
+    print(f"regret on unseen stream: network {net:.3f} selector {chosen:.3f} rule {rule:.3f} "
+          f"fixed LockNU {locknu:.3f} fixed PhaseNU {phasenu:.3f}; validation {sel.validation}")
+    assert net < locknu and net < phasenu
+    assert chosen < locknu and chosen < phasenu
