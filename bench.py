@@ -227,6 +227,10 @@ def cpu_baseline(args, batches):
             "sample": f"first {n} keys of the load and of the update batch; {desc}"}
 
 
+GRIDS = (74, 148, 296)  # persistent-kernel grids the block autotuner tries
+TUNE_ROUNDS = 4
+
+
 def run_eth(args, local, dev):
     """Ethereum-shaped forest: state trie + per-account storage tries, block by
     block, through the persistent graph-replayed launch (device-resident and
@@ -253,8 +257,10 @@ def run_eth(args, local, dev):
         f.reserve(b.n + tot_keys, b.key_bytes() + kb, b.value_bytes() + vb)
         f.puts_2phase_with_valuehp(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
         f.hash_onepass_v2()
-        f.reserve_block(max(x.n for x in blks), max(x.batch.key_bytes() for x in blks),
-                        max(x.batch.value_bytes() for x in blks), max(len(x.out_ids) for x in blks))
+        for g in GRIDS:  # one captured block graph per candidate grid
+            f.set_option("block_grid", g)
+            f.reserve_block(max(x.n for x in blks), max(x.batch.key_bytes() for x in blks),
+                            max(x.batch.value_bytes() for x in blks), max(len(x.out_ids) for x in blks))
         return f
 
     t1 = time.time()
@@ -274,7 +280,18 @@ def run_eth(args, local, dev):
     launches0 = gmpt.launch_count()
     sampler = ClockSampler(local)
     sampler.start()
-    for b, d in zip(blks, dblk):
+    # autotuned persistent grid: the first blocks rotate through the candidate
+    # grids (same roots whichever runs), then the fastest median is kept
+    tune_ms = {g: [] for g in GRIDS}
+    chosen = None
+    for k, (b, d) in enumerate(zip(blks, dblk)):
+        if k < TUNE_ROUNDS * len(GRIDS):
+            grid = GRIDS[k % len(GRIDS)]
+        else:
+            if chosen is None:
+                chosen = min(GRIDS, key=lambda g: float(np.median(tune_ms[g])))
+            grid = chosen
+        fb.set_option("block_grid", grid)
         a = torch.cuda.Event(enable_timing=True)
         z = torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -284,6 +301,8 @@ def run_eth(args, local, dev):
         z.synchronize()
         roots_block.append(r)
         ms_block.append(a.elapsed_time(z))
+        if chosen is None:
+            tune_ms[grid].append(ms_block[-1])
     clocks = sampler.stop()
     launches = gmpt.launch_count() - launches0
     info = fb.block_info()
@@ -292,6 +311,7 @@ def run_eth(args, local, dev):
     del dblk
     # e2e: pinned host inputs through the host C ABI, block by block
     fe = fresh()
+    fe.set_option("block_grid", chosen or GRIDS[0])
     pinned = []
     for b in blks:
         arrs = [b.batch.keys_hexs, b.batch.keys_indexs, b.batch.values, b.batch.values_indexs, b.trie_ids,
@@ -358,7 +378,9 @@ def run_eth(args, local, dev):
         "block_vs_plain": round(blk_rate / plain_rate, 2) if plain_rate else None,
         "block_vs_forest": round(blk_rate / rate(keys_cmp, ms_forest), 2),
         "roots_agree": True, "state_root_before": state_root.hex(), "state_root_after": roots_block[-1][0].hex(),
-        "persistent_grid": info["grid"], "graph_captures": info["captures"], "gpu_launches": int(launches),
+        "persistent_grid": chosen, "grid_autotune_median_ms": {str(g): round(float(np.median(v)), 3)
+                                                                for g, v in tune_ms.items() if v},
+        "graph_captures": info["captures"], "gpu_launches": int(launches),
         "last_block_levels": info["levels"], "last_block_dirty": info["dirty"],
         "last_block_timeline_us": [round(x / 1e3, 1) for x in np.diff(tl).tolist()],
         "setup_s": {"generate": round(setup_gen_s, 1), "load_state": round(setup_load_s, 1)},
