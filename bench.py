@@ -33,6 +33,9 @@ sys.path.insert(0, str(REPO / "gpu-merkle-patricia-trie_b200"))
 from gmpt import workloads as W  # noqa: E402
 
 PEAKS_FILE = REPO / "MEASURED_PEAKS.json"
+# DRAM bytes per hashed node of k_hash_level, from one ncu capture of the
+# largest level of a 1M-key YCSB load (276.7 MB over 701K nodes)
+HASH_TRAFFIC_B_PER_NODE = 394.7
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -44,6 +47,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=1 << 24, help="keys per batch")
     p.add_argument("--strategy", default="auto", help="auto | 2phase | latching | 2phase,latching")
+    p.add_argument("--latch-ways", type=int, default=4, help="keys per LockNU thread (1, 2, 4)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=1 << 20)
@@ -546,6 +550,7 @@ def run_ours(args, world, rank, local):
             v=torch.from_numpy(b.values).to(dev), vi=torch.from_numpy(b.values_indexs).to(dev),
             n=b.n, kb=b.key_bytes(), vb=b.value_bytes()))
     t = gmpt.MPT(device=local)
+    t.set_option("latch_ways", args.latch_ways)
     stream = torch.cuda.ExternalStream(t.stream_ptr(), device=dev)
     keys_per_step = sum(b.n for b in batches)
 
@@ -620,6 +625,7 @@ def run_ours(args, world, rank, local):
     perms = [h["last_keccak_blocks"] for info in stats_all for (_, h) in info]
     hash_ms_step = sum(hk_ms) / len(stats_all)
     alg_bytes_per_launch = sum(enc) / sum(hk_launch)
+    nodes_per_launch = sum(h["last_hashed"] for info in stats_all for (_, h) in info) / sum(hk_launch)
     avg_launch_s = (sum(hk_ms) / 1e3) / sum(hk_launch)
     hbm_peak, peak_kind = peaks()
     kpeak = gmpt.keccak_peak(local)
@@ -699,7 +705,11 @@ def run_ours(args, world, rank, local):
         "phases_ms": phase,
         "roofline": {"bound": "hbm", "kernel": "k_hash_level (fused RLP encode + Keccak-256)",
                      "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "frac": round(achieved / hbm_peak, 4),
+                     "traffic": int(HASH_TRAFFIC_B_PER_NODE * nodes_per_launch),
+                     "traffic_source": "ncu dram__bytes_read+write per hashed node of the largest 1M-key YCSB level "
+                                       "(profiles/k_hash_level_ycsb1m.md) x hashed nodes per level here",
+                     "peak_kind": peak_kind,
                      "alg_bytes_per_launch": int(alg_bytes_per_launch),
                      "avg_launch_us": round(avg_launch_s * 1e6, 2)},
         "keccak": {"permutations_per_step": int(sum(perms) / len(stats_all)),
