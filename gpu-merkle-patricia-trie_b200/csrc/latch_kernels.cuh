@@ -181,25 +181,45 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
 // handed to latch_from at the slot where its descent stopped.
 constexpr int kLatchWays = 4;
 
-// Keys t + w * nthreads (w < kWays) of koff/klen[0..n), record ids
-// vid_base + i, trie ids tid[i] (null: trie 0).
+// Which keys a LockNU launch walks: all of [0, n), or (dedup) the positions
+// sel[0 .. *count) -- the last occurrence of every distinct key -- unless
+// *collision is set, in which case all keys are walked after all.
+struct KeySelect {
+  const uint32_t *sel = nullptr;
+  const unsigned long long *count = nullptr;
+  const uint32_t *collision = nullptr;
+};
+
+// Keys t + w * nthreads (w < kWays) of koff/klen[0..n) (or of the selected
+// positions), record ids vid_base + i, trie ids tid[i] (null: trie 0).
 template <int kWays = kLatchWays>
 __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, const uint64_t *koff,
                                            const uint32_t *klen, int n, uint64_t vid_base, uint32_t retry_limit,
-                                           const int *tid, int t, int nthreads) {
+                                           const int *tid, int t, int nthreads, KeySelect ks = KeySelect()) {
   const uint32_t gen = tv.gen;
+  const uint32_t *sel = ks.sel;
+  int n_eff = n;
+  if (sel) {
+    if (*ks.collision)
+      sel = nullptr;
+    else
+      n_eff = (int)(*ks.count & 0xFFFFFFFFull);
+  }
   uint32_t *sp[kWays];
-  uint32_t x[kWays], len[kWays];
+  uint32_t x[kWays], len[kWays], key[kWays];
   uint64_t ko[kWays];
   uint8_t st[kWays];  // 0 done, 1 walking, 2 hand off to latch_from
 #pragma unroll
   for (int w = 0; w < kWays; ++w) {
-    const int i = t + w * nthreads;
-    st[w] = i < n ? 1 : 0;
-    sp[w] = tv.roots + ((i < n && tid) ? tid[i] : 0);
+    const int j = t + w * nthreads;
+    const bool on = j < n_eff;
+    const int i = on ? (sel ? (int)sel[j] : j) : 0;
+    key[w] = (uint32_t)i;
+    st[w] = on ? 1 : 0;
+    sp[w] = tv.roots + ((on && tid) ? tid[i] : 0);
     x[w] = 0;
-    ko[w] = i < n ? koff[i] : 0;
-    len[w] = i < n ? klen[i] : 0;
+    ko[w] = on ? koff[i] : 0;
+    len[w] = on ? klen[i] : 0;
   }
   // Each round moves every walking key down one node in phases, so the loads
   // of all ways are in flight together: (1) slot + node fields + dirty
@@ -281,7 +301,7 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
         x[w] += sl[w];
         any = true;
       } else if (kind == KIND_VALUE && x[w] == len[w]) {
-        atomicMax(&tv.value_vid[idx], vid_base + (unsigned long long)(t + w * nthreads));
+        atomicMax(&tv.value_vid[idx], vid_base + (unsigned long long)key[w]);
         st[w] = 0;
       } else {
         st[w] = 2;  // empty slot (new leaf) or malformed key
@@ -304,16 +324,105 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
 #pragma unroll
   for (int w = 0; w < kWays; ++w)
     if (st[w] != 0)
-      latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)(t + w * nthreads),
-                 retry_limit);
+      latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)key[w], retry_limit);
 }
 
 template <int kWays>
 __global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
                                                       const uint32_t *klen, int n, uint64_t vid_base,
-                                                      uint32_t retry_limit, const int *tid) {
+                                                      uint32_t retry_limit, const int *tid, KeySelect ks) {
   latch_keys<kWays>(tv, dl, koff, klen, n, vid_base, retry_limit, tid, blockIdx.x * blockDim.x + threadIdx.x,
-                    gridDim.x * blockDim.x);
+                    gridDim.x * blockDim.x, ks);
+}
+
+// ---------------------------------------------------------------------------
+// Batch dedup before LockNU: a duplicate-heavy batch (zipf updates) walks the
+// trie once per distinct key instead of once per occurrence.  An
+// open-addressing table keyed by a 64-bit hash of (trie, key nibbles) keeps
+// the largest batch position per hash (= the occurrence that must win); a
+// second pass compares every other occurrence's key with its slot's winner,
+// and a mismatch (two different keys with one hash) sets *collision, which
+// makes the insert walk every key as if there were no dedup.  Results never
+// depend on the hash.
+
+constexpr unsigned long long kDedupEmpty = ~0ull;
+
+struct DedupTable {
+  unsigned long long *hash;  // [size], kDedupEmpty = free
+  uint32_t *pos;             // [size] largest batch position with that hash
+  uint64_t mask;             // size - 1 (size a power of two)
+  uint64_t hmask;            // hash bits kept (narrower only to test collisions)
+};
+
+__device__ __forceinline__ uint64_t dedup_hash(const uint8_t *k, uint32_t len, uint32_t trie, uint64_t hmask) {
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ ((uint64_t)len << 32) ^ trie;
+  uint32_t o = 0;
+  for (; o + 8 <= len; o += 8) {
+    h = (h ^ load_u64_unaligned(k + o)) * 0xFF51AFD7ED558CCDull;
+    h ^= h >> 32;
+  }
+  if (o < len) {
+    h = (h ^ (load_u64_unaligned(k + o) & low_mask64((int)(len - o)))) * 0xC4CEB9FE1A85EC53ull;
+    h ^= h >> 29;
+  }
+  h = (h ^ (h >> 31)) * 0x94D049BB133111EBull;
+  h ^= h >> 32;
+  h &= hmask;
+  return h == kDedupEmpty ? 0ull : h;
+}
+
+__device__ __forceinline__ uint64_t dedup_home(uint64_t h, uint64_t mask) {
+  return ((h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull >> 17) & mask;
+}
+
+__global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
+                               DedupTable t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long h = dedup_hash(tv.keys + koff[i], klen[i], tid ? (uint32_t)tid[i] : 0u, t.hmask);
+  uint64_t s = dedup_home(h, t.mask);
+  for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask) {
+    const unsigned long long old = atomicCAS(&t.hash[s], kDedupEmpty, h);
+    if (old == kDedupEmpty || old == h) {
+      atomicMax(&t.pos[s], (uint32_t)i);
+      return;
+    }
+  }
+}
+
+__global__ void k_dedup_mark(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
+                             DedupTable t, unsigned long long *keep, uint32_t *collision) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
+  const uint8_t *k = tv.keys + koff[i];
+  const uint32_t len = klen[i];
+  const unsigned long long h = dedup_hash(k, len, tr, t.hmask);
+  uint64_t s = dedup_home(h, t.mask);
+  bool found = false;
+  for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask)
+    if (t.hash[s] == h) {
+      found = true;
+      break;
+    }
+  if (!found) {  // cannot happen after k_dedup_insert; walk every key then
+    atomicOr(collision, 1u);
+    keep[i] = 1ull;
+    return;
+  }
+  const uint32_t w = t.pos[s];
+  bool kept = w == (uint32_t)i;
+  if (!kept) {
+    const bool same = klen[w] == len && (tid ? (uint32_t)tid[w] == tr : true) &&
+                      match_nibbles(tv.keys + koff[w], k, (int)len) == (int)len;
+    if (!same) atomicOr(collision, 1u);
+  }
+  keep[i] = kept ? 1ull : 0ull;
+}
+
+__global__ void k_dedup_compact(const unsigned long long *keep, const unsigned long long *pos, int n, uint32_t *sel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && keep[i]) sel[pos[i]] = (uint32_t)i;
 }
 
 }  // namespace gmpt

@@ -29,6 +29,8 @@ constexpr int kHashThreads = 128;
 constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);
 // levels with at most this many branch nodes hash them one warp each
 constexpr int kWarpFullMax = 4096;
+// LockNU batches of at least this many keys drop repeated keys first
+constexpr int kDedupMinKeys = 1 << 16;
 
 inline unsigned blocks_for(int64_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
@@ -98,7 +100,7 @@ Trie::~Trie() {
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
                         &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
-                        &ws_.tid, &ws_.misc};
+                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.misc};
   for (DevBlock *b : blocks) b->release();
   for (int k = 0; k < 2; ++k) {
     ws_.s_start[k].release();
@@ -878,10 +880,40 @@ int Trie::put_latching(const BatchIn &b) {
   if ((rc = sync_counters())) return rc;
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
+  KeySelect ks;
+  if (opt_latch_dedup_ == 2 || (opt_latch_dedup_ == 1 && b.n >= kDedupMinKeys)) {
+    // walk each distinct key once (its last occurrence); see k_dedup_*
+    cudaError_t e = cudaSuccess;
+    uint64_t size = 1024;
+    while (size < 2ull * (uint64_t)b.n) size <<= 1;
+    unsigned long long *hash = wsp<unsigned long long>(ws_.dd_hash, size, e);
+    uint32_t *pos = wsp<uint32_t>(ws_.dd_pos, size, e);
+    uint32_t *sel = wsp<uint32_t>(ws_.dd_sel, (size_t)b.n, e);
+    unsigned long long *keep = wsp<unsigned long long>(ws_.flags, (size_t)b.n, e);
+    unsigned long long *rank = wsp<unsigned long long>(ws_.pos, (size_t)b.n, e);
+    unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+    uint32_t *collision = reinterpret_cast<uint32_t *>(d_tot + 1);
+    if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(b.n));
+    if (e == cudaSuccess) e = cudaMemsetAsync(hash, 0xFF, sizeof(unsigned long long) * size, st_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pos, 0, sizeof(uint32_t) * size, st_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(collision, 0, 4, st_);
+    if (e != cudaSuccess) return check_cuda(e, "dedup alloc");
+    const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
+    DedupTable tab{hash, pos, size - 1, hmask};
+    count_launch(), k_dedup_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab);
+    count_launch(), k_dedup_mark<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab, keep,
+                                                                        collision);
+    if ((e = exclusive_scan<unsigned long long>(keep, rank, b.n, d_tot, scan_ws_, st_)) != cudaSuccess)
+      return check_cuda(e, "dedup scan");
+    count_launch(), k_dedup_compact<<<blocks_for(b.n), kThreads, 0, st_>>>(keep, rank, b.n, sel);
+    ks.sel = sel;
+    ks.count = d_tot;
+    ks.collision = collision;
+  }
   const int ways = opt_latch_ways_;
   auto kern = ways == 1 ? k_latch_insert<1> : (ways == 2 ? k_latch_insert<2> : k_latch_insert<4>);
   count_launch(), kern<<<blocks_for((b.n + ways - 1) / ways), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base,
-                                                                                 1u << 20, tid);
+                                                                                 1u << 20, tid, ks);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
   if ((rc = sync_counters())) return rc;
   if (timing_) {
@@ -1126,6 +1158,16 @@ int Trie::set_option(const std::string &name, int64_t value) {
   if (name == "block_grid") {
     if (value < 0 || value > 1 << 20) return fail(E_ARG, "block_grid must be in [0, 2^20]");
     opt_block_grid_ = (int)value;
+    return OK;
+  }
+  if (name == "latch_dedup") {
+    if (value < 0 || value > 2) return fail(E_ARG, "latch_dedup must be 0, 1 or 2");
+    opt_latch_dedup_ = (int)value;
+    return OK;
+  }
+  if (name == "latch_dedup_bits") {
+    if (value < 1 || value > 64) return fail(E_ARG, "latch_dedup_bits must be in [1, 64]");
+    opt_dedup_bits_ = (int)value;
     return OK;
   }
   if (name == "latch_ways") {

@@ -147,6 +147,8 @@ class Trie {
   bool opt_local_build_ = true;  // finish small build segments in one CTA each
   bool opt_local_sort_ = true;   // finish small tied sort runs in one CTA each
   int opt_latch_ways_ = 4;       // LockNU keys per thread (1, 2, 4)
+  int opt_latch_dedup_ = 1;      // 0 off, 1 batches >= kDedupMinKeys, 2 always
+  int opt_dedup_bits_ = 64;      // hash bits the dedup keeps (fewer only to test collisions)
 
   // node pools (capacities in elements)
   TrieView tv_{};
@@ -200,6 +202,7 @@ class Trie {
     DevBlock bins, cursor, sorted_dirty;                        // hash buckets
     DevBlock g_keys, g_idx, g_hp, g_len, g_tid;                 // gets
     DevBlock tid;                                               // trie ids of the batch
+    DevBlock dd_hash, dd_pos, dd_sel;                           // LockNU batch dedup
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;

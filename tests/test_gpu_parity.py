@@ -270,6 +270,41 @@ def test_pipeline_knobs_do_not_change_results(gpu_lib, local):
         assert t.get_values(b.keys_hexs, b.keys_indexs) == o.gets(b.keys_hexs, b.keys_indexs)
 
 
+@pytest.mark.parametrize("dedup,bits", [(0, 64), (2, 64), (2, 3), (1, 64)])
+def test_locknu_dedup_does_not_change_results(gpu_lib, dedup, bits):
+    # duplicate-heavy LockNU batches with the repeated-key filter off, on, and
+    # on with a 3-bit hash (different keys share hashes: the insert must fall
+    # back to walking every key), forest and single trie
+    load = W.ycsb_load(20000, seed=81)
+    upd = [W.ycsb_zipf_updates(20000, 70000, theta=1.1, seed=82 + k) for k in range(2)]
+    roots, o = oracle_root([load] + upd)
+    t = gpu_lib.MPT()
+    t.set_option("latch_dedup", dedup)
+    t.set_option("latch_dedup_bits", bits)
+    for b, r in zip([load] + upd, roots):
+        t.puts_latching_with_valuehp_v2(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+        t.hash_onepass_v2()
+        assert t.get_root_hash() == r
+    u = upd[-1]
+    assert t.get_values(u.keys_hexs, u.keys_indexs) == o.gets(u.keys_hexs, u.keys_indexs)
+    # the same keys in two tries of a forest must not be merged by the filter
+    f = gpu_lib.MPT(max_tries=2)
+    f.set_option("latch_dedup", dedup)
+    f.set_option("latch_dedup_bits", bits)
+    b = upd[0]
+    tids = (np.arange(b.n) % 2).astype(np.int32)
+    f.puts_forest(False, b.keys_hexs, b.keys_indexs, b.values, b.values_indexs, tids)
+    f.hash_onepass_v2()
+    want = []
+    for tr in (0, 1):
+        ot = O.OracleTrie()
+        sub = b.subset(np.nonzero(tids == tr)[0])
+        ot.puts(sub.keys_hexs, sub.keys_indexs, sub.values, sub.values_indexs)
+        ot.hash()
+        want.append(ot.root())
+    assert f.get_roots(n=2) == want
+
+
 def test_key_streams_with_gaps_between_keys(gpu_lib):
     # index pairs need not tile the key stream; bytes between keys are ignored
     b = W.random_keys(2000, seed=91)
