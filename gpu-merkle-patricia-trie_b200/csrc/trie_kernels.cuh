@@ -1142,9 +1142,11 @@ __global__ void __launch_bounds__(128) k_hash_full_warp(TrieView tv, const uint3
     hash_node<false>(tv, r, stage_all + threadIdx.x, blockDim.x);
 }
 
-// 96 registers (five 128-thread CTAs per SM): the permutation keeps its 25
-// lanes in registers without spilling at this bound.
-__global__ void __launch_bounds__(128, 5) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
+// Six 128-thread CTAs per SM (at most 85 registers): the permutation keeps
+// its 25 lanes in registers; a few encoder temporaries spill, and the extra
+// resident warps hide more of the child / record gathers (measured faster
+// than five CTAs at 96 registers without spills).
+__global__ void __launch_bounds__(128, 6) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
