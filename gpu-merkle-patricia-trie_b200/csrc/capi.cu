@@ -323,6 +323,19 @@ int gmpt_batch_features_device(const uint8_t *d_keys_hexs, const int *d_keys_ind
   return record(rc, err);
 }
 
+int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs, const int *const *keys_indexs,
+                       const uint8_t *const *values_bytes, const int64_t *const *values_indexs,
+                       const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
+                       uint8_t *roots32, int *root_sizes) {
+  if (!t || count < 0 || (count > 0 && (!keys_hexs || !keys_indexs || !values_bytes || !values_indexs || !counts)))
+    return record(GMPT_E_ARG, "null argument");
+  std::vector<gmpt::BatchIn> bs((size_t)count);
+  for (int i = 0; i < count; ++i)
+    bs[i] = host_batch(keys_hexs[i], keys_indexs[i], values_bytes[i], values_indexs[i],
+                       values_hps ? values_hps[i] : nullptr, counts[i]);
+  return record_trie(t->t->puts_pipeline(bs.data(), two_phase, count, roots32, root_sizes), t->t);
+}
+
 int gmpt_hash_onepass(gmpt_trie *t) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(t->t->hash(), t->t);

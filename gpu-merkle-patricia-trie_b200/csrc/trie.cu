@@ -119,6 +119,13 @@ Trie::~Trie() {
     if (c.exec) cudaGraphExecDestroy(c.exec);
     if (c.graph) cudaGraphDestroy(c.graph);
   }
+  for (auto &ps : pipe_) {
+    DevBlock *pb[] = {&ps.keys, &ps.kidx, &ps.vals, &ps.vidx, &ps.hp, &ps.tid};
+    for (DevBlock *b : pb) b->release();
+    if (ps.ready) cudaEventDestroy(ps.ready);
+    if (ps.free) cudaEventDestroy(ps.free);
+  }
+  if (copy_st_) cudaStreamDestroy(copy_st_);
   if (blk_.d_desc) cudaFree(blk_.d_desc);
   if (blk_.h_desc) cudaFreeHost(blk_.h_desc);
   if (h_ctr_) cudaFreeHost(h_ctr_);
@@ -1624,6 +1631,100 @@ int batch_features_device(const uint8_t *d_keys, const int *d_kidx, int n, int64
     return E_CUDA;
   }
   return OK;
+}
+
+}  // namespace gmpt
+
+// ---------------------------------------------------------------------------
+// Host batches with the copy of the next batch overlapping this one's work
+// (the reference's two-stream puts_2phase_pipeline / puts_latching_pipeline_v2,
+// gpu_mpt.cuh:1715-1823 and 926-982).
+
+namespace gmpt {
+
+int Trie::puts_pipeline(const BatchIn *bs, const int *two_phase, int count, uint8_t *roots32, int *sizes) {
+  err_.clear();
+  if (count < 0 || (count > 0 && (!bs || !two_phase || !roots32 || !sizes))) return fail(E_ARG, "null argument");
+  if (count == 0) return OK;
+  cudaSetDevice(dev_);
+  std::vector<int64_t> kb(count), vb(count);
+  int64_t mk = 0, mv = 0;
+  int mn = 0;
+  for (int i = 0; i < count; ++i) {
+    const BatchIn &b = bs[i];
+    if (b.device) return fail(E_ARG, "puts_pipeline takes host batches");
+    if (b.n < 0 || b.n > (1 << 26)) return fail(E_ARG, "batch size must be in [0, 2^26]");
+    if (b.n > 0 && (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs))
+      return fail(E_ARG, "null batch array");
+    kb[i] = b.n ? (int64_t)b.keys_indexs[2 * b.n - 1] + 1 : 0;
+    vb[i] = b.n ? (int64_t)b.values_indexs[2 * b.n - 1] + 1 : 0;
+    if (kb[i] < 0 || vb[i] < 0) return fail(E_ARG, "bad index pairs");
+    mk = std::max(mk, kb[i]);
+    mv = std::max(mv, vb[i]);
+    mn = std::max(mn, b.n);
+  }
+  cudaError_t e = cudaSuccess;
+  if (!copy_st_) e = cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking);
+  for (auto &ps : pipe_) {  // size both slots for the largest batch up front
+    if (e == cudaSuccess && !ps.ready) e = cudaEventCreateWithFlags(&ps.ready, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ps.free) e = cudaEventCreateWithFlags(&ps.free, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = ps.keys.ensure((size_t)mk + 64);
+    if (e == cudaSuccess) e = ps.kidx.ensure(8 * (size_t)std::max(mn, 1));
+    if (e == cudaSuccess) e = ps.vals.ensure((size_t)mv + 64);
+    if (e == cudaSuccess) e = ps.vidx.ensure(16 * (size_t)std::max(mn, 1));
+    if (e == cudaSuccess) e = ps.hp.ensure(8 * (size_t)std::max(mn, 1));
+    if (e == cudaSuccess) e = ps.tid.ensure(4 * (size_t)std::max(mn, 1));
+    if (e == cudaSuccess) e = cudaEventRecord(ps.free, copy_st_);
+  }
+  if (e != cudaSuccess) return check_cuda(e, "pipeline buffers");
+  auto issue = [&](int i) -> cudaError_t {
+    const BatchIn &b = bs[i];
+    PipeSlot &ps = pipe_[i & 1];
+    cudaError_t x = cudaStreamWaitEvent(copy_st_, ps.free, 0);  // its previous batch is staged
+    if (x == cudaSuccess && kb[i]) x = cudaMemcpyAsync(ps.keys.p, b.keys_hexs, (size_t)kb[i], cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess && b.n) x = cudaMemcpyAsync(ps.kidx.p, b.keys_indexs, 8 * (size_t)b.n, cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess && vb[i]) x = cudaMemcpyAsync(ps.vals.p, b.values, (size_t)vb[i], cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess && b.n)
+      x = cudaMemcpyAsync(ps.vidx.p, b.values_indexs, 16 * (size_t)b.n, cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess && b.n && b.values_hps)
+      x = cudaMemcpyAsync(ps.hp.p, b.values_hps, 8 * (size_t)b.n, cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess && b.n && b.trie_ids)
+      x = cudaMemcpyAsync(ps.tid.p, b.trie_ids, 4 * (size_t)b.n, cudaMemcpyHostToDevice, copy_st_);
+    if (x == cudaSuccess) x = cudaEventRecord(ps.ready, copy_st_);
+    return x;
+  };
+  int rc = OK;
+  if ((e = issue(0)) != cudaSuccess) return check_cuda(e, "pipeline copy");
+  for (int i = 0; i < count && rc == OK; ++i) {
+    if (i + 1 < count && (e = issue(i + 1)) != cudaSuccess) {
+      rc = check_cuda(e, "pipeline copy");
+      break;
+    }
+    PipeSlot &ps = pipe_[i & 1];
+    if ((e = cudaStreamWaitEvent(st_, ps.ready, 0)) != cudaSuccess) {
+      rc = check_cuda(e, "pipeline wait");
+      break;
+    }
+    const BatchIn &h = bs[i];
+    BatchIn d;
+    d.keys_hexs = ps.keys.as<uint8_t>();
+    d.keys_indexs = ps.kidx.as<int>();
+    d.values = ps.vals.as<uint8_t>();
+    d.values_indexs = ps.vidx.as<int64_t>();
+    d.values_hps = h.values_hps ? ps.hp.as<uint64_t>() : nullptr;
+    d.trie_ids = h.trie_ids ? ps.tid.as<int>() : nullptr;
+    d.n = h.n;
+    d.keys_bytes = kb[i];
+    d.values_bytes = vb[i];
+    d.device = true;
+    rc = two_phase[i] ? put_2phase(d) : put_latching(d);
+    // the put has copied the slot into the arenas (it synchronises its stream)
+    if ((e = cudaEventRecord(ps.free, st_)) != cudaSuccess && rc == OK) rc = check_cuda(e, "pipeline event");
+    if (rc == OK) rc = hash();
+    if (rc == OK) rc = root(roots32 + 32 * (size_t)i, sizes + i);
+  }
+  cudaStreamSynchronize(copy_st_);
+  return rc;
 }
 
 }  // namespace gmpt

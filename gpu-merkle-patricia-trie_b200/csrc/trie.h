@@ -129,6 +129,10 @@ class Trie {
   // grow the pools and arenas now for n_keys more keys of the given byte
   // totals (no growth stalls, and no block graph rebuild, until then)
   int reserve(uint64_t n_keys, uint64_t key_bytes, uint64_t value_bytes);
+  // Host batches applied in order, each followed by PhaseHC and a root read
+  // (roots32[32 i..], sizes[i]); batch i+1 is copied to the device on a copy
+  // stream while batch i is inserted and hashed.  two_phase[i] picks PhaseNU.
+  int puts_pipeline(const BatchIn *batches, const int *two_phase, int count, uint8_t *roots32, int *sizes);
   // the same with explicit headroom per pool
   int reserve_nodes(uint64_t full, uint64_t shorts, uint64_t values, uint64_t records, uint64_t key_bytes,
                     uint64_t value_bytes);
@@ -188,6 +192,13 @@ class Trie {
   bool opt_block_graph_ = true;  // replay a captured graph (else plain launches)
   int block_launch(bool launch = true);
   int block_buffers(int64_t n, int64_t kb, int64_t vb, int64_t n_out);
+
+  // double-buffered host -> device staging of puts_pipeline
+  struct PipeSlot {
+    DevBlock keys, kidx, vals, vidx, hp, tid;
+    cudaEvent_t ready = nullptr, free = nullptr;
+  } pipe_[2];
+  cudaStream_t copy_st_ = nullptr;
 
   // per-batch workspaces
   struct Ws {

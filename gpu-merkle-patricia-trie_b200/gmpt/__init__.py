@@ -36,7 +36,7 @@ EXPORTS = [
     "gmpt_create_forest", "gmpt_max_tries", "gmpt_puts_2phase_forest", "gmpt_puts_latching_forest",
     "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
-    "gmpt_reserve_nodes", "gmpt_batch_features_device",
+    "gmpt_reserve_nodes", "gmpt_batch_features_device", "gmpt_puts_pipeline",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
@@ -124,6 +124,7 @@ def lib():
     L.gmpt_gen_keys.argtypes = [C.c_uint64, vp, i64, i32, vp, vp, vp]
     L.gmpt_gen_values.argtypes = [C.c_uint64, i64, i32, vp, vp, vp]
     L.gmpt_batch_features_device.argtypes = [vp, vp, i32, i64, vp, vp]
+    L.gmpt_puts_pipeline.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -443,6 +444,31 @@ class MPT:
         _check(self._L.gmpt_gets_forest_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes),
                                                _p(hps), _p(sizes)))
         return hps[:n], sizes[:n]
+
+    def puts_pipeline(self, batches, two_phase, hps=None, raw=None) -> list:
+        """Host batches in order, each inserted, hashed and its root read, the
+        next batch's copy overlapping this one's work.  batches: objects with
+        keys_hexs / keys_indexs / values / values_indexs (numpy), or raw =
+        [(keys_ptr, kidx_ptr, vals_ptr, vidx_ptr, n), ...] host addresses
+        (e.g. pinned tensors)."""
+        if raw is None:
+            arrs = [_arrays(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs) for b in batches]
+            raw = [(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, len(a[1]) // 2)
+                   for a in arrs]
+        k = len(raw)
+        P = C.c_void_p * max(k, 1)
+        cols = [P(*[C.c_void_p(r[j]) for r in raw]) for j in range(4)]
+        hp = None
+        if hps is not None:
+            hp_arrs = [None if h is None else np.ascontiguousarray(h, dtype=np.uint64) for h in hps]
+            hp = P(*[None if h is None else h.ctypes.data_as(C.c_void_p) for h in hp_arrs])
+        counts = np.array([r[4] for r in raw], dtype=np.int32)
+        tp = np.array([1 if x else 0 for x in two_phase], dtype=np.int32)
+        out = np.zeros(32 * max(k, 1), dtype=np.uint8)
+        sizes = np.zeros(max(k, 1), dtype=np.int32)
+        _check(self._L.gmpt_puts_pipeline(self._h, k, cols[0], cols[1], cols[2], cols[3], hp, _p(counts), _p(tp),
+                                          _p(out), _p(sizes)))
+        return [out[32 * i: 32 * i + sizes[i]].tobytes() for i in range(k)]
 
     def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
                     values_bytes: int, d_hps: int = 0):

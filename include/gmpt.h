@@ -195,6 +195,19 @@ int gmpt_gen_values(uint64_t seed, int64_t n, int value_bytes, uint8_t *d_values
 int gmpt_batch_features_device(const uint8_t *d_keys_hexs, const int *d_keys_indexs, int n, int64_t keys_bytes,
                                float out[4], void *stream);
 
+/* A sequence of HOST batches, each inserted (two_phase[i] != 0: PhaseNU,
+ * else LockNU), hashed and its root read (roots32[32 i..], root_sizes[i]),
+ * with the host -> device copy of batch i+1 running on a second stream while
+ * batch i is inserted and hashed (the reference's two-stream pipelines,
+ * puts_2phase_pipeline gpu_mpt.cuh:1715-1823 and puts_latching_pipeline_v2
+ * gpu_mpt.cuh:926-982).  Per-batch arrays as for gmpt_puts_2phase;
+ * values_hps may be NULL (or hold NULL entries).  Copies overlap only from
+ * page-locked host memory. */
+int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs, const int *const *keys_indexs,
+                       const uint8_t *const *values_bytes, const int64_t *const *values_indexs,
+                       const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
+                       uint8_t *roots32, int *root_sizes);
+
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
 int gmpt_hash_onepass(gmpt_trie *t);

@@ -327,3 +327,22 @@ def test_key_streams_with_gaps_between_keys(gpu_lib):
         bad[ki[10] + 5] = 16  # a terminator inside a key
         with pytest.raises(gpu_lib.GmptError):
             f(bad, ki, b.values, b.values_indexs)
+
+
+@pytest.mark.parametrize("strategies", [(1, 0, 0, 1), (0, 0, 1, 1), (1, 1, 1, 1)])
+def test_pipelined_host_batches(gpu_lib, strategies):
+    # next batch's copy overlaps this batch's insert + hash; roots after every
+    # batch, lookups and echoed host pointers must be as if run one by one
+    batches = [W.ycsb_load(30000, seed=201), W.ycsb_zipf_updates(30000, 40000, seed=202),
+               W.vocab_keys(20000, seed=203, vmin=40, vmax=300, vmu=4.5),
+               W.ycsb_zipf_updates(30000, 25000, theta=0.5, seed=204)]
+    roots, o = oracle_root(batches)
+    t = gpu_lib.MPT()
+    hps = [np.arange(b.n, dtype=np.uint64) + 1000 * (k + 1) for k, b in enumerate(batches)]
+    got = t.puts_pipeline(batches, [bool(x) for x in strategies], hps=hps)
+    assert got == roots
+    last = batches[-1]
+    assert t.get_values(last.keys_hexs, last.keys_indexs) == o.gets(last.keys_hexs, last.keys_indexs)
+    h, sizes = t.gets_parallel(last.keys_hexs, last.keys_indexs)
+    # a key's echoed pointer is the one given with the last batch position that wrote it
+    assert np.all(sizes > 0) and np.all(h >= 1000)
