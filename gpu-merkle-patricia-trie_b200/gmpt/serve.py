@@ -146,6 +146,7 @@ class Runner:
 
     def _fill(self, tenants):
         self.tenants = tenants
+        self.tenant_of = {t.tid: t for t in tenants}
         self.count = {t.tid: 0 for t in tenants}
         for t in tenants:  # initial contents, PhaseNU bulk loads
             left = t.initial
@@ -188,14 +189,16 @@ class Runner:
         vmax = max(t.value_bytes for t in self.tenants)
         puts = [r for r in reqs if r.kind == "put"]
         total = sum(r.n for r in puts)
-        kbytes = sum(r.n * (2 * self.tenants[r.tenant].key_bytes + 1 + 8) for r in puts)
-        vbytes = sum(r.n * self.tenants[r.tenant].value_bytes for r in puts)
         big = max([r.n for r in reqs] + [merged_keys, 1])
+        total += 2 * big  # the warm-up puts
+        kbytes = sum(r.n * (2 * self.tenant_of[r.tenant].key_bytes + 1 + 8) for r in puts) + 2 * big * (kmax + 8)
+        vbytes = sum(r.n * self.tenant_of[r.tenant].value_bytes for r in puts) + 2 * big * 16
         # growth of the stream (a new key adds about one short node and a
         # fraction of a branch) plus the per-batch headroom the inserts check
         # for (PhaseNU: 2 branches and 4 short nodes per key of the batch)
         self.mpt.reserve_nodes(total // 2 + 2 * big, total + total // 4 + 4 * big, total + big, total + big,
                                kbytes + big * kmax, vbytes + big * vmax)
+        self.warm(big)
         gets = [r for r in reqs if r.kind == "get"]
         if gets:  # grow the lookup workspaces and result buffers now (read only)
             g = max(gets, key=lambda r: r.n)
@@ -208,17 +211,39 @@ class Runner:
                 self.mpt.reserve_block(big, big * kmax, big * vmax, len(self.tenants))
         self.stage.ensure(big, big * kmax, big * vmax)
 
+    def warm(self, n: int):
+        """Grow every insert workspace for batches of up to n keys: one put of
+        n fresh keys under each strategy into a scratch trie (the forest's
+        last id, outside the tenants), so no timed request pays for growth."""
+        tid = self.mpt_max_tries() - 1
+        if tid in self.tenant_of or n <= 0:
+            return
+        kmax = max(t.key_bytes for t in self.tenants)
+        scratch = Tenant(tid, kmax, 16, 0)
+        self.tenant_of[tid] = scratch
+        self.count[tid] = 0
+        for k in (TU.FIXED_PHASENU, TU.FIXED_LOCKNU):
+            r = Request(-1, "put", tid, n, 0.0, 1.0, 0x5C7A7C4 + k)
+            nn, kb, vb = self.build([r])
+            TU.apply_config(self.mpt, k)
+            s = self.stage
+            self.mpt.puts_forest_device(TU.CONFIGS[k]["two_phase"], s.keys.data_ptr(), s.kidx.data_ptr(),
+                                        s.vals.data_ptr(), s.vidx.data_ptr(), s.tids.data_ptr(), nn, kb, vb)
+            self.mpt.hash_onepass_v2()
+        del self.tenant_of[tid]
+        del self.count[tid]
+
     def build(self, reqs):
         """Generate the merged batch of same-kind requests into the stage."""
         s = self.stage
         torch = s.torch
         n = sum(r.n for r in reqs)
-        kb = sum(r.n * (2 * self.tenants[r.tenant].key_bytes + 1) for r in reqs)
-        vb = sum(r.n * self.tenants[r.tenant].value_bytes for r in reqs) if reqs[0].kind == "put" else 0
+        kb = sum(r.n * (2 * self.tenant_of[r.tenant].key_bytes + 1) for r in reqs)
+        vb = sum(r.n * self.tenant_of[r.tenant].value_bytes for r in reqs) if reqs[0].kind == "put" else 0
         s.ensure(n, kb, max(vb, 1))
         off = koff = voff = 0
         for r in reqs:
-            t = self.tenants[r.tenant]
+            t = self.tenant_of[r.tenant]
             cnt = self.count[t.tid]
             ids = s.ids[off: off + r.n]
             if r.kind == "put":
@@ -350,16 +375,47 @@ class ServeResult:
     service_ms: np.ndarray | None = None  # per request (one-at-a-time server)
 
 
+def _groups(window):
+    """Merge a drained window into forest calls: tenants are independent tries,
+    so requests of different tenants commute; each tenant's requests keep
+    their order.  Repeatedly, every tenant whose next request is of the kind
+    of the oldest pending head contributes its leading run of that kind."""
+    queues = {}
+    for r in window:
+        queues.setdefault(r.tenant, []).append(r)
+    out = []
+    while queues:
+        heads = [q[0] for q in queues.values()]
+        kind = min(heads, key=lambda r: r.i).kind
+        run = []
+        for t in list(queues):
+            q = queues[t]
+            k = 0
+            while k < len(q) and q[k].kind == kind:
+                k += 1
+            run.extend(q[:k])
+            if k == len(q):
+                del queues[t]
+            else:
+                queues[t] = q[k:]
+        out.append(sorted(run, key=lambda r: r.i))
+    return out
+
+
 def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> ServeResult:
     """Live server on a virtual clock.  policy(runner, reqs, n, kb, vb) ->
-    configuration index (its own time is part of the service time)."""
+    configuration index (its own time is part of the service time).  With
+    batching, the requests that arrived while the server was busy are drained
+    and merged by _groups; get_sizes holds each get request's result sizes
+    (None for puts), in request order."""
     lat = np.zeros(len(reqs))
     svc = np.zeros(len(reqs))
     free = 0.0
     busy = 0.0
     groups = 0
     choices = {}
-    gets = []
+    gets = [None] * len(reqs)
+    base = reqs[0].i if reqs else 0
     i = 0
     while i < len(reqs):
         start = max(free, reqs[i].arrival)
@@ -369,14 +425,8 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> Serv
             while j < len(reqs) and reqs[j].arrival <= start and tot + reqs[j].n <= max_keys:
                 tot += reqs[j].n
                 j += 1
-        # runs of same-kind requests, in arrival order
-        a = i
         t = start
-        while a < j:
-            b = a + 1
-            while b < j and reqs[b].kind == reqs[a].kind:
-                b += 1
-            run = reqs[a:b]
+        for run in (_groups(reqs[i:j]) if batching else [[reqs[i]]]):
             n, kb, vb = runner.build(run)
             t0 = time.perf_counter()
             if run[0].kind == "put":
@@ -384,15 +434,18 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> Serv
                 choices[k] = choices.get(k, 0) + 1
                 runner.put(run, k, n, kb, vb)
             else:
-                gets.append(runner.get(n, kb))
+                sizes = runner.get(n, kb)
+                at = 0
+                for r in run:
+                    gets[r.i - base] = sizes[at: at + r.n]
+                    at += r.n
             ms = (time.perf_counter() - t0) * 1e3
             busy += ms
             t += ms / 1e3
             groups += 1
             for r in run:
-                lat[r.i - reqs[0].i] = (t - r.arrival) * 1e3
-                svc[r.i - reqs[0].i] = ms / len(run)
-            a = b
+                lat[r.i - base] = (t - r.arrival) * 1e3
+                svc[r.i - base] = ms / len(run)
         free = t
         i = j
     return ServeResult(lat, busy, sum(r.n for r in reqs), 0, groups, choices, gets, svc)

@@ -135,3 +135,22 @@ def test_keys_to_hexs_fixed_and_ragged_paths_agree_with_per_key_expansion():
             want = nib(kb[pos: pos + ln].tobytes())
             pos += ln
             assert kh[ki[2 * i]: ki[2 * i + 1] + 1].tolist() == want
+
+
+def test_request_groups_keep_each_tenants_order():
+    from gmpt import serve as S
+
+    tenants = S.make_tenants([10, 10, 10, 10])
+    reqs = S.make_stream(5, 200, tenants, 0.5, 10, 100, load_frac=0.2)
+    groups = S._groups(reqs)
+    assert sorted(r.i for g in groups for r in g) == [r.i for r in reqs]
+    for g in groups:
+        assert len({r.kind for r in g}) == 1
+    # per tenant, the order of its requests is unchanged
+    seen = {}
+    for g in groups:
+        for r in g:
+            seen.setdefault(r.tenant, []).append(r.i)
+    for t, order in seen.items():
+        assert order == sorted(order)
+    assert len(groups) < len(reqs)
