@@ -672,9 +672,24 @@ def run_ours(args, world, rank, local):
             t.reset()
             return t.puts_pipeline(None, tp, raw=ptrs)
 
+        # the same batches with raw key bytes (nibbles made on the device)
+        pinned_raw, h2d_raw = [], 0
+        for b in batches:
+            rk, rki = W.hexs_to_keys(b.keys_hexs, b.keys_indexs)
+            arrs = [torch.from_numpy(a).pin_memory() for a in (rk, rki, b.values, b.values_indexs)]
+            pinned_raw.append(arrs)
+            h2d_raw += sum(a.numel() * a.element_size() for a in arrs)
+        ptrs_raw = [(a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr(), a[3].data_ptr(), b.n)
+                    for a, b in zip(pinned_raw, batches)]
+
+        def step_pipelined_raw():
+            t.reset()
+            return t.puts_pipeline(None, tp, raw=ptrs_raw, raw_keys=True)
+
         t.set_timing(False)
         step_host()
         step_pipelined()
+        step_pipelined_raw()
         seq_ms = []
         for _ in range(args.steps):
             t.reset()
@@ -695,21 +710,37 @@ def run_ours(args, world, rank, local):
             z.synchronize()
             e2e_ms.append(a.elapsed_time(z))
             assert r2 == roots_s, "host and device paths disagree"
+        raw_ms = []
+        for _ in range(args.steps):
+            t.reset()
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            z = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r3 = step_pipelined_raw()
+            z.record(stream)
+            z.synchronize()
+            raw_ms.append(a.elapsed_time(z))
+            assert r3 == roots_s, "raw-key and hex-key paths disagree"
         barrier()
         ems = statistics.mean(e2e_ms)
+        rms = statistics.mean(raw_ms)
         if world > 1:
             import torch.distributed as dist
 
-            x = torch.tensor([ems], device=dev)
+            x = torch.tensor([ems, rms], device=dev)
             dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            ems = float(x.item())
+            ems, rms = float(x[0].item()), float(x[1].item())
         e2e = {"value": round(keys_per_step * world / (ems / 1e3) / 1e6, 3), "unit": "Mkeys/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 32 * len(batches),
                "ms_per_step": round(ems, 3),
                "path": "gmpt_puts_pipeline (next batch's H2D overlaps this batch's insert + hash)",
                "no_overlap": {"value": round(keys_per_step * world / (statistics.mean(seq_ms) / 1e3) / 1e6, 3),
                               "ms_per_step": round(statistics.mean(seq_ms), 3),
-                              "path": "one gmpt_puts_* + gmpt_hash_onepass + root read per batch"}}
+                              "path": "one gmpt_puts_* + gmpt_hash_onepass + root read per batch"},
+               "raw_keys": {"value": round(keys_per_step * world / (rms / 1e3) / 1e6, 3),
+                            "ms_per_step": round(rms, 3), "h2d_bytes_per_step": int(h2d_raw),
+                            "path": "gmpt_puts_pipeline_raw (raw key bytes; nibbles made on the device)"}}
 
     line = {
         "metric": "put+root-hash Mkeys/s", "value": round(value, 3), "unit": "Mkeys/s", "n_gpus": world,

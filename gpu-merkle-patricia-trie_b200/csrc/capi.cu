@@ -336,6 +336,42 @@ int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs,
   return record_trie(t->t->puts_pipeline(bs.data(), two_phase, count, roots32, root_sizes), t->t);
 }
 
+int gmpt_puts_pipeline_raw(gmpt_trie *t, int count, const uint8_t *const *keys, const int *const *keys_indexs,
+                           const uint8_t *const *values_bytes, const int64_t *const *values_indexs,
+                           const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
+                           uint8_t *roots32, int *root_sizes) {
+  if (!t || count < 0 || (count > 0 && (!keys || !keys_indexs || !values_bytes || !values_indexs || !counts)))
+    return record(GMPT_E_ARG, "null argument");
+  std::vector<gmpt::BatchIn> bs((size_t)count);
+  for (int i = 0; i < count; ++i) {
+    bs[i] = host_batch(keys[i], keys_indexs[i], values_bytes[i], values_indexs[i],
+                       values_hps ? values_hps[i] : nullptr, counts[i]);
+    bs[i].raw_keys = true;
+  }
+  return record_trie(t->t->puts_pipeline(bs.data(), two_phase, count, roots32, root_sizes), t->t);
+}
+
+int gmpt_puts_raw(gmpt_trie *t, int two_phase, const uint8_t *keys, const int *keys_indexs,
+                  const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                  const int *trie_ids, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  gmpt::BatchIn b = host_batch(keys, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  b.raw_keys = true;
+  return record_trie(two_phase ? t->t->put_2phase(b) : t->t->put_latching(b), t->t);
+}
+
+int gmpt_puts_raw_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys, const int *d_keys_indexs,
+                         const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const uint64_t *d_values_hps,
+                         const int *d_trie_ids, int n, int64_t keys_bytes, int64_t values_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  gmpt::BatchIn b = device_batch(d_keys, d_keys_indexs, d_values_bytes, d_values_indexs, d_values_hps, n, keys_bytes,
+                                 values_bytes);
+  b.trie_ids = d_trie_ids;
+  b.raw_keys = true;
+  return record_trie(two_phase ? t->t->put_2phase(b) : t->t->put_latching(b), t->t);
+}
+
 int gmpt_hash_onepass(gmpt_trie *t) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(t->t->hash(), t->t);

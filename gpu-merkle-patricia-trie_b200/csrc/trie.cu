@@ -100,7 +100,7 @@ Trie::~Trie() {
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
                         &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
-                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.misc};
+                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.misc};
   for (DevBlock *b : blocks) b->release();
   for (int k = 0; k < 2; ++k) {
     ws_.s_start[k].release();
@@ -276,18 +276,38 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
                 uint32_t *maxlen, const int **tid_out) {
   const int n = b.n;
   cudaError_t e = cudaSuccess;
+  const cudaMemcpyKind kind = b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   int64_t kbytes = b.keys_bytes, vbytes = b.values_bytes;
   if (kbytes < 0 || vbytes < 0) {
     if (b.device) return fail(E_ARG, "device batches must give keys_bytes and values_bytes");
     kbytes = (int64_t)b.keys_indexs[2 * n - 1] + 1;
     vbytes = (int64_t)b.values_indexs[2 * n - 1] + 1;
   }
+  const int64_t raw_bytes = b.raw_keys ? kbytes : 0;
+  unsigned long long *raw_pos = nullptr;
+  if (b.raw_keys) {
+    // pass 1: hex length of every key (pairs may overlap, so the expanded
+    // stream is sized by a scan, not by the raw byte count)
+    int *ki = wsp<int>(ws_.ki, 2 * (size_t)n, e);
+    unsigned long long *lens = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
+    raw_pos = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
+    unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+    if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ki, b.keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+    if (e != cudaSuccess) return check_cuda(e, "stage raw lengths");
+    count_launch(), k_raw_lens<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, n, raw_bytes, lens);
+    if ((e = exclusive_scan<unsigned long long>(lens, raw_pos, n, d_tot, scan_ws_, st_)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "stage raw scan");
+    kbytes = (int64_t)h_small_[0];
+    if (kbytes >= (1ll << 31)) return fail(E_ARG, "key stream exceeds the int32 index range");
+  }
   int rc = ensure_capacity(2ull * n, 4ull * n, (uint64_t)n, (uint64_t)n, (uint64_t)kbytes, (uint64_t)vbytes);
   if (rc) return rc;
   key_base = key_used_;
   vid_base = n_rec_;
   uint64_t val_base = val_used_;
-  cudaMemcpyKind kind = b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   uint8_t *karena = const_cast<uint8_t *>(tv_.keys);
   uint8_t *varena = const_cast<uint8_t *>(tv_.vals);
   int *ki = wsp<int>(ws_.ki, 2 * (size_t)n, e);
@@ -295,13 +315,24 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   uint64_t *hp = b.values_hps ? wsp<uint64_t>(ws_.hp, (size_t)n, e) : nullptr;
   *koff = wsp<uint64_t>(ws_.koff, (size_t)n, e);
   *klen = wsp<uint32_t>(ws_.klen, (size_t)n, e);
-  uint32_t *d_max = wsp<uint32_t>(ws_.misc, 16, e);
+  uint32_t *d_max = wsp<uint32_t>(ws_.misc, 32, e);  // same block size as the scan totals
   int *tid = b.trie_ids ? wsp<int>(ws_.tid, (size_t)n, e) : nullptr;
   if (e != cudaSuccess) return check_cuda(e, "stage alloc");
   *tid_out = tid;
-  e = cudaMemcpyAsync(karena + key_base, b.keys_hexs, (size_t)kbytes, kind, st_);
+  if (b.raw_keys) {
+    // pass 2: nibbles + terminator written straight into the arena (device
+    // batches are read where they lie; host bytes cross once)
+    const uint8_t *raw = b.device ? b.keys_hexs : wsp<uint8_t>(ws_.raw, (size_t)raw_bytes + 8, e);
+    if (e == cudaSuccess && raw_bytes && !b.device)
+      e = cudaMemcpyAsync(const_cast<uint8_t *>(raw), b.keys_hexs, (size_t)raw_bytes, kind, st_);
+    if (e != cudaSuccess) return check_cuda(e, "stage raw keys");
+    count_launch(), k_raw_expand<<<blocks_for(n), kThreads, 0, st_>>>(raw, ki, raw_pos, n, raw_bytes,
+                                                                     karena + key_base);
+  } else {
+    e = cudaMemcpyAsync(karena + key_base, b.keys_hexs, (size_t)kbytes, kind, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ki, b.keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(varena + val_base, b.values, (size_t)vbytes, kind, st_);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ki, b.keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(vi, b.values_indexs, sizeof(int64_t) * 2 * (size_t)n, kind, st_);
   if (e == cudaSuccess && hp) e = cudaMemcpyAsync(hp, b.values_hps, sizeof(uint64_t) * (size_t)n, kind, st_);
   if (e == cudaSuccess && tid) e = cudaMemcpyAsync(tid, b.trie_ids, sizeof(int) * (size_t)n, kind, st_);
@@ -311,7 +342,7 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if ((e = cudaMemsetAsync(&ctr_->stream_terms, 0, 24, st_)) != cudaSuccess) return check_cuda(e, "stage reset");
   count_launch(), k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
                                                 *koff, *klen, d_max, tid);
-  if (kbytes > 0)
+  if (kbytes > 0 && !b.raw_keys)  // expanded raw keys are well formed by construction
     count_launch(), k_stage_stream<<<std::min<unsigned>(blocks_for(kbytes / 8 + 1), 148 * 8), kThreads, 0, st_>>>(
         tv_, karena + key_base, kbytes);
   e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_);
@@ -319,7 +350,9 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "stage");
   *maxlen = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
-  if (h_ctr_->noncontig) {
+  if (b.raw_keys) {
+    // nothing to check beyond k_raw_lens (errors come back with the counters)
+  } else if (h_ctr_->noncontig) {
     // index pairs do not tile the stream: check every key's interior
     count_launch(), k_stage_keys<<<blocks_for(n), kThreads, 0, st_>>>(tv_, *koff, *klen, n);
   } else if (h_ctr_->bad_byte || h_ctr_->stream_terms != h_ctr_->key_terms) {
@@ -1717,6 +1750,7 @@ int Trie::puts_pipeline(const BatchIn *bs, const int *two_phase, int count, uint
     d.keys_bytes = kb[i];
     d.values_bytes = vb[i];
     d.device = true;
+    d.raw_keys = h.raw_keys;
     rc = two_phase[i] ? put_2phase(d) : put_latching(d);
     // the put has copied the slot into the arenas (it synchronises its stream)
     if ((e = cudaEventRecord(ps.free, st_)) != cudaSuccess && rc == OK) rc = check_cuda(e, "pipeline event");

@@ -35,6 +35,8 @@ struct BatchIn {
   int64_t keys_bytes = -1;    // total key stream bytes (derived if < 0, host only)
   int64_t values_bytes = -1;  // total value stream bytes
   bool device = false;        // pointers are device memory
+  bool raw_keys = false;      // keys_hexs holds raw key bytes, keys_indexs byte ranges
+                              // (expanded to nibbles + terminator on the device)
 };
 
 // One persistent two-stage update of a forest (Trie::block_update): keys
@@ -214,6 +216,7 @@ class Trie {
     DevBlock g_keys, g_idx, g_hp, g_len, g_tid;                 // gets
     DevBlock tid;                                               // trie ids of the batch
     DevBlock dd_hash, dd_pos, dd_sel;                           // LockNU batch dedup
+    DevBlock raw;                                               // raw key bytes of the batch
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;

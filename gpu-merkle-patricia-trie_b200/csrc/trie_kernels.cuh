@@ -152,6 +152,45 @@ __global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uin
   tv.rec_hp[vid] = hp ? hp[i] : 0ull;
 }
 
+// Raw key bytes (the caller skips the hex conversion, util/utils.cuh:340-349
+// key_bytes_to_hex).  A pair (s, e) is a key of e - s + 1 bytes, e = s - 1
+// the empty key; its hex form is 2 * bytes + 1 nibbles.
+__device__ __forceinline__ int raw_key_len(const int *ki, int i, int64_t raw_bytes) {
+  const int s = ki[2 * i], e = ki[2 * i + 1];
+  const bool bad = s < 0 || e < s - 1 || (int64_t)e >= raw_bytes || 2ll * (e - s + 1) + 1 > kMaxKeyNibbles;
+  return bad ? -1 : e - s + 1;
+}
+
+// Hex length of every key into flags (for the offset scan); a malformed pair
+// sets ERR_BAD_KEY and counts as the empty key so later stages stay in bounds.
+__global__ void k_raw_lens(TrieView tv, const int *ki, int n, int64_t raw_bytes, unsigned long long *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int len = raw_key_len(ki, i, raw_bytes);
+  if (len < 0) set_error(tv.ctr, ERR_BAD_KEY);
+  flags[i] = 2ull * (uint64_t)max(len, 0) + 1ull;
+}
+
+// Expand key i to nibbles (high, low per byte) + terminator 16 at hex offset
+// pos[i] of `out`, and rewrite its index pair (in place) to the hex range.
+__global__ void k_raw_expand(const uint8_t *raw, int *ki, const unsigned long long *pos, int n, int64_t raw_bytes,
+                             uint8_t *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int len = max(raw_key_len(ki, i, raw_bytes), 0);
+  const int s = ki[2 * i];
+  const uint64_t p = pos[i];
+  uint8_t *o = out + p;
+  for (int b = 0; b < len; ++b) {
+    const uint8_t x = raw[s + b];
+    o[2 * b] = x >> 4;
+    o[2 * b + 1] = x & 15;
+  }
+  o[2 * len] = 16;
+  ki[2 * i] = (int)p;
+  ki[2 * i + 1] = (int)(p + 2 * (uint64_t)len);
+}
+
 // Coalesced check of a key stream that the index pairs tile: no byte > 16,
 // and exactly as many 16s as keys that end in one (so none is interior).
 __global__ void k_stage_stream(TrieView tv, const uint8_t *stream, int64_t nbytes) {

@@ -37,6 +37,7 @@ EXPORTS = [
     "gmpt_get_roots", "gmpt_gets_forest", "gmpt_block_update", "gmpt_block_update_device", "gmpt_block_info",
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
     "gmpt_reserve_nodes", "gmpt_batch_features_device", "gmpt_puts_pipeline",
+    "gmpt_puts_raw", "gmpt_puts_raw_device", "gmpt_puts_pipeline_raw",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
@@ -125,6 +126,9 @@ def lib():
     L.gmpt_gen_values.argtypes = [C.c_uint64, i64, i32, vp, vp, vp]
     L.gmpt_batch_features_device.argtypes = [vp, vp, i32, i64, vp, vp]
     L.gmpt_puts_pipeline.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.gmpt_puts_pipeline_raw.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.gmpt_puts_raw.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32]
+    L.gmpt_puts_raw_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32, i64, i64]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
     for f in ("gmpt_puts_2phase", "gmpt_puts_latching"):
@@ -445,12 +449,31 @@ class MPT:
                                                _p(hps), _p(sizes)))
         return hps[:n], sizes[:n]
 
-    def puts_pipeline(self, batches, two_phase, hps=None, raw=None) -> list:
+    def puts_raw(self, two_phase: bool, keys, keys_indexs, values, values_indexs, trie_ids=None, hps=None):
+        """Put with RAW key bytes (keys_indexs: inclusive byte ranges, end =
+        start - 1 for the empty key); the device expands them to nibbles +
+        terminator.  Same result as the hex puts on keys_to_hexs of the keys."""
+        k, ki, v, vi = _arrays(keys, keys_indexs, values, values_indexs)
+        n = len(ki) // 2
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        hp_arr = None if hps is None else np.ascontiguousarray(hps, dtype=np.uint64)
+        _check(self._L.gmpt_puts_raw(self._h, 1 if two_phase else 0, _p(k), _p(ki), _p(v), _p(vi),
+                                     None if hp_arr is None else _p(hp_arr), None if tid is None else _p(tid), n))
+
+    def puts_raw_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
+                        values_bytes: int, d_tids: int = 0):
+        """puts_raw with inputs already in HBM (raw device addresses)."""
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_puts_raw_device(self._h, 1 if two_phase else 0, v(d_keys), v(d_kidx), v(d_vals),
+                                            v(d_vidx), None, v(d_tids), int(n), int(keys_bytes), int(values_bytes)))
+
+    def puts_pipeline(self, batches, two_phase, hps=None, raw=None, raw_keys: bool = False) -> list:
         """Host batches in order, each inserted, hashed and its root read, the
         next batch's copy overlapping this one's work.  batches: objects with
         keys_hexs / keys_indexs / values / values_indexs (numpy), or raw =
         [(keys_ptr, kidx_ptr, vals_ptr, vidx_ptr, n), ...] host addresses
-        (e.g. pinned tensors)."""
+        (e.g. pinned tensors).  raw_keys: the key arrays hold raw key bytes
+        (as puts_raw), expanded to nibbles on the device."""
         if raw is None:
             arrs = [_arrays(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs) for b in batches]
             raw = [(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, len(a[1]) // 2)
@@ -466,8 +489,8 @@ class MPT:
         tp = np.array([1 if x else 0 for x in two_phase], dtype=np.int32)
         out = np.zeros(32 * max(k, 1), dtype=np.uint8)
         sizes = np.zeros(max(k, 1), dtype=np.int32)
-        _check(self._L.gmpt_puts_pipeline(self._h, k, cols[0], cols[1], cols[2], cols[3], hp, _p(counts), _p(tp),
-                                          _p(out), _p(sizes)))
+        f = self._L.gmpt_puts_pipeline_raw if raw_keys else self._L.gmpt_puts_pipeline
+        _check(f(self._h, k, cols[0], cols[1], cols[2], cols[3], hp, _p(counts), _p(tp), _p(out), _p(sizes)))
         return [out[32 * i: 32 * i + sizes[i]].tobytes() for i in range(k)]
 
     def puts_device(self, two_phase: bool, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,

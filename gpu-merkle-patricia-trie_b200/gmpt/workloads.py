@@ -174,6 +174,30 @@ def keys_to_hexs(key_bytes: np.ndarray, key_lens: np.ndarray):
     return out, idx.astype(np.int32)
 
 
+def hexs_to_keys(keys_hexs: np.ndarray, keys_indexs: np.ndarray):
+    """Inverse of keys_to_hexs for terminated keys of whole bytes: (raw key
+    bytes back to back, int32 inclusive byte pairs) for gmpt_puts_raw."""
+    ki = np.asarray(keys_indexs, dtype=np.int64).reshape(-1, 2)
+    n = len(ki)
+    nib = ki[:, 1] - ki[:, 0]  # nibbles before the terminator
+    if n == 0:
+        return np.zeros(0, dtype=np.uint8), np.zeros(0, dtype=np.int32)
+    if np.any(nib % 2) or np.any(keys_hexs[ki[:, 1]] != 16):
+        raise ValueError("keys must be whole bytes with a terminator")
+    lens = nib // 2
+    offs = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=offs[1:])
+    kid = np.repeat(np.arange(n, dtype=np.int64), lens)
+    within = np.arange(int(offs[-1]), dtype=np.int64) - offs[kid]
+    src = ki[kid, 0] + 2 * within
+    kh = np.asarray(keys_hexs, dtype=np.uint8)
+    out = ((kh[src] << 4) | kh[src + 1]).astype(np.uint8)
+    idx = np.empty(2 * n, dtype=np.int32)
+    idx[0::2] = offs[:-1]
+    idx[1::2] = offs[1:] - 1
+    return out, idx
+
+
 def fixed_values(rng: Xoshiro256ss, n: int, size: int):
     vb = rng.bytes(n * size)
     vi = np.empty(2 * n, dtype=np.int64)

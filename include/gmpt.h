@@ -208,6 +208,30 @@ int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs,
                        const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
                        uint8_t *roots32, int *root_sizes);
 
+/* ---- raw-key batches ----
+ * The reference's callers convert every key to hex nibbles on the host
+ * (test/experiments.cu:50-73 keys_bytes_to_hexs over util/utils.cuh:340-349
+ * key_bytes_to_hex) and pass the nibble stream to the puts above.  These take the
+ * raw key bytes instead: keys_indexs[2 i], [2 i + 1] is the inclusive byte
+ * range of key i (end = start - 1 for the empty key), and the device writes
+ * nibbles (high, low per byte) plus terminator 16 straight into the trie's
+ * key arena.  Results are identical to the hex puts on key_bytes_to_hex of
+ * the same keys; the key stream crosses PCIe at half the size.  two_phase
+ * picks PhaseNU (1) or LockNU (0); trie_ids may be NULL (trie 0).  No
+ * counterpart in the reference. */
+int gmpt_puts_raw(gmpt_trie *t, int two_phase, const uint8_t *keys, const int *keys_indexs,
+                  const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                  const int *trie_ids, int n);
+/* gmpt_puts_raw with DEVICE arrays (read in place; keys_bytes = raw key bytes). */
+int gmpt_puts_raw_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys, const int *d_keys_indexs,
+                         const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const uint64_t *d_values_hps,
+                         const int *d_trie_ids, int n, int64_t keys_bytes, int64_t values_bytes);
+/* gmpt_puts_pipeline with raw-key host batches. */
+int gmpt_puts_pipeline_raw(gmpt_trie *t, int count, const uint8_t *const *keys, const int *const *keys_indexs,
+                           const uint8_t *const *values_bytes, const int64_t *const *values_indexs,
+                           const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
+                           uint8_t *roots32, int *root_sizes);
+
 /* hash_onepass_v2 (gpu_mpt.cuh:131, 1162-1191): PhaseHC over every node made
  * dirty since the last call. */
 int gmpt_hash_onepass(gmpt_trie *t);

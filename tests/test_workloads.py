@@ -1,5 +1,6 @@
 """Seeded synthetic workloads: deterministic and of the stated shapes."""
 import numpy as np
+import pytest
 
 from gmpt import workloads as W
 
@@ -154,3 +155,15 @@ def test_request_groups_keep_each_tenants_order():
     for t, order in seen.items():
         assert order == sorted(order)
     assert len(groups) < len(reqs)
+
+
+def test_hexs_to_keys_inverts_keys_to_hexs():
+    rng = np.random.default_rng(11)
+    for lens in (np.full(50, 23), rng.integers(0, 9, 200)):
+        kb = rng.integers(0, 256, int(lens.sum()), dtype=np.uint8)
+        kh, ki = W.keys_to_hexs(kb, lens)
+        raw, ri = W.hexs_to_keys(kh, ki)
+        assert np.array_equal(raw, kb)
+        assert np.array_equal(ri[1::2] - ri[0::2] + 1, lens)
+    with pytest.raises(ValueError):
+        W.hexs_to_keys(np.array([1, 2, 3, 16], np.uint8), np.array([0, 3], np.int32))
