@@ -372,6 +372,50 @@ int gmpt_puts_raw_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys, con
   return record_trie(two_phase ? t->t->put_2phase(b) : t->t->put_latching(b), t->t);
 }
 
+static int puts_with_read(gmpt_trie *t, bool two_phase, const gmpt::BatchIn &b, const uint8_t *rw_flags,
+                          uint64_t *read_hps, int *read_sizes, int *read_num) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (!read_num || (b.n > 0 && (!rw_flags || !read_hps || !read_sizes))) return record(GMPT_E_ARG, "null argument");
+  return record_trie(t->t->put_rw(b, rw_flags, two_phase, read_hps, read_sizes, read_num), t->t);
+}
+
+int gmpt_puts_latching_with_read(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int *read_num,
+                                 const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                                 const uint8_t *const *values_hps, int n, const uint8_t **read_values_hps,
+                                 int *read_values_sizes) {
+  return puts_with_read(t, false, host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n),
+                        rw_flags, reinterpret_cast<uint64_t *>(read_values_hps), read_values_sizes, read_num);
+}
+
+int gmpt_puts_2phase_with_read(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int *read_num,
+                               const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                               const uint8_t *const *values_hps, int n, const uint8_t **read_values_hps,
+                               int *read_values_sizes) {
+  return puts_with_read(t, true, host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n),
+                        rw_flags, reinterpret_cast<uint64_t *>(read_values_hps), read_values_sizes, read_num);
+}
+
+int gmpt_puts_with_read_forest(gmpt_trie *t, int two_phase, const uint8_t *keys_hexs, const int *keys_indexs,
+                               const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                               const uint8_t *const *values_hps, const int *trie_ids, int n,
+                               const uint8_t **read_values_hps, int *read_values_sizes, int *read_num) {
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  return puts_with_read(t, two_phase != 0, b, rw_flags, reinterpret_cast<uint64_t *>(read_values_hps),
+                        read_values_sizes, read_num);
+}
+
+int gmpt_puts_with_read_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                               const uint8_t *d_rw_flags, const uint8_t *d_values_bytes,
+                               const int64_t *d_values_indexs, const uint64_t *d_values_hps, const int *d_trie_ids,
+                               int n, int64_t keys_bytes, int64_t values_bytes, uint64_t *d_read_values_hps,
+                               int *d_read_values_sizes, int *read_num) {
+  gmpt::BatchIn b = device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs, d_values_hps, n,
+                                 keys_bytes, values_bytes);
+  b.trie_ids = d_trie_ids;
+  return puts_with_read(t, two_phase != 0, b, d_rw_flags, d_read_values_hps, d_read_values_sizes, read_num);
+}
+
 int gmpt_hash_onepass(gmpt_trie *t) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(t->t->hash(), t->t);

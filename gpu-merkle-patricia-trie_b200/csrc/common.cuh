@@ -32,6 +32,7 @@ enum : uint32_t {
   ERR_INTERNAL = 1u << 4,
   ERR_BAD_TRIE = 1u << 5,      // trie id outside [0, number of tries)
   ERR_BARRIER = 1u << 6,       // a grid barrier wait gave up (persistent launch)
+  ERR_BAD_FLAG = 1u << 7,      // read/write flag other than 0 (read) or 1 (write)
 };
 
 // Where a new subtree gets linked: a branch child slot, or the root word of

@@ -163,6 +163,7 @@ int Trie::apply_counters() {
     if (err & ERR_KEY_TOO_LONG) return fail(E_BAD_KEY, "key longer than the supported maximum");
     if (err & ERR_BAD_TRIE) return fail(E_ARG, "trie id outside [0, max_tries)");
     if (err & ERR_BARRIER) return fail(E_INTERNAL, "grid barrier wait gave up");
+    if (err & ERR_BAD_FLAG) return fail(E_ARG, "read/write flag other than 0 (read) or 1 (write)");
     if (err & ERR_BAD_KEY)
       return fail(E_BAD_KEY, "malformed key: nibble > 16, terminator not last, or a key that is a prefix of another");
     return fail(E_INTERNAL, "internal consistency check failed");
@@ -428,6 +429,7 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
     stats_.sort_passes += passes;
     count_launch(), k_sort_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act, skey, sval, K, order, eqprev);
   }
+  if (rw_) return resolve_rw(n, order, eqprev, koff, klen, tid, uord_out, m_out);
   count_launch(), k_keep_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
   if (e == cudaSuccess) count_launch(), k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, order, n, uord);
@@ -437,6 +439,48 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   *m_out = (int)(h_small_[0] & 0xFFFFFFFFu);
   *uord_out = uord;
   return OK;
+}
+
+// Mixed read/write batch after the sort: answer every read (k_rw_resolve)
+// and keep the last write of every run, in sorted order, as uord[0..m).
+int Trie::resolve_rw(int n, const uint32_t *order, const uint8_t *eqprev, const uint64_t *koff,
+                     const uint32_t *klen, const int *tid, uint32_t **uord_out, int *m_out) {
+  cudaError_t e = cudaSuccess;
+  unsigned long long *A = wsp<unsigned long long>(ws_.rw_a, (size_t)n, e);  // is_write, then is_read
+  unsigned long long *wrank = wsp<unsigned long long>(ws_.rw_b, (size_t)n, e);
+  unsigned long long *head = wsp<unsigned long long>(ws_.rw_c, (size_t)n, e);
+  unsigned long long *hbefore = wsp<unsigned long long>(ws_.rw_d, (size_t)n, e);
+  unsigned long long *rrank = wsp<unsigned long long>(ws_.rw_e, (size_t)n, e);
+  uint32_t *wpos = wsp<uint32_t>(ws_.rw_wpos, (size_t)n, e);
+  unsigned long long *keep = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
+  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)n, e);
+  unsigned long long *tot = wsp<unsigned long long>(ws_.rw_tot, 8, e);  // writes, heads, reads, kept
+  if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
+  if (e == cudaSuccess) e = cudaMemsetAsync(tot, 0, 64, st_);  // tot[4]: LockNU's (unused) collision word
+  if (e != cudaSuccess) return check_cuda(e, "rw alloc");
+  count_launch(), k_rw_sorted_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, order, rw_->flags, n, A, head);
+  if ((e = exclusive_scan<unsigned long long>(A, wrank, n, tot + 0, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "rw scan");
+  count_launch(), k_rw_wpos<<<blocks_for(n), kThreads, 0, st_>>>(A, wrank, n, wpos);
+  if ((e = exclusive_scan<unsigned long long>(head, hbefore, n, tot + 1, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "rw scan");
+  count_launch(), k_rw_read_flags<<<blocks_for(n), kThreads, 0, st_>>>(tv_, rw_->flags, n, A);
+  if ((e = exclusive_scan<unsigned long long>(A, rrank, n, tot + 2, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "rw scan");
+  count_launch(), k_rw_resolve<<<blocks_for(n), kThreads, 0, st_>>>(tv_, order, rw_->flags, head, hbefore, wrank, wpos,
+                                                                     tot + 0, rrank, koff, klen, tid, rw_->vid_base, n,
+                                                                     rw_->hp, rw_->len, keep);
+  if ((e = exclusive_scan<unsigned long long>(keep, pos, n, tot + 3, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "rw scan");
+  count_launch(), k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(keep, pos, order, n, uord);
+  if ((e = cudaMemcpyAsync(h_small_, tot, 32, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "rw resolve");
+  rw_->reads = h_small_[2];
+  *m_out = (int)h_small_[3];
+  *uord_out = uord;
+  return sync_counters();  // a bad flag rejects the batch before any insert
 }
 
 // Level-synchronous construction over the T sorted items in ws_.sb_*.
@@ -548,10 +592,16 @@ int Trie::put_2phase(const BatchIn &b) {
   const int n = b.n;
   uint32_t *uord;
   int m = 0;
+  if (rw_) rw_->vid_base = vid_base;
   if ((rc = sort_unique(n, koff, klen, maxlen, tid, &uord, &m))) return rc;
   stats_.last_unique = (uint64_t)m;
   if (timing_) cudaEventRecord(ev[2], st_);
   cudaError_t e = cudaSuccess;
+  if (m == 0) {  // a mixed batch of reads only
+    if (timing_)
+      for (auto &x : ev) cudaEventDestroy(x);
+    return sync_counters();
+  }
 
   if (empty_) {
     // bulk load: one group (the root), items already sorted, no walk
@@ -921,7 +971,23 @@ int Trie::put_latching(const BatchIn &b) {
   if (timing_) cudaEventRecord(ev[1], st_);
   DirtyList dl{dirty_ref_, dirty_depth_};
   KeySelect ks;
-  if (opt_latch_dedup_ == 2 || (opt_latch_dedup_ == 1 && b.n >= kDedupMinKeys)) {
+  if (rw_) {
+    // mixed batch: the sort answers the reads and selects the last write of
+    // every key (in key order) for the insert
+    rw_->vid_base = vid_base;
+    uint32_t *uord;
+    int m = 0;
+    if ((rc = sort_unique(b.n, koff, klen, maxlen, tid, &uord, &m))) return rc;
+    if ((rc = sync_counters())) return rc;
+    if (m == 0) {
+      if (timing_)
+        for (auto &x : ev) cudaEventDestroy(x);
+      return OK;
+    }
+    ks.sel = uord;
+    ks.count = ws_.rw_tot.as<unsigned long long>() + 3;
+    ks.collision = reinterpret_cast<const uint32_t *>(ws_.rw_tot.as<unsigned long long>() + 4);  // zeroed
+  } else if (opt_latch_dedup_ == 2 || (opt_latch_dedup_ == 1 && b.n >= kDedupMinKeys)) {
     // walk each distinct key once (its last occurrence); see k_dedup_*
     cudaError_t e = cudaSuccess;
     uint64_t size = 1024;
@@ -1674,6 +1740,38 @@ int batch_features_device(const uint8_t *d_keys, const int *d_kidx, int n, int64
 // gpu_mpt.cuh:1715-1823 and 926-982).
 
 namespace gmpt {
+
+int Trie::put_rw(const BatchIn &b, const uint8_t *rw, bool two_phase, uint64_t *read_hps, int *read_sizes,
+                 int *read_num) {
+  err_.clear();
+  if (b.n < 0 || b.n > (1 << 26)) return fail(E_ARG, "batch size must be in [0, 2^26]");
+  if (read_num) *read_num = 0;
+  if (b.n == 0) return OK;
+  if (!rw || !read_hps || !read_sizes || !read_num) return fail(E_ARG, "null argument");
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  const size_t n = (size_t)b.n;
+  RwState st;
+  st.flags = wsp<uint8_t>(ws_.rw_flags, n, e);
+  st.hp = b.device ? read_hps : wsp<uint64_t>(ws_.rw_hp, n, e);
+  st.len = b.device ? read_sizes : wsp<int>(ws_.rw_len, n, e);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(const_cast<uint8_t *>(st.flags), rw, n,
+                        b.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_);
+  if (e != cudaSuccess) return check_cuda(e, "rw flags");
+  rw_ = &st;
+  int rc = two_phase ? put_2phase(b) : put_latching(b);
+  rw_ = nullptr;
+  if (rc) return rc;
+  *read_num = (int)st.reads;
+  if (!b.device && st.reads) {
+    e = cudaMemcpyAsync(read_hps, st.hp, 8 * st.reads, cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(read_sizes, st.len, 4 * st.reads, cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+    if (e != cudaSuccess) return check_cuda(e, "rw results");
+  }
+  return OK;
+}
 
 int Trie::puts_pipeline(const BatchIn *bs, const int *two_phase, int count, uint8_t *roots32, int *sizes) {
   err_.clear();

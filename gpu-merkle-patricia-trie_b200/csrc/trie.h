@@ -92,6 +92,13 @@ class Trie {
 
   int put_2phase(const BatchIn &b);
   int put_latching(const BatchIn &b);
+  // Mixed read/write batch: rw[i] = 0 reads key i, 1 writes it (rw host or
+  // device as b.device).  Applied as if in index order: a read sees the last
+  // earlier write of its key in the batch, else the trie before the batch.
+  // Read i's result lands at its rank among the reads: read_hps / read_sizes
+  // (host arrays, or device arrays when b.device), *read_num = reads.
+  int put_rw(const BatchIn &b, const uint8_t *rw, bool two_phase, uint64_t *read_hps, int *read_sizes,
+             int *read_num);
   int hash();
   int root(uint8_t out[32], int *len, int trie = 0);
   // roots of tries ids[0..n) (host array; null = tries 0..n-1): out32[32 i..]
@@ -217,11 +224,23 @@ class Trie {
     DevBlock tid;                                               // trie ids of the batch
     DevBlock dd_hash, dd_pos, dd_sel;                           // LockNU batch dedup
     DevBlock raw;                                               // raw key bytes of the batch
+    DevBlock rw_flags, rw_a, rw_b, rw_c, rw_d, rw_e, rw_wpos;   // mixed read/write resolution
+    DevBlock rw_hp, rw_len, rw_tot;
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;
   DevBlock scan_ws_;
   uint64_t *h_small_ = nullptr;  // pinned scratch for small readbacks
+  // set by put_rw for the duration of one put: sort_unique then resolves the
+  // reads and keeps the last write of every key
+  struct RwState {
+    const uint8_t *flags = nullptr;  // device, batch order
+    uint64_t *hp = nullptr;          // device, read rank order
+    int *len = nullptr;
+    uint64_t vid_base = 0;
+    uint64_t reads = 0;              // out
+  };
+  RwState *rw_ = nullptr;
 
   int fail(int code, const std::string &msg);
   int check_cuda(cudaError_t e, const char *what);
@@ -232,6 +251,8 @@ class Trie {
                       uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact = false);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
+  int resolve_rw(int n, const uint32_t *order, const uint8_t *eqprev, const uint64_t *koff, const uint32_t *klen,
+                 const int *tid, uint32_t **uord_out, int *m_out);
   int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                   uint32_t **uord, int *m);
   int build_levels(int T);

@@ -301,6 +301,68 @@ __global__ void k_keep_scatter(const unsigned long long *flags, const unsigned l
 }
 
 // ---------------------------------------------------------------------------
+// mixed read/write batches (puts_*_with_read, gpu_mpt.cuh:684-765 and
+// 1609-1713).  The sort leaves equal keys (same trie) in runs, in batch
+// order; p is a sorted position, order[p] its batch index, rw[i] = 1 for a
+// write.  A read takes the last write before it in its run, else the trie
+// as it was before the batch; each run keeps its last write for the insert.
+
+__global__ void k_rw_sorted_flags(const uint8_t *eqprev, const uint32_t *order, const uint8_t *rw, int n,
+                                  unsigned long long *is_write, unsigned long long *is_head) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  is_write[p] = rw[order[p]] ? 1ull : 0ull;
+  is_head[p] = eqprev[p] ? 0ull : 1ull;
+}
+
+__global__ void k_rw_read_flags(TrieView tv, const uint8_t *rw, int n, unsigned long long *is_read) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (rw[i] > 1) set_error(tv.ctr, ERR_BAD_FLAG);
+  is_read[i] = rw[i] ? 0ull : 1ull;
+}
+
+// wpos[k] = sorted position of the k-th write in sorted order
+__global__ void k_rw_wpos(const unsigned long long *is_write, const unsigned long long *wrank, int n, uint32_t *wpos) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (is_write[p]) wpos[wrank[p]] = (uint32_t)p;
+}
+
+__device__ __forceinline__ int64_t lookup(const TrieView &tv, uint32_t root, const uint8_t *kb, uint32_t len);
+
+__global__ void k_rw_resolve(TrieView tv, const uint32_t *order, const uint8_t *rw, const unsigned long long *is_head,
+                             const unsigned long long *heads_before, const unsigned long long *wrank,
+                             const uint32_t *wpos, const unsigned long long *n_writes, const unsigned long long *rrank,
+                             const uint64_t *koff, const uint32_t *klen, const int *tid, uint64_t vid_base, int n,
+                             uint64_t *out_hp, int *out_len, unsigned long long *keep) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const uint32_t i = order[p];
+  // run id of a sorted position: heads up to and including it, minus one
+  auto run = [&](uint32_t q) { return heads_before[q] + is_head[q]; };
+  const unsigned long long k = wrank[p];  // writes before p in sorted order
+  const unsigned long long nw = *n_writes;
+  if (rw[i]) {
+    keep[p] = (k + 1 >= nw || run(wpos[k + 1]) != run(p)) ? 1ull : 0ull;
+    return;
+  }
+  keep[p] = 0ull;
+  int64_t vid = -1;
+  if (k > 0) {
+    const uint32_t q = wpos[k - 1];
+    if (run(q) == run(p)) vid = (int64_t)(vid_base + order[q]);
+  }
+  if (vid < 0) {
+    const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
+    vid = tr < tv.n_tries ? lookup(tv, tv.roots[tr], tv.keys + koff[i], klen[i]) : -1;
+  }
+  const unsigned long long r = rrank[i];
+  out_hp[r] = vid < 0 ? 0ull : tv.rec_hp[vid];
+  out_len[r] = vid < 0 ? 0 : (int)tv.rec_len[vid];
+}
+
+// ---------------------------------------------------------------------------
 // walk (PhaseNU against an existing trie)
 
 enum : uint8_t { W_EXISTS = 0, W_NEW = 1, W_SPLIT = 2, W_ERROR = 3 };

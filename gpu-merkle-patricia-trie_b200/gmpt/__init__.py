@@ -38,6 +38,8 @@ EXPORTS = [
     "gmpt_block_times", "gmpt_reserve", "gmpt_block_timeline", "gmpt_reserve_block",
     "gmpt_reserve_nodes", "gmpt_batch_features_device", "gmpt_puts_pipeline",
     "gmpt_puts_raw", "gmpt_puts_raw_device", "gmpt_puts_pipeline_raw",
+    "gmpt_puts_latching_with_read", "gmpt_puts_2phase_with_read", "gmpt_puts_with_read_forest",
+    "gmpt_puts_with_read_device",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
@@ -128,6 +130,10 @@ def lib():
     L.gmpt_puts_pipeline.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.gmpt_puts_pipeline_raw.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.gmpt_puts_raw.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32]
+    for f in ("gmpt_puts_latching_with_read", "gmpt_puts_2phase_with_read"):
+        getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+    L.gmpt_puts_with_read_forest.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp]
+    L.gmpt_puts_with_read_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, i64, i64, vp, vp, vp]
     L.gmpt_puts_raw_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32, i64, i64]
     L.gmpt_destroy.argtypes = [vp]
     L.gmpt_reset.argtypes = [vp]
@@ -356,6 +362,33 @@ class MPT:
         tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
         f = self._L.gmpt_puts_2phase_forest if two_phase else self._L.gmpt_puts_latching_forest
         _check(f(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), _p(tid), len(ki) // 2))
+
+    def puts_with_read(self, two_phase: bool, keys_hexs, keys_indexs, rw_flags, values, values_indexs,
+                       trie_ids=None, values_hps=None):
+        """Mixed batch (rw_flags[i] 0 = read, 1 = write), applied as if in
+        index order; returns (hps, sizes) of the reads in read order."""
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        n = len(ki) // 2
+        rw = np.ascontiguousarray(rw_flags, dtype=np.uint8)
+        hp = None if values_hps is None else np.ascontiguousarray(values_hps, dtype=np.uint64)
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        out_hp = np.zeros(max(n, 1), dtype=np.uint64)
+        out_len = np.zeros(max(n, 1), dtype=np.int32)
+        cnt = C.c_int(0)
+        _check(self._L.gmpt_puts_with_read_forest(self._h, 1 if two_phase else 0, _p(kh), _p(ki), _p(rw), _p(vb),
+                                                  _p(vi), _p(hp), _p(tid), n, _p(out_hp), _p(out_len),
+                                                  C.byref(cnt)))
+        return out_hp[:cnt.value], out_len[:cnt.value]
+
+    def puts_with_read_device(self, two_phase: bool, d_keys, d_kidx, d_rw, d_vals, d_vidx, n: int, keys_bytes: int,
+                              values_bytes: int, d_out_hp, d_out_len, d_tids: int = 0) -> int:
+        """Mixed batch from device memory; results into device arrays; returns the read count."""
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        cnt = C.c_int(0)
+        _check(self._L.gmpt_puts_with_read_device(self._h, 1 if two_phase else 0, v(d_keys), v(d_kidx), v(d_rw),
+                                                  v(d_vals), v(d_vidx), None, v(d_tids), int(n), int(keys_bytes),
+                                                  int(values_bytes), v(d_out_hp), v(d_out_len), C.byref(cnt)))
+        return cnt.value
 
     def get_roots(self, trie_ids=None, n: int | None = None) -> list:
         """Root bytes of each trie in trie_ids (default: tries 0..n-1)."""

@@ -208,6 +208,42 @@ int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs,
                        const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
                        uint8_t *roots32, int *root_sizes);
 
+/* ---- mixed read/write batches ----
+ * puts_latching_with_valuehp_v2_with_read (gpu_mpt.cuh:684-765) and
+ * puts_2phase_with_valuehp_with_read (gpu_mpt.cuh:1609-1713): rw_flags[i] = 0
+ * (READ_FLAG, util/utils.cuh:26) looks key i up, 1 (WRITE_FLAG) puts it; any
+ * other flag is GMPT_E_ARG.  Every key has a value pair (ignored for reads;
+ * empty pairs allowed).  Deterministic where the reference is not: the batch
+ * acts as if applied in index order -- a read returns the last earlier write
+ * of its key in the batch, else the value before the batch -- and read i's
+ * result is at its rank among the reads (the reference fills read slots in
+ * atomicAdd order, its reads race with the batch's writes).  Results: the
+ * host pointer given with the value (NULL if absent or none was given) and
+ * the size (0 if absent); *read_num = number of reads.  Writes then behave as
+ * gmpt_puts_2phase / gmpt_puts_latching (last write of a key wins) and need
+ * gmpt_hash_onepass like them. */
+int gmpt_puts_latching_with_read(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int *read_num,
+                                 const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                                 const uint8_t *const *values_hps, int n, const uint8_t **read_values_hps,
+                                 int *read_values_sizes);
+int gmpt_puts_2phase_with_read(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, int *read_num,
+                               const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                               const uint8_t *const *values_hps, int n, const uint8_t **read_values_hps,
+                               int *read_values_sizes);
+/* The same over a forest (trie_ids may be NULL: trie 0); two_phase picks
+ * PhaseNU (1) or LockNU (0). */
+int gmpt_puts_with_read_forest(gmpt_trie *t, int two_phase, const uint8_t *keys_hexs, const int *keys_indexs,
+                               const uint8_t *rw_flags, const uint8_t *values_bytes, const int64_t *values_indexs,
+                               const uint8_t *const *values_hps, const int *trie_ids, int n,
+                               const uint8_t **read_values_hps, int *read_values_sizes, int *read_num);
+/* DEVICE inputs and DEVICE result arrays (n entries each; the first
+ * *read_num are written); *read_num is a host int. */
+int gmpt_puts_with_read_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                               const uint8_t *d_rw_flags, const uint8_t *d_values_bytes,
+                               const int64_t *d_values_indexs, const uint64_t *d_values_hps, const int *d_trie_ids,
+                               int n, int64_t keys_bytes, int64_t values_bytes, uint64_t *d_read_values_hps,
+                               int *d_read_values_sizes, int *read_num);
+
 /* ---- raw-key batches ----
  * The reference's callers convert every key to hex nibbles on the host
  * (test/experiments.cu:50-73 keys_bytes_to_hexs over util/utils.cuh:340-349

@@ -54,6 +54,27 @@ class MPT {
     return targets();
   }
 
+  // gpu_mpt.cuh:74-77 / 684-765: mixed batch, rw_flags[i] = 0 read, 1 write;
+  // reads see the batch's earlier writes of their key (index order)
+  std::tuple<const uint32_t *, int> puts_latching_with_valuehp_v2_with_read(
+      const uint8_t *keys_hexs, int *keys_indexs, int &read_num, const uint8_t *rw_flags,
+      const uint8_t *values_bytes, int64_t *values_indexs, const uint8_t **values_hps, int n,
+      const uint8_t **read_values_hps, int *read_values_sizes) {
+    check(gmpt_puts_latching_with_read(t_, keys_hexs, keys_indexs, &read_num, rw_flags, values_bytes, values_indexs,
+                                       values_hps, n, read_values_hps, read_values_sizes));
+    return targets();
+  }
+
+  // gpu_mpt.cuh:105-108 / 1609-1713
+  std::tuple<const uint32_t *, int> puts_2phase_with_valuehp_with_read(
+      const uint8_t *keys_hexs, int *keys_indexs, int &read_num, const uint8_t *rw_flags,
+      const uint8_t *values_bytes, int64_t *values_indexs, const uint8_t **values_hps, int n,
+      const uint8_t **read_values_hps, int *read_values_sizes) {
+    check(gmpt_puts_2phase_with_read(t_, keys_hexs, keys_indexs, &read_num, rw_flags, values_bytes, values_indexs,
+                                     values_hps, n, read_values_hps, read_values_sizes));
+    return targets();
+  }
+
   // gpu_mpt.cuh:131: hashes every pending dirty node (the targets returned by
   // the puts since the last call)
   void hash_onepass_v2(const uint32_t * /*d_hash_nodes*/ = nullptr, int /*n*/ = 0) {
