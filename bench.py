@@ -466,12 +466,12 @@ def run_requests(args, local, dev):
         rn = reps[0]
         res = {}
 
-        def live(name, policy, batching):
+        def live(name, policy, batching, mixed=False):
             rn.reset(tenants)
             if batching:
                 rn.reserve_for(ev, merged_keys=MERGE_KEYS)
             fb0 = sel.fallbacks
-            r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS)
+            r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS, mixed=mixed)
             assert rn.roots() == final, f"{name}: roots differ from the fixed-schedule replicas"
             res[name] = {"mkeys_s": round(r.keys / (r.busy_ms / 1e3) / 1e6, 3),
                          "p50_ms": round(float(np.percentile(r.latency_ms, 50)), 3),
@@ -498,6 +498,8 @@ def run_requests(args, local, dev):
         res["plain_live"]["p99_ms"] = round(float(np.percentile(lat, 99)), 3)
         live("learned_live", learned_policy, False)
         live("learned_batched_live", learned_policy, True)
+        # drained windows with puts and gets as one mixed read/write call
+        live("learned_mixed_live", learned_policy, True, mixed=True)
         # the same arrivals against per-request times of the timing matrix
         choice = {"matrix_fixed_locknu": np.full(len(ev), TU.FIXED_LOCKNU),
                   "matrix_fixed_phasenu": np.full(len(ev), TU.FIXED_PHASENU),
@@ -523,6 +525,9 @@ def run_requests(args, local, dev):
                                                 res["plain_live"]["mkeys_s"], 3)
         res["p99_learned_batched_vs_plain"] = round(res["learned_batched_live"]["p99_ms"] /
                                                     res["plain_live"]["p99_ms"], 3)
+        res["learned_mixed_vs_plain"] = round(res["learned_mixed_live"]["mkeys_s"] / res["plain_live"]["mkeys_s"], 3)
+        res["p99_learned_mixed_vs_plain"] = round(res["learned_mixed_live"]["p99_ms"] /
+                                                  res["plain_live"]["p99_ms"], 3)
         res["roots_bit_exact"] = True
         out["streams"][label] = res
     for r in reps:

@@ -420,6 +420,40 @@ __global__ void k_dedup_mark(TrieView tv, const uint64_t *koff, const uint32_t *
   keep[i] = kept ? 1ull : 0ull;
 }
 
+// Mixed read/write batches: the hash-table slot of every key (k_dedup_insert
+// filled the table) as the sort key of a stable radix sort, which then groups
+// equal keys in batch order.  A key unequal to its slot's representative (a
+// hash collision) sets *collision: the caller sorts by full keys instead.
+__global__ void k_rw_slots(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
+                           DedupTable t, uint64_t *skey, uint32_t *sval, uint32_t *collision) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
+  const uint8_t *k = tv.keys + koff[i];
+  const uint32_t len = klen[i];
+  const unsigned long long h = dedup_hash(k, len, tr, t.hmask);
+  uint64_t s = dedup_home(h, t.mask);
+  bool found = false;
+  for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask)
+    if (t.hash[s] == h) {
+      found = true;
+      break;
+    }
+  if (!found) {
+    atomicOr(collision, 1u);
+    s = 0;
+  } else {
+    const uint32_t w = t.pos[s];
+    if (w != (uint32_t)i) {
+      const bool same = klen[w] == len && (tid ? (uint32_t)tid[w] == tr : true) &&
+                        match_nibbles(tv.keys + koff[w], k, (int)len) == (int)len;
+      if (!same) atomicOr(collision, 1u);
+    }
+  }
+  skey[i] = s;
+  sval[i] = (uint32_t)i;
+}
+
 __global__ void k_dedup_compact(const unsigned long long *keep, const unsigned long long *pos, int n, uint32_t *sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && keep[i]) sel[pos[i]] = (uint32_t)i;

@@ -100,7 +100,10 @@ Trie::~Trie() {
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
                         &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
-                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.misc};
+                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.rw_flags,
+                        &ws_.rw_a, &ws_.rw_b, &ws_.rw_c, &ws_.rw_d, &ws_.rw_e, &ws_.rw_wpos, &ws_.rw_hp,
+                        &ws_.rw_len, &ws_.rw_tot, &ws_.rw_kept, &ws_.rw_koff, &ws_.rw_klen, &ws_.rw_tid,
+                        &ws_.misc};
   for (DevBlock *b : blocks) b->release();
   for (int k = 0; k < 2; ++k) {
     ws_.s_start[k].release();
@@ -369,10 +372,11 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   return OK;
 }
 
-// Lexicographic order of the batch (terminator before nibble 0) with the last
-// occurrence of every key kept: uord[0..m) are batch indices.
-int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
-                      uint32_t **uord_out, int *m_out) {
+// Lexicographic order of keys koff/klen[0..n) (terminator before nibble 0;
+// a forest orders by trie first), stable: order[0..n) are positions, and
+// eqprev[p] = 1 when key p equals key p - 1.
+int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                     uint32_t **order_out, uint8_t **eqprev_out) {
   cudaError_t e = cudaSuccess;
   uint32_t *order = wsp<uint32_t>(ws_.order, (size_t)n, e);
   uint8_t *eqprev = wsp<uint8_t>(ws_.eqprev, (size_t)n + 1, e);
@@ -381,7 +385,6 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   uint32_t *act = wsp<uint32_t>(ws_.act, (size_t)n, e);
   uint64_t *skey = wsp<uint64_t>(ws_.skey, (size_t)n, e);
   uint32_t *sval = wsp<uint32_t>(ws_.sval, (size_t)n, e);
-  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)n, e);
   unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
   if (e != cudaSuccess) return check_cuda(e, "sort alloc");
@@ -429,7 +432,27 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
     stats_.sort_passes += passes;
     count_launch(), k_sort_scatter<<<blocks_for(K), kThreads, 0, st_>>>(act, skey, sval, K, order, eqprev);
   }
-  if (rw_) return resolve_rw(n, order, eqprev, koff, klen, tid, uord_out, m_out);
+  *order_out = order;
+  *eqprev_out = eqprev;
+  return OK;
+}
+
+// Lexicographic order of the batch with the last occurrence of every key
+// kept: uord[0..m) are batch indices.  A mixed read/write batch (rw_ set)
+// goes through sort_rw instead.
+int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                      uint32_t **uord_out, int *m_out) {
+  if (rw_) return sort_rw(n, koff, klen, maxlen, tid, uord_out, m_out);
+  uint32_t *order;
+  uint8_t *eqprev;
+  int rc = sort_batch(n, koff, klen, maxlen, tid, &order, &eqprev);
+  if (rc) return rc;
+  cudaError_t e = cudaSuccess;
+  unsigned long long *flags = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
+  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)n, e);
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+  if (e != cudaSuccess) return check_cuda(e, "unique alloc");
   count_launch(), k_keep_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
   e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
   if (e == cudaSuccess) count_launch(), k_keep_scatter<<<blocks_for(n), kThreads, 0, st_>>>(flags, pos, order, n, uord);
@@ -437,6 +460,65 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "unique");
   *m_out = (int)(h_small_[0] & 0xFFFFFFFFu);
+  *uord_out = uord;
+  return OK;
+}
+
+
+// Mixed read/write batch: group equal keys in batch order (hash-table slots
+// + a stable radix sort of the slots; full-key sort if two keys share a
+// 64-bit hash), answer the reads, keep the last write of every key; PhaseNU
+// then gets the kept writes in key order.
+int Trie::sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                  uint32_t **uord_out, int *m_out) {
+  cudaError_t e = cudaSuccess;
+  uint64_t size = 1024;
+  while (size < 2ull * (uint64_t)n) size <<= 1;
+  unsigned long long *hash = wsp<unsigned long long>(ws_.dd_hash, size, e);
+  uint32_t *hpos = wsp<uint32_t>(ws_.dd_pos, size, e);
+  uint64_t *skey = wsp<uint64_t>(ws_.skey, (size_t)n, e);
+  uint32_t *sval = wsp<uint32_t>(ws_.sval, (size_t)n, e);
+  uint32_t *order = wsp<uint32_t>(ws_.order, (size_t)n, e);
+  uint8_t *eqprev = wsp<uint8_t>(ws_.eqprev, (size_t)n + 1, e);
+  unsigned long long *tot = wsp<unsigned long long>(ws_.rw_tot, 8, e);
+  uint32_t *collision = reinterpret_cast<uint32_t *>(tot + 5);
+  if (e == cudaSuccess) e = cudaMemsetAsync(hash, 0xFF, sizeof(unsigned long long) * size, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(hpos, 0, sizeof(uint32_t) * size, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tot, 0, 64, st_);
+  if (e != cudaSuccess) return check_cuda(e, "rw group alloc");
+  const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
+  DedupTable tab{hash, hpos, size - 1, hmask};
+  count_launch(), k_dedup_insert<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab);
+  count_launch(), k_rw_slots<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, skey, sval, collision);
+  if ((e = cudaMemcpyAsync(h_small_, collision, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "rw group");
+  const bool grouped = (h_small_[0] & 0xFFFFFFFFu) == 0;
+  int rc = OK;
+  if (grouped) {
+    int passes = 0;
+    if ((e = sorter_.sort(skey, sval, n, st_, &passes)) != cudaSuccess) return check_cuda(e, "rw group sort");
+    stats_.sort_passes = (uint32_t)passes;
+    count_launch(), k_rw_groups<<<blocks_for(n + 1), kThreads, 0, st_>>>(skey, sval, n, order, eqprev);
+  } else if ((rc = sort_batch(n, koff, klen, maxlen, tid, &order, &eqprev))) {
+    return rc;
+  }
+  uint32_t *kept;
+  int m = 0;
+  if ((rc = resolve_rw(n, order, eqprev, koff, klen, tid, &kept, &m))) return rc;
+  *m_out = m;
+  *uord_out = kept;
+  if (!rw_->key_order || !grouped || m <= 1) return OK;
+  uint64_t *koff2 = wsp<uint64_t>(ws_.rw_koff, (size_t)m, e);
+  uint32_t *klen2 = wsp<uint32_t>(ws_.rw_klen, (size_t)m, e);
+  int *tid2 = tid ? wsp<int>(ws_.rw_tid, (size_t)m, e) : nullptr;
+  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)m, e);
+  if (e != cudaSuccess) return check_cuda(e, "rw key order alloc");
+  count_launch(), k_rw_gather<<<blocks_for(m), kThreads, 0, st_>>>(kept, m, koff, klen, tid, koff2, klen2, tid2);
+  uint32_t *order2;
+  uint8_t *eqprev2;
+  if ((rc = sort_batch(m, koff2, klen2, maxlen, tid2, &order2, &eqprev2))) return rc;
+  count_launch(), k_rw_map<<<blocks_for(m), kThreads, 0, st_>>>(order2, kept, m, uord);
   *uord_out = uord;
   return OK;
 }
@@ -454,7 +536,7 @@ int Trie::resolve_rw(int n, const uint32_t *order, const uint8_t *eqprev, const 
   uint32_t *wpos = wsp<uint32_t>(ws_.rw_wpos, (size_t)n, e);
   unsigned long long *keep = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
   unsigned long long *pos = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
-  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)n, e);
+  uint32_t *uord = wsp<uint32_t>(ws_.rw_kept, (size_t)n, e);
   unsigned long long *tot = wsp<unsigned long long>(ws_.rw_tot, 8, e);  // writes, heads, reads, kept
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
   if (e == cudaSuccess) e = cudaMemsetAsync(tot, 0, 64, st_);  // tot[4]: LockNU's (unused) collision word
@@ -1752,6 +1834,7 @@ int Trie::put_rw(const BatchIn &b, const uint8_t *rw, bool two_phase, uint64_t *
   cudaError_t e = cudaSuccess;
   const size_t n = (size_t)b.n;
   RwState st;
+  st.key_order = two_phase;
   st.flags = wsp<uint8_t>(ws_.rw_flags, n, e);
   st.hp = b.device ? read_hps : wsp<uint64_t>(ws_.rw_hp, n, e);
   st.len = b.device ? read_sizes : wsp<int>(ws_.rw_len, n, e);

@@ -225,7 +225,7 @@ class Trie {
     DevBlock dd_hash, dd_pos, dd_sel;                           // LockNU batch dedup
     DevBlock raw;                                               // raw key bytes of the batch
     DevBlock rw_flags, rw_a, rw_b, rw_c, rw_d, rw_e, rw_wpos;   // mixed read/write resolution
-    DevBlock rw_hp, rw_len, rw_tot;
+    DevBlock rw_hp, rw_len, rw_tot, rw_kept, rw_koff, rw_klen, rw_tid;
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;
@@ -238,6 +238,7 @@ class Trie {
     uint64_t *hp = nullptr;          // device, read rank order
     int *len = nullptr;
     uint64_t vid_base = 0;
+    bool key_order = false;          // kept writes in key order (PhaseNU)
     uint64_t reads = 0;              // out
   };
   RwState *rw_ = nullptr;
@@ -251,6 +252,10 @@ class Trie {
                       uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact = false);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
+  int sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                 uint32_t **order_out, uint8_t **eqprev_out);
+  int sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid, uint32_t **uord_out,
+              int *m_out);
   int resolve_rw(int n, const uint32_t *order, const uint8_t *eqprev, const uint64_t *koff, const uint32_t *klen,
                  const int *tid, uint32_t **uord_out, int *m_out);
   int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,

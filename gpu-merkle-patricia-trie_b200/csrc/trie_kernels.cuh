@@ -315,6 +315,30 @@ __global__ void k_rw_sorted_flags(const uint8_t *eqprev, const uint32_t *order, 
   is_head[p] = eqprev[p] ? 0ull : 1ull;
 }
 
+// sorted slots -> order / eqprev as the full-key sort leaves them
+__global__ void k_rw_groups(const uint64_t *skey, const uint32_t *sval, int n, uint32_t *order, uint8_t *eqprev) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > n) return;
+  if (p < n) order[p] = sval[p];
+  eqprev[p] = (p > 0 && p < n && skey[p] == skey[p - 1]) ? 1 : 0;
+}
+
+// the kept writes' key records, for a key-order sort of them alone
+__global__ void k_rw_gather(const uint32_t *kept, int m, const uint64_t *koff, const uint32_t *klen, const int *tid,
+                            uint64_t *koff_out, uint32_t *klen_out, int *tid_out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t i = kept[j];
+  koff_out[j] = koff[i];
+  klen_out[j] = klen[i];
+  if (tid) tid_out[j] = tid[i];
+}
+
+__global__ void k_rw_map(const uint32_t *order, const uint32_t *kept, int m, uint32_t *uord) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) uord[j] = kept[order[j]];
+}
+
 __global__ void k_rw_read_flags(TrieView tv, const uint8_t *rw, int n, unsigned long long *is_read) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;

@@ -122,6 +122,9 @@ class Stage:
             self.kidx = t.empty(2 * self.cap, dtype=t.int32, device=self.dev)
             self.vidx = t.empty(2 * self.cap, dtype=t.int64, device=self.dev)
             self.tids = t.empty(self.cap, dtype=t.int32, device=self.dev)
+            self.rw = t.empty(self.cap, dtype=t.uint8, device=self.dev)        # mixed batches
+            self.out_hp = t.empty(self.cap, dtype=t.int64, device=self.dev)
+            self.out_len = t.empty(self.cap, dtype=t.int32, device=self.dev)
         if kb > self.kcap:
             self.kcap = int(kb * 1.25) + 4096
             self.keys = t.empty(self.kcap + 64, dtype=t.uint8, device=self.dev)
@@ -230,16 +233,26 @@ class Runner:
             self.mpt.puts_forest_device(TU.CONFIGS[k]["two_phase"], s.keys.data_ptr(), s.kidx.data_ptr(),
                                         s.vals.data_ptr(), s.vidx.data_ptr(), s.tids.data_ptr(), nn, kb, vb)
             self.mpt.hash_onepass_v2()
+        # and the read/write resolution of a mixed batch of that size
+        rec, self.record = self.record, None
+        run = [Request(-1, "put", tid, n // 2 + 1, 0.5, 0.5, 0x5C7A7C7), Request(-1, "get", tid, n // 2 + 1, 0.5,
+                                                                                0.0, 0x5C7A7C8)]
+        nn, kb, vb = self.build(run)
+        self.mixed(run, TU.FIXED_LOCKNU, nn, kb, vb)
+        self.record = rec
         del self.tenant_of[tid]
         del self.count[tid]
 
     def build(self, reqs):
-        """Generate the merged batch of same-kind requests into the stage."""
+        """Generate the merged batch of the requests into the stage, in
+        request order; in a mixed batch get keys have empty values and
+        stage.rw flags every key (1 put, 0 get)."""
         s = self.stage
         torch = s.torch
         n = sum(r.n for r in reqs)
         kb = sum(r.n * (2 * self.tenant_of[r.tenant].key_bytes + 1) for r in reqs)
-        vb = sum(r.n * self.tenant_of[r.tenant].value_bytes for r in reqs) if reqs[0].kind == "put" else 0
+        vb = sum(r.n * self.tenant_of[r.tenant].value_bytes for r in reqs if r.kind == "put")
+        mixed = len(set(r.kind for r in reqs)) > 1
         s.ensure(n, kb, max(vb, 1))
         off = koff = voff = 0
         for r in reqs:
@@ -262,6 +275,11 @@ class Runner:
                 if voff:
                     s.vidx[2 * off: 2 * (off + r.n)] += voff
                 voff += r.n * t.value_bytes
+            elif mixed:
+                s.vidx[2 * off: 2 * (off + r.n): 2] = voff
+                s.vidx[2 * off + 1: 2 * (off + r.n): 2] = voff - 1
+            if mixed:
+                s.rw[off: off + r.n] = 1 if r.kind == "put" else 0
             s.tids[off: off + r.n] = t.tid
             off += r.n
             koff += r.n * w
@@ -296,6 +314,24 @@ class Runner:
                                     s.tids.data_ptr(), n, kb, vb)
         self.mpt.hash_onepass_v2()
         return self.mpt.get_roots(touched)
+
+    def mixed(self, reqs, k: int, n, kb, vb):
+        """A built mixed batch in one gmpt_puts_with_read_device call (as if
+        applied in request order) + PhaseHC + roots of the written tries;
+        returns the read sizes in read order.  A persistent configuration
+        (no read support) runs as LockNU with its latch ways."""
+        s = self.stage
+        if self.record is not None:
+            b, tids = self.snapshot(n, kb, vb)
+            sel = np.nonzero(s.rw[:n].cpu().numpy() == 1)[0]
+            self.record.append((b.subset(sel), tids[sel]))
+        two = TU.apply_config(self.mpt, k) and not TU.CONFIGS[k].get("persistent")
+        cnt = self.mpt.puts_with_read_device(two, s.keys.data_ptr(), s.kidx.data_ptr(), s.rw.data_ptr(),
+                                             s.vals.data_ptr(), s.vidx.data_ptr(), n, kb, vb,
+                                             s.out_hp.data_ptr(), s.out_len.data_ptr(), d_tids=s.tids.data_ptr())
+        self.mpt.hash_onepass_v2()
+        self.mpt.get_roots(sorted(set(r.tenant for r in reqs if r.kind == "put")))
+        return s.out_len[:cnt].cpu().numpy()
 
     def get(self, n, kb):
         s = self.stage
@@ -402,12 +438,14 @@ def _groups(window):
     return out
 
 
-def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> ServeResult:
+def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23, mixed: bool = False) -> ServeResult:
     """Live server on a virtual clock.  policy(runner, reqs, n, kb, vb) ->
     configuration index (its own time is part of the service time).  With
     batching, the requests that arrived while the server was busy are drained
-    and merged by _groups; get_sizes holds each get request's result sizes
-    (None for puts), in request order."""
+    and merged by _groups; with mixed as well, a drained window holding puts
+    and gets is one mixed read/write call instead (the batch acts as if
+    applied in request order, so results are unchanged).  get_sizes holds
+    each get request's result sizes (None for puts), in request order."""
     lat = np.zeros(len(reqs))
     svc = np.zeros(len(reqs))
     free = 0.0
@@ -426,10 +464,26 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23) -> Serv
                 tot += reqs[j].n
                 j += 1
         t = start
-        for run in (_groups(reqs[i:j]) if batching else [[reqs[i]]]):
+        window = reqs[i:j]
+        if not batching:
+            runs = [[reqs[i]]]
+        elif mixed and len(set(r.kind for r in window)) > 1:
+            runs = [window]
+        else:
+            runs = _groups(window)
+        for run in runs:
             n, kb, vb = runner.build(run)
             t0 = time.perf_counter()
-            if run[0].kind == "put":
+            if len(set(r.kind for r in run)) > 1:
+                k = policy(runner, run, n, kb, vb)
+                choices[k] = choices.get(k, 0) + 1
+                sizes = runner.mixed(run, k, n, kb, vb)
+                at = 0
+                for r in run:
+                    if r.kind == "get":
+                        gets[r.i - base] = sizes[at: at + r.n]
+                        at += r.n
+            elif run[0].kind == "put":
                 k = policy(runner, run, n, kb, vb)
                 choices[k] = choices.get(k, 0) + 1
                 runner.put(run, k, n, kb, vb)

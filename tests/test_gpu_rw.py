@@ -165,3 +165,23 @@ def test_mixed_batch_forest_and_device(gpu_lib):
         g.hash_onepass_v2()
         assert g.get_roots(n=n_tries) == roots
         g.close()
+
+
+@pytest.mark.parametrize("two_phase", [True, False])
+def test_mixed_batch_hash_collisions_fall_back_exactly(gpu_lib, two_phase):
+    # 3-bit key hashes: every slot is shared by different keys, so grouping
+    # by hash slot is refused and the full-key sort groups the batch
+    rng = W.Xoshiro256ss(0x5D3 + two_phase)
+    pool = keyset(rng, 600, 7, 16)
+    t = gpu_lib.MPT()
+    state = load(t, rng, pool, two_phase)
+    t.set_option("latch_dedup_bits", 3)
+    keys, flags, vals, hps = mixed_ops(rng, pool, 3000, 0.5, keyset(rng, 50, 5, 256))
+    want = expect(state, keys, flags, vals, hps)
+    b = make_batch([nib(k) for k in keys], vals)
+    rh, rs = t.puts_with_read(two_phase, b.keys_hexs, b.keys_indexs, flags, b.values, b.values_indexs,
+                              values_hps=hps)
+    assert list(zip(rh.tolist(), rs.tolist())) == want
+    t.hash_onepass_v2()
+    assert t.get_root_hash() == oracle_root(O.MODE_REF, state)
+    t.close()

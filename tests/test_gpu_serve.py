@@ -40,7 +40,7 @@ def test_served_stream_matches_oracle_under_every_schedule(gpu_lib, dev):
     S.poisson_arrivals(reqs, 5000.0)  # dense arrivals: the batched server merges
     rng = np.random.default_rng(0)
     runs = []
-    for batching in (False, True):
+    for batching, mixed in ((False, False), (True, False), (True, True)):
         r = S.Runner(gpu_lib, tenants, 0, dev, record=True)
         picks = []
 
@@ -49,17 +49,20 @@ def test_served_stream_matches_oracle_under_every_schedule(gpu_lib, dev):
             picks.append(k)
             return k
 
-        res = S.serve(r, reqs, policy, batching)
+        res = S.serve(r, reqs, policy, batching, mixed=mixed)
         runs.append((r.roots(), res, r.record, picks))
         r.close()
-    (roots_a, res_a, rec_a, picks_a), (roots_b, res_b, rec_b, _) = runs
-    assert roots_a == roots_b
+    (roots_a, res_a, rec_a, picks_a), (roots_b, res_b, rec_b, _), (roots_c, res_c, rec_c, _) = runs
+    assert roots_a == roots_b == roots_c
     assert roots_a == _oracle_roots(rec_a, tenants)
+    assert roots_c == _oracle_roots(rec_c, tenants)
     assert len(set(picks_a)) > 3  # many configurations exercised
     assert res_b.groups < res_a.groups  # merging happened
+    assert res_c.groups < res_b.groups  # mixed windows became single calls
     # lookups answer the same whichever way they were grouped
-    for x, y in zip(res_a.get_sizes, res_b.get_sizes):
-        assert (x is None) == (y is None) and (x is None or np.array_equal(x, y))
+    for x, y, z in zip(res_a.get_sizes, res_b.get_sizes, res_c.get_sizes):
+        assert (x is None) == (y is None) == (z is None)
+        assert x is None or (np.array_equal(x, y) and np.array_equal(x, z))
 
 
 def test_time_matrix_replicas_agree_and_selector_trains(gpu_lib, dev):
