@@ -1041,8 +1041,12 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
   // pass 1: payload size (all child loads issued together, sources prefetched)
   uint64_t payload = 0;
   EncItem it1{0, 0, 0, nullptr, 0}, it2{0, 0, 0, nullptr, 0};  // short: key, child
+  const uint32_t *chp = tv.full_child + (size_t)idx * 17;
+  // branch whose children are all hashed nodes (32-byte references) and whose
+  // value slot is empty: its encoding is regular and is generated word by word
+  uint32_t present = 0;
+  bool regular = full;
   if (full) {
-    const uint32_t *chp = tv.full_child + (size_t)idx * 17;
     uint32_t ch[17];
 #pragma unroll
     for (int k = 0; k < 17; ++k) ch[k] = ldn<kCoh>(chp + k);
@@ -1052,6 +1056,11 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
     for (int k = 0; k < 17; ++k) {
       EncItem it = child_item<kCoh>(tv, ch[k]);
       payload += it.pren + it.blen;
+      const uint32_t kd = ref_kind(ch[k]);
+      if (kd != KIND_NULL) {
+        present |= 1u << k;
+        regular = regular && k < 16 && kd != KIND_VALUE && it.blen == 32 && it.pren == 1;
+      }
     }
   } else {
     uint32_t child = ldn<kCoh>(tv.short_child + idx);
@@ -1108,6 +1117,58 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
       for (int w = 0; w < 17; ++w) sp.a[w] = st[w * S];
       keccak_f1600(sp.a);
     }
+  } else if (regular) {
+  // regular branch: pending message bytes (little-endian), next slot, words
+  // left of the current child's hash
+  uint64_t buf = hdr;
+  uint32_t nb = hn, slot = 0, hj = 8;
+  const uint32_t *hw = nullptr;
+  bool last = false;
+  while (true) {
+    {  // one block: 0x80 per empty slot, 0xa0 + 32 hash bytes per child, then
+       // the Keccak padding (rlp.cuh:132-155, node.cuh:46-112)
+      uint64_t *st = sp.stage;
+      const uint32_t S = sp.stride;
+      for (int w = 0; w < 17; ++w) {
+        uint64_t word = 0;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          while (nb < 4) {
+            if (hj < 8) {
+              buf |= (uint64_t)ldn<kCoh>(hw + hj) << (8 * nb);
+              nb += 4;
+              ++hj;
+            } else if (slot < 17) {
+              if ((present >> slot) & 1u) {
+                const uint32_t r = ldn<kCoh>(chp + slot);
+                hw = reinterpret_cast<const uint32_t *>(
+                    (ref_kind(r) == KIND_FULL ? tv.full_hash : tv.short_hash) + (size_t)ref_idx(r) * 32);
+                buf |= 0xa0ull << (8 * nb);
+                hj = 0;
+              } else {
+                buf |= 0x80ull << (8 * nb);
+              }
+              nb += 1;
+              ++slot;
+            } else if (!last) {
+              buf |= 0x01ull << (8 * nb);  // Keccak padding starts here
+              nb += 1;
+              last = true;
+            } else {
+              nb = 4;  // zeros to the end of the block
+            }
+          }
+          word |= (buf & 0xFFFFFFFFull) << (32 * half);
+          buf >>= 32;
+          nb -= 4;
+        }
+        st[w * S] = word;
+      }
+      if (last) st[16 * S] |= 0x8000000000000000ull;
+    }
+    sp.absorb();
+    if (last) break;
+  }
   } else {
   // pass 2: stream
   int item = 0;
