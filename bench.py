@@ -16,6 +16,7 @@ from the reference sources) on the host cores instead.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -283,6 +284,10 @@ def run_eth(args, local, dev):
     roots_block, ms_block = [], []
     launches0 = gmpt.launch_count()
     sampler = ClockSampler(local)
+    # no collector pause of this process inside a timed block (the events
+    # bracket the host call, so a pause would count as block time)
+    gc.collect()
+    gc.disable()
     sampler.start()
     # autotuned persistent grid: the first blocks rotate through the candidate
     # grids (same roots whichever runs), then the fastest median is kept
@@ -308,6 +313,7 @@ def run_eth(args, local, dev):
         if chosen is None:
             tune_ms[grid].append(ms_block[-1])
     clocks = sampler.stop()
+    gc.enable()
     launches = gmpt.launch_count() - launches0
     info = fb.block_info()
     tl = fb.block_timeline()
@@ -372,6 +378,7 @@ def run_eth(args, local, dev):
         "keys": tot_keys, "tries_touched_per_block": round(float(np.mean([len(b.storage_ids) + 1 for b in blks])), 1),
         "keys_per_block": round(tot_keys / len(blks), 1),
         "block_mkeys_s": blk_rate, "block_p50_ms": round(float(np.percentile(ms_block, 50)), 3),
+        "block_max_ms": round(float(np.max(ms_block)), 3),
         "block_p99_ms": round(float(np.percentile(ms_block, 99)), 3),
         "e2e_mkeys_s": rate(tot_keys, ms_e2e), "e2e_p50_ms": round(float(np.percentile(ms_e2e, 50)), 3),
         "e2e_p99_ms": round(float(np.percentile(ms_e2e, 99)), 3), "e2e_h2d_bytes": int(h2d),
@@ -459,7 +466,10 @@ def run_requests(args, local, dev):
         for r in reps:
             r.reset(tenants)
             r.reserve_for(ev)
+        gc.collect()
+        gc.disable()
         T, G, F = S.time_matrix(reps, ev)
+        gc.enable()
         final = reps[0].roots()
         isput = np.array([r.kind == "put" for r in ev])
         keys = sum(r.n for r in ev)
@@ -471,12 +481,15 @@ def run_requests(args, local, dev):
             if batching:
                 rn.reserve_for(ev, merged_keys=MERGE_KEYS)
             fb0 = sel.fallbacks
+            gc.collect()
+            gc.disable()  # service times are host wall clock: no collector pauses inside
             r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS, mixed=mixed)
+            gc.enable()
             assert rn.roots() == final, f"{name}: roots differ from the fixed-schedule replicas"
             res[name] = {"mkeys_s": round(r.keys / (r.busy_ms / 1e3) / 1e6, 3),
                          "p50_ms": round(float(np.percentile(r.latency_ms, 50)), 3),
                          "p99_ms": round(float(np.percentile(r.latency_ms, 99)), 3),
-                         "groups": r.groups, "rule_fallbacks": sel.fallbacks - fb0,
+                         "groups": r.groups, "rule_fallbacks": sel.fallbacks - fb0, "slowest_calls": r.slowest,
                          "choices": {TU.CONFIGS[k]["name"]: v for k, v in sorted(r.choices.items())}}
             return r
 
@@ -590,6 +603,8 @@ def run_ours(args, world, rank, local):
     stats_all = []
     barrier()
     launches0 = gmpt.launch_count()
+    gc.collect()
+    gc.disable()
     sampler.start()
     for _ in range(args.steps):
         a = torch.cuda.Event(enable_timing=True)
@@ -747,6 +762,7 @@ def run_ours(args, world, rank, local):
                             "ms_per_step": round(rms, 3), "h2d_bytes_per_step": int(h2d_raw),
                             "path": "gmpt_puts_pipeline_raw (raw key bytes; nibbles made on the device)"}}
 
+    gc.enable()
     line = {
         "metric": "put+root-hash Mkeys/s", "value": round(value, 3), "unit": "Mkeys/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,

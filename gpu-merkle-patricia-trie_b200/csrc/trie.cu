@@ -26,7 +26,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHashThreads = 128;
-constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);
+constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);          // (depth, kind)
+constexpr int kHashBins = kMaxDepthBins * (int)kHashClasses;       // (depth, kind, hash class)
 // levels with at most this many branch nodes hash them one warp each
 constexpr int kWarpFullMax = 4096;
 // LockNU batches of at least this many keys drop repeated keys first
@@ -100,7 +101,7 @@ Trie::~Trie() {
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
                         &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
-                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.rw_flags,
+                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.dirty_cls, &ws_.rw_flags,
                         &ws_.rw_a, &ws_.rw_b, &ws_.rw_c, &ws_.rw_d, &ws_.rw_e, &ws_.rw_wpos, &ws_.rw_hp,
                         &ws_.rw_len, &ws_.rw_tot, &ws_.rw_kept, &ws_.rw_koff, &ws_.rw_klen, &ws_.rw_tid,
                         &ws_.misc};
@@ -795,25 +796,27 @@ int Trie::bucket_and_hash() {
   stats_.last_dirty = nd;
   stats_.last_hash_levels = 0;
   if (nd == 0) return OK;
-  uint32_t *bins = wsp<uint32_t>(ws_.bins, kMaxDepthBins + 1, e);
-  uint32_t *cursor = wsp<uint32_t>(ws_.cursor, kMaxDepthBins + 1, e);
+  uint32_t *bins = wsp<uint32_t>(ws_.bins, kHashBins + 1, e);
+  uint32_t *cursor = wsp<uint32_t>(ws_.cursor, kHashBins + 1, e);
   uint32_t *sorted = wsp<uint32_t>(ws_.sorted_dirty, nd, e);
-  if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * (kMaxDepthBins + 1), st_);
+  uint8_t *cls = wsp<uint8_t>(ws_.dirty_cls, nd, e);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * (kHashBins + 1), st_);
   if (e != cudaSuccess) return check_cuda(e, "hash alloc");
   int grid = std::min<int>(blocks_for(nd), 148 * 4);
-  count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kMaxDepthBins, st_>>>(dirty_ref_, dirty_depth_, (int)nd, bins,
-                                                                          kMaxDepthBins);
-  std::vector<uint32_t> hb(kMaxDepthBins), off(kMaxDepthBins + 1);
-  if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyDeviceToHost, st_)) !=
+  count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kHashBins, st_>>>(tv_, dirty_ref_, dirty_depth_,
+                                                                                      (int)nd, bins, kHashBins, cls);
+  std::vector<uint32_t> hb(kHashBins), off(kHashBins + 1);
+  if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kHashBins, cudaMemcpyDeviceToHost, st_)) !=
           cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
     return check_cuda(e, "hash bins");
   off[0] = 0;
-  for (int b = 0; b < kMaxDepthBins; ++b) off[b + 1] = off[b] + hb[b];
-  if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kMaxDepthBins, cudaMemcpyHostToDevice, st_)) !=
+  for (int b = 0; b < kHashBins; ++b) off[b + 1] = off[b] + hb[b];
+  if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kHashBins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
-  count_launch(), k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, (int)nd, cursor, sorted);
+  count_launch(), k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, cls, (int)nd, cursor,
+                                                                        sorted);
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;
   if ((e = cudaMemsetAsync(&ctr_->hashed, 0, 4, st_)) != cudaSuccess ||
@@ -827,7 +830,8 @@ int Trie::bucket_and_hash() {
   }
   const size_t smem_warp = smem + 4 * kWarpMsgBytes;
   for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
-    uint32_t a = off[2 * d], m = off[2 * d + 1], z = off[2 * d + 2];
+    const uint32_t C = kHashClasses;
+    uint32_t a = off[2 * d * C], m = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];
     if (z == a) continue;
     ++levels;
     if (z - m > 0 && z - m <= (uint32_t)kWarpFullMax) {

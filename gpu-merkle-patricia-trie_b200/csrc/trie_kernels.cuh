@@ -838,24 +838,58 @@ __global__ void k_level_scatter(const uint32_t *act, const uint32_t *aseg, const
 // ---------------------------------------------------------------------------
 // PhaseHC: dirty nodes bucketed by (nibble depth, kind), deepest first
 
-__global__ void k_dirty_hist(const uint32_t *ref, const uint16_t *depth, int n, uint32_t *bins, int nbins) {
+// Keccak blocks a dirty node's encoding is expected to take, minus one,
+// capped at 3: a branch's children counted as 33-byte references, a leaf's
+// value length read from its record.  Hashing threads of one warp then hold
+// nodes of one block count, so no lane idles through another's extra
+// permutations.
+constexpr uint32_t kHashClasses = 4;
+
+__device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
+  const uint32_t kind = ref_kind(r), idx = ref_idx(r);
+  uint32_t bytes;
+  if (kind == KIND_FULL) {
+    const uint32_t *c = tv.full_child + (size_t)idx * 17;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int k = 0; k < 17; ++k) cnt += c[k] != 0u ? 1u : 0u;
+    bytes = 20u + 32u * cnt;
+  } else {
+    if (tv.short_dead[idx]) return 0u;
+    const uint32_t ch = tv.short_child[idx];
+    bytes = tv.short_klen[idx] / 2u + 8u;
+    bytes += ref_kind(ch) == KIND_VALUE ? tv.rec_len[tv.value_vid[ref_idx(ch)]] : 33u;
+  }
+  return min(bytes / 136u, kHashClasses - 1u);
+}
+
+// bin of a dirty node: (nibble depth, kind, hash class)
+__device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
+  return (2u * depth + (ref_kind(r) == KIND_FULL ? 1u : 0u)) * kHashClasses + cls;
+}
+
+__global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *depth, int n, uint32_t *bins,
+                             int nbins, uint8_t *cls) {
   extern __shared__ uint32_t h[];
   for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0;
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t b = 2u * depth[i] + (ref_kind(ref[i]) == KIND_FULL ? 1u : 0u);
-    atomicAdd(&h[b], 1u);
+    const uint32_t r = ref[i];
+    const uint32_t c = hash_class(tv, r);
+    cls[i] = (uint8_t)c;
+    atomicAdd(&h[dirty_bin(depth[i], r, c)], 1u);
   }
   __syncthreads();
   for (int b = threadIdx.x; b < nbins; b += blockDim.x)
     if (h[b]) atomicAdd(&bins[b], h[b]);
 }
 
-__global__ void k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, int n, uint32_t *cursor, uint32_t *out) {
+__global__ void k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, const uint8_t *cls, int n,
+                                uint32_t *cursor, uint32_t *out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t r = ref[i];
-  uint32_t b = 2u * depth[i] + (ref_kind(r) == KIND_FULL ? 1u : 0u);
+  uint32_t b = dirty_bin(depth[i], r, cls[i]);
   unsigned peers = __match_any_sync(__activemask(), b);
   int leader = __ffs(peers) - 1;
   uint32_t base = 0;

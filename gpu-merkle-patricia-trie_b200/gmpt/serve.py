@@ -409,6 +409,7 @@ class ServeResult:
     choices: dict = field(default_factory=dict)
     get_sizes: list = field(default_factory=list)
     service_ms: np.ndarray | None = None  # per request (one-at-a-time server)
+    slowest: list = field(default_factory=list)  # (ms, kinds, keys) of the slowest calls
 
 
 def _groups(window):
@@ -453,6 +454,7 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23, mixed: 
     groups = 0
     choices = {}
     gets = [None] * len(reqs)
+    calls = []
     base = reqs[0].i if reqs else 0
     i = 0
     while i < len(reqs):
@@ -494,6 +496,7 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23, mixed: 
                     gets[r.i - base] = sizes[at: at + r.n]
                     at += r.n
             ms = (time.perf_counter() - t0) * 1e3
+            calls.append((round(ms, 3), "".join(sorted(set(r.kind[0] for r in run))), n))
             busy += ms
             t += ms / 1e3
             groups += 1
@@ -502,4 +505,5 @@ def serve(runner, reqs, policy, batching: bool, max_keys: int = 1 << 23, mixed: 
                 svc[r.i - base] = ms / len(run)
         free = t
         i = j
-    return ServeResult(lat, busy, sum(r.n for r in reqs), 0, groups, choices, gets, svc)
+    return ServeResult(lat, busy, sum(r.n for r in reqs), 0, groups, choices, gets, svc,
+                       sorted(calls, reverse=True)[:3])
