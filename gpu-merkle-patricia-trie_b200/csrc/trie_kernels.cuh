@@ -840,20 +840,24 @@ __global__ void k_level_scatter(const uint32_t *act, const uint32_t *aseg, const
 
 // Keccak blocks a dirty node's encoding is expected to take, minus one,
 // capped at 3: a branch's children counted as 33-byte references, a leaf's
-// value length read from its record.  Hashing threads of one warp then hold
-// nodes of one block count, so no lane idles through another's extra
-// permutations.
+// value length read from its record.  k_hash_level orders each CTA's nodes by
+// it, so the lanes of a warp need the same number of permutations and none
+// idles through another's extra ones.
 constexpr uint32_t kHashClasses = 4;
+
+__device__ __forceinline__ uint32_t full_class(const TrieView &tv, uint32_t idx) {
+  const uint32_t *c = tv.full_child + (size_t)idx * 17;
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int k = 0; k < 17; ++k) cnt += c[k] != 0u ? 1u : 0u;
+  return min((20u + 32u * cnt) / 136u, kHashClasses - 1u);
+}
 
 __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   const uint32_t kind = ref_kind(r), idx = ref_idx(r);
   uint32_t bytes;
   if (kind == KIND_FULL) {
-    const uint32_t *c = tv.full_child + (size_t)idx * 17;
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int k = 0; k < 17; ++k) cnt += c[k] != 0u ? 1u : 0u;
-    bytes = 20u + 32u * cnt;
+    return full_class(tv, idx);
   } else {
     if (tv.short_dead[idx]) return 0u;
     const uint32_t ch = tv.short_child[idx];
@@ -863,7 +867,9 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   return min(bytes / 136u, kHashClasses - 1u);
 }
 
-// bin of a dirty node: (nibble depth, kind, hash class)
+// bin of a dirty node: (nibble depth, kind, hash class); the class is
+// counted for branches only (one read of the child slots), leaves are
+// ordered inside each hashing CTA
 __device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
   return (2u * depth + (ref_kind(r) == KIND_FULL ? 1u : 0u)) * kHashClasses + cls;
 }
@@ -875,7 +881,7 @@ __global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *d
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t r = ref[i];
-    const uint32_t c = hash_class(tv, r);
+    const uint32_t c = ref_kind(r) == KIND_FULL ? full_class(tv, ref_idx(r)) : 0u;
     cls[i] = (uint8_t)c;
     atomicAdd(&h[dirty_bin(depth[i], r, c)], 1u);
   }
@@ -1366,11 +1372,36 @@ __global__ void __launch_bounds__(128) k_hash_full_warp(TrieView tv, const uint3
 // its 25 lanes in registers; a few encoder temporaries spill, and the extra
 // resident warps hide more of the child / record gathers (measured faster
 // than five CTAs at 96 registers without spills).
+// One level, thread per node; the CTA's 128 nodes are first reordered by
+// hash class (stable counting partition from warp ballots), so warps hold
+// nodes of one Keccak block count.
 __global__ void __launch_bounds__(128, 6) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count) return;
-  hash_node<false>(tv, refs[t], stage_all + threadIdx.x, blockDim.x);
+  __shared__ uint32_t s_ref[128];
+  __shared__ uint32_t s_cnt[kHashClasses][4];  // [class][warp]
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool valid = t < count;
+  const uint32_t r = valid ? refs[t] : 0u;
+  const uint32_t c = valid ? hash_class(tv, r) : kHashClasses;
+  uint32_t mine = 0;
+#pragma unroll
+  for (uint32_t v = 0; v < kHashClasses; ++v) {
+    const unsigned b = __ballot_sync(0xffffffffu, c == v);
+    if (lane == 0) s_cnt[v][warp] = (uint32_t)__popc(b);
+    if (c == v) mine = (uint32_t)__popc(b & ((1u << lane) - 1u));
+  }
+  __syncthreads();
+  if (valid) {
+    uint32_t pos = mine;
+    for (uint32_t v = 0; v < kHashClasses; ++v)
+      for (int w = 0; w < 4; ++w)
+        if (v < c || (v == c && w < warp)) pos += s_cnt[v][w];
+    s_ref[pos] = r;
+  }
+  __syncthreads();
+  if (!valid) return;  // the valid nodes fill s_ref[0 .. valid count)
+  hash_node<false>(tv, s_ref[threadIdx.x], stage_all + threadIdx.x, blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
