@@ -382,9 +382,13 @@ __global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t
   const unsigned long long h = dedup_hash(tv.keys + koff[i], klen[i], tid ? (uint32_t)tid[i] : 0u, t.hmask);
   uint64_t s = dedup_home(h, t.mask);
   for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask) {
-    const unsigned long long old = atomicCAS(&t.hash[s], kDedupEmpty, h);
+    // read before the atomics: a zipf-hot key repeats up to millions of
+    // times, and a CAS or max that cannot change the slot would serialise
+    // every one of them on the same address
+    unsigned long long old = __ldcg(&t.hash[s]);
+    if (old == kDedupEmpty) old = atomicCAS(&t.hash[s], kDedupEmpty, h);
     if (old == kDedupEmpty || old == h) {
-      atomicMax(&t.pos[s], (uint32_t)i);
+      if (__ldcg(&t.pos[s]) < (uint32_t)i) atomicMax(&t.pos[s], (uint32_t)i);
       return;
     }
   }
