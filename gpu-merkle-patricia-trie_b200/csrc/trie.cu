@@ -345,7 +345,7 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
   if (e != cudaSuccess) return check_cuda(e, "stage copy");
   if ((e = cudaMemsetAsync(&ctr_->stream_terms, 0, 24, st_)) != cudaSuccess) return check_cuda(e, "stage reset");
-  count_launch(), k_stage<<<blocks_for(n), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
+  count_launch(), k_stage<<<std::min<unsigned>(blocks_for(n), 148 * 8), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
                                                 *koff, *klen, d_max, tid);
   if (kbytes > 0 && !b.raw_keys)  // expanded raw keys are well formed by construction
     count_launch(), k_stage_stream<<<std::min<unsigned>(blocks_for(kbytes / 8 + 1), 148 * 8), kThreads, 0, st_>>>(
@@ -815,7 +815,7 @@ int Trie::bucket_and_hash() {
   if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kHashBins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
-  count_launch(), k_dirty_scatter<<<blocks_for(nd), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, cls, (int)nd, cursor,
+  count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, cls, (int)nd, cursor,
                                                                         sorted);
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;

@@ -99,57 +99,77 @@ __device__ __forceinline__ uint32_t new_short(const TrieView &tv, DirtyList d, u
 // ---------------------------------------------------------------------------
 // staging
 
-__global__ void k_stage(TrieView tv, const int *ki, const int64_t *vi, const uint64_t *hp, int n,
-                        uint64_t key_base, uint64_t val_base, uint64_t vid_base, int64_t kbytes,
-                        int64_t vbytes, uint64_t *koff, uint32_t *klen, uint32_t *maxlen, const int *tid) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (tid && (uint32_t)tid[i] >= tv.n_tries) set_error(tv.ctr, ERR_BAD_TRIE);
-  int ks = ki[2 * i], ke = ki[2 * i + 1];
-  bool bad = ks < 0 || ke < ks || (int64_t)ke >= kbytes;  // index pair outside the key stream
-  if (bad) ks = ke = 0;
-  int len = ke - ks + 1;
-  uint64_t off = key_base + (uint64_t)ks;
-  if (len > kMaxKeyNibbles) {
-    set_error(tv.ctr, ERR_KEY_TOO_LONG);
-    bad = true;
-  }
-  // Interior nibbles are checked by k_stage_stream over the whole stream when
-  // the index pairs tile it (the usual layout), else by k_stage_keys.
-  bool term = false;
-  if (!bad) {
-    uint8_t last = tv.keys[off + len - 1];
-    if (last > 16) bad = true;
-    term = last == 16;
-  }
-  bool gap = (i == 0) ? (ks != 0) : (ks != ki[2 * i - 1] + 1);
-  {
-    unsigned am = __activemask();
-    unsigned tb = __ballot_sync(am, term && !bad), gb = __ballot_sync(am, gap);
-    if ((int)(threadIdx.x & 31) == __ffs(am) - 1) {
-      if (tb) atomicAdd(&tv.ctr->key_terms, (uint32_t)__popc(tb));
-      if (gb) atomicOr(&tv.ctr->noncontig, 1u);
+// Per-key records of a staged batch.  Grid-stride, with the stream counters
+// (terminated keys, index-pair gaps, longest key) reduced per CTA: one
+// atomic per CTA and counter instead of one per warp, which serialised on
+// the three counter addresses at 16M keys.
+__global__ void __launch_bounds__(256) k_stage(TrieView tv, const int *ki, const int64_t *vi, const uint64_t *hp,
+                                               int n, uint64_t key_base, uint64_t val_base, uint64_t vid_base,
+                                               int64_t kbytes, int64_t vbytes, uint64_t *koff, uint32_t *klen,
+                                               uint32_t *maxlen, const int *tid) {
+  uint32_t terms = 0, gaps = 0, lmax = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (tid && (uint32_t)tid[i] >= tv.n_tries) set_error(tv.ctr, ERR_BAD_TRIE);
+    int ks = ki[2 * i], ke = ki[2 * i + 1];
+    bool bad = ks < 0 || ke < ks || (int64_t)ke >= kbytes;  // index pair outside the key stream
+    if (bad) ks = ke = 0;
+    int len = ke - ks + 1;
+    uint64_t off = key_base + (uint64_t)ks;
+    if (len > kMaxKeyNibbles) {
+      set_error(tv.ctr, ERR_KEY_TOO_LONG);
+      bad = true;
     }
+    // Interior nibbles are checked by k_stage_stream over the whole stream
+    // when the index pairs tile it (the usual layout), else by k_stage_keys.
+    bool term = false;
+    if (!bad) {
+      uint8_t last = tv.keys[off + len - 1];
+      if (last > 16) bad = true;
+      term = last == 16;
+    }
+    const bool gap = (i == 0) ? (ks != 0) : (ks != ki[2 * i - 1] + 1);
+    terms += (term && !bad) ? 1u : 0u;
+    gaps |= gap ? 1u : 0u;
+    if (bad) {
+      set_error(tv.ctr, ERR_BAD_KEY);
+      len = 1;  // keep later stages in bounds
+    }
+    koff[i] = off;
+    klen[i] = (uint32_t)len;
+    lmax = max(lmax, (uint32_t)len);
+    int64_t vs = vi[2 * i], ve = vi[2 * i + 1];
+    if (vs < 0 || ve < vs - 1 || ve >= vbytes || ve - vs + 1 > 0x7FFFFFFF) {  // empty values allowed
+      set_error(tv.ctr, ERR_BAD_KEY);
+      vs = 0;
+      ve = -1;
+    }
+    uint64_t vid = vid_base + (uint64_t)i;
+    tv.rec_off[vid] = val_base + (uint64_t)vs;
+    tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
+    tv.rec_hp[vid] = hp ? hp[i] : 0ull;
   }
-  if (bad) {
-    set_error(tv.ctr, ERR_BAD_KEY);
-    len = 1;  // keep later stages in bounds
+  __shared__ uint32_t red[3][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  terms = __reduce_add_sync(0xffffffffu, terms);
+  gaps = __reduce_or_sync(0xffffffffu, gaps);
+  lmax = __reduce_max_sync(0xffffffffu, lmax);
+  if (lane == 0) {
+    red[0][warp] = terms;
+    red[1][warp] = gaps;
+    red[2][warp] = lmax;
   }
-  koff[i] = off;
-  klen[i] = (uint32_t)len;
-  unsigned am = __activemask();
-  uint32_t wmax = __reduce_max_sync(am, (uint32_t)len);
-  if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomicMax(maxlen, wmax);
-  int64_t vs = vi[2 * i], ve = vi[2 * i + 1];
-  if (vs < 0 || ve < vs - 1 || ve >= vbytes || ve - vs + 1 > 0x7FFFFFFF) {  // empty values allowed
-    set_error(tv.ctr, ERR_BAD_KEY);
-    vs = 0;
-    ve = -1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0, g = 0, m = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      t += red[0][w];
+      g |= red[1][w];
+      m = max(m, red[2][w]);
+    }
+    if (t) atomicAdd(&tv.ctr->key_terms, t);
+    if (g) atomicOr(&tv.ctr->noncontig, 1u);
+    if (m) atomicMax(maxlen, m);
   }
-  uint64_t vid = vid_base + (uint64_t)i;
-  tv.rec_off[vid] = val_base + (uint64_t)vs;
-  tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
-  tv.rec_hp[vid] = hp ? hp[i] : 0ull;
 }
 
 // Raw key bytes (the caller skips the hex conversion, util/utils.cuh:340-349
@@ -890,18 +910,43 @@ __global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *d
     if (h[b]) atomicAdd(&bins[b], h[b]);
 }
 
-__global__ void k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, const uint8_t *cls, int n,
-                                uint32_t *cursor, uint32_t *out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t r = ref[i];
-  uint32_t b = dirty_bin(depth[i], r, cls[i]);
-  unsigned peers = __match_any_sync(__activemask(), b);
-  int leader = __ffs(peers) - 1;
-  uint32_t base = 0;
-  if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&cursor[b], (uint32_t)__popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  out[base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1u))] = r;
+// Scatter of the dirty list into its bins, 256 entries per CTA pass.  Counts
+// are aggregated per warp (match_any) and then per CTA in a shared table of
+// the bins the pass touches, so a hot bin (a level of millions of leaves)
+// takes one global atomic per CTA pass instead of one per warp.
+__global__ void __launch_bounds__(256) k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, const uint8_t *cls,
+                                                       int n, uint32_t *cursor, uint32_t *out) {
+  constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+  __shared__ uint32_t tbin[256], tcnt[256], tbase[256];
+  const int lane = threadIdx.x & 31;
+  for (int c0 = blockIdx.x * 256; c0 < n; c0 += gridDim.x * 256) {
+    tbin[threadIdx.x] = kEmpty;
+    tcnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = c0 + threadIdx.x;
+    const bool ok = i < n;
+    const uint32_t r = ok ? ref[i] : 0u;
+    const uint32_t b = ok ? dirty_bin(depth[i], r, cls[i]) : kEmpty;
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0, off = 0;
+    if (ok && lane == leader) {
+      slot = (b * 0x9E3779B1u) >> 24;  // at most 256 bins per pass: a free slot exists
+      while (true) {
+        const uint32_t prev = atomicCAS(&tbin[slot], kEmpty, b);
+        if (prev == kEmpty || prev == b) break;
+        slot = (slot + 1) & 255u;
+      }
+      off = atomicAdd(&tcnt[slot], (uint32_t)__popc(peers));
+    }
+    slot = __shfl_sync(0xffffffffu, slot, leader);
+    off = __shfl_sync(0xffffffffu, off, leader);
+    __syncthreads();
+    if (tbin[threadIdx.x] != kEmpty) tbase[threadIdx.x] = atomicAdd(&cursor[tbin[threadIdx.x]], tcnt[threadIdx.x]);
+    __syncthreads();
+    if (ok) out[tbase[slot] + off + __popc(peers & ((1u << lane) - 1u))] = r;
+    __syncthreads();
+  }
 }
 
 // one message item: <= 8 prefix bytes, then a body read from memory
