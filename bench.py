@@ -104,6 +104,11 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up (driver attach, first query) must not fall
+            # inside the timed region: wait for its first sample
+            t0 = time.time()
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 5.0:
+                time.sleep(0.01)
         except FileNotFoundError:
             self.proc = None
 
@@ -378,7 +383,7 @@ def run_eth(args, local, dev):
         "keys": tot_keys, "tries_touched_per_block": round(float(np.mean([len(b.storage_ids) + 1 for b in blks])), 1),
         "keys_per_block": round(tot_keys / len(blks), 1),
         "block_mkeys_s": blk_rate, "block_p50_ms": round(float(np.percentile(ms_block, 50)), 3),
-        "block_max_ms": round(float(np.max(ms_block)), 3),
+        "block_max_ms": round(float(np.max(ms_block)), 3), "block_max_at": int(np.argmax(ms_block)),
         "block_p99_ms": round(float(np.percentile(ms_block, 99)), 3),
         "e2e_mkeys_s": rate(tot_keys, ms_e2e), "e2e_p50_ms": round(float(np.percentile(ms_e2e, 50)), 3),
         "e2e_p99_ms": round(float(np.percentile(ms_e2e, 99)), 3), "e2e_h2d_bytes": int(h2d),
