@@ -306,6 +306,9 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
         (e = cudaStreamSynchronize(st_)) != cudaSuccess)
       return check_cuda(e, "stage raw scan");
     kbytes = (int64_t)h_small_[0];
+    // malformed pairs are reported (and the error word cleared) before any
+    // other early return, so the next call does not inherit them
+    if (int rc0 = sync_counters()) return rc0;
     if (kbytes >= (1ll << 31)) return fail(E_ARG, "key stream exceeds the int32 index range");
   }
   int rc = ensure_capacity(2ull * n, 4ull * n, (uint64_t)n, (uint64_t)n, (uint64_t)kbytes, (uint64_t)vbytes);
