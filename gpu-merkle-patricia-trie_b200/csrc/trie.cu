@@ -25,7 +25,7 @@ namespace gmpt {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kHashThreads = 128;
+constexpr int kHashThreads = kHashLevelThreads;
 constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);          // (depth, kind)
 constexpr int kHashBins = kMaxDepthBins * (int)kHashClasses;       // (depth, kind, hash class)
 // levels with at most this many branch nodes hash them one warp each

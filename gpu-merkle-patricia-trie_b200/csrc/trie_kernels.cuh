@@ -1420,10 +1420,12 @@ __global__ void __launch_bounds__(128) k_hash_full_warp(TrieView tv, const uint3
 // One level, thread per node; the CTA's 128 nodes are first reordered by
 // hash class (stable counting partition from warp ballots), so warps hold
 // nodes of one Keccak block count.
-__global__ void __launch_bounds__(128, 6) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
+constexpr int kHashLevelThreads = 128;  // k_hash_level's block size (the partition assumes it)
+
+__global__ void __launch_bounds__(kHashLevelThreads, 6) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
-  __shared__ uint32_t s_ref[128];
-  __shared__ uint32_t s_cnt[kHashClasses][4];  // [class][warp]
+  __shared__ uint32_t s_ref[kHashLevelThreads];
+  __shared__ uint32_t s_cnt[kHashClasses][kHashLevelThreads / 32];  // [class][warp]
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool valid = t < count;
@@ -1440,7 +1442,7 @@ __global__ void __launch_bounds__(128, 6) k_hash_level(TrieView tv, const uint32
   if (valid) {
     uint32_t pos = mine;
     for (uint32_t v = 0; v < kHashClasses; ++v)
-      for (int w = 0; w < 4; ++w)
+      for (int w = 0; w < kHashLevelThreads / 32; ++w)
         if (v < c || (v == c && w < warp)) pos += s_cnt[v][w];
     s_ref[pos] = r;
   }
