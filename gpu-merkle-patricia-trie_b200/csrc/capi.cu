@@ -416,6 +416,18 @@ int gmpt_puts_with_read_device(gmpt_trie *t, int two_phase, const uint8_t *d_key
   return puts_with_read(t, two_phase != 0, b, d_rw_flags, d_read_values_hps, d_read_values_sizes, read_num);
 }
 
+int gmpt_deletes(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const int *trie_ids, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  return record_trie(t->t->del(keys_hexs, keys_indexs, n, false, -1, trie_ids), t->t);
+}
+
+int gmpt_deletes_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
+                        int n, int64_t keys_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (keys_bytes < 0) return record(GMPT_E_ARG, "keys_bytes must be given for device keys");
+  return record_trie(t->t->del(d_keys_hexs, d_keys_indexs, n, true, keys_bytes, d_trie_ids), t->t);
+}
+
 int gmpt_hash_onepass(gmpt_trie *t) {
   if (!t) return record(GMPT_E_ARG, "null trie");
   return record_trie(t->t->hash(), t->t);

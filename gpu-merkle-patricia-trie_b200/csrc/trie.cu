@@ -18,6 +18,7 @@
 #include "local_build.cuh"
 #include "local_sort.cuh"
 #include "block_update.cuh"
+#include "delete_kernels.cuh"
 #include "gen_kernels.cuh"
 
 namespace gmpt {
@@ -104,6 +105,7 @@ Trie::~Trie() {
                         &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.dirty_cls, &ws_.rw_flags,
                         &ws_.rw_a, &ws_.rw_b, &ws_.rw_c, &ws_.rw_d, &ws_.rw_e, &ws_.rw_wpos, &ws_.rw_hp,
                         &ws_.rw_len, &ws_.rw_tot, &ws_.rw_kept, &ws_.rw_koff, &ws_.rw_klen, &ws_.rw_tid,
+                        &ws_.del_hslot, &ws_.del_hext, &ws_.del_stamp,
                         &ws_.misc};
   for (DevBlock *b : blocks) b->release();
   for (int k = 0; k < 2; ++k) {
@@ -788,17 +790,10 @@ int Trie::put_2phase(const BatchIn &b) {
   return OK;
 }
 
-// PhaseHC over every node marked dirty since the last hash.
-int Trie::bucket_and_hash() {
+// Counting sort of the nd dirty nodes by (depth, kind, hash class) into
+// ws_.sorted_dirty; off[b] .. off[b + 1] is bin b (dirty_bin).
+int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off) {
   cudaError_t e = cudaSuccess;
-  uint32_t nd = 0;
-  if ((e = cudaMemcpyAsync(h_small_, &ctr_->n_dirty, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
-    return check_cuda(e, "dirty count");
-  nd = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
-  stats_.last_dirty = nd;
-  stats_.last_hash_levels = 0;
-  if (nd == 0) return OK;
   uint32_t *bins = wsp<uint32_t>(ws_.bins, kHashBins + 1, e);
   uint32_t *cursor = wsp<uint32_t>(ws_.cursor, kHashBins + 1, e);
   uint32_t *sorted = wsp<uint32_t>(ws_.sorted_dirty, nd, e);
@@ -808,7 +803,8 @@ int Trie::bucket_and_hash() {
   int grid = std::min<int>(blocks_for(nd), 148 * 4);
   count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kHashBins, st_>>>(tv_, dirty_ref_, dirty_depth_,
                                                                                       (int)nd, bins, kHashBins, cls);
-  std::vector<uint32_t> hb(kHashBins), off(kHashBins + 1);
+  std::vector<uint32_t> hb(kHashBins);
+  off.assign(kHashBins + 1, 0);
   if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kHashBins, cudaMemcpyDeviceToHost, st_)) !=
           cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
@@ -820,6 +816,25 @@ int Trie::bucket_and_hash() {
     return check_cuda(e, "hash cursor");
   count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, cls, (int)nd, cursor,
                                                                         sorted);
+  *sorted_out = sorted;
+  return OK;
+}
+
+// PhaseHC over every node marked dirty since the last hash.
+int Trie::bucket_and_hash() {
+  cudaError_t e = cudaSuccess;
+  uint32_t nd = 0;
+  if ((e = cudaMemcpyAsync(h_small_, &ctr_->n_dirty, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "dirty count");
+  nd = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  stats_.last_dirty = nd;
+  stats_.last_hash_levels = 0;
+  if (nd == 0) return OK;
+  uint32_t *sorted = nullptr;
+  std::vector<uint32_t> off;
+  int rc = bucket_dirty(nd, &sorted, off);
+  if (rc) return rc;
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;
   if ((e = cudaMemsetAsync(&ctr_->hashed, 0, 4, st_)) != cudaSuccess ||
@@ -1829,6 +1844,79 @@ int batch_features_device(const uint8_t *d_keys, const int *d_kidx, int n, int64
 // gpu_mpt.cuh:1715-1823 and 926-982).
 
 namespace gmpt {
+
+int Trie::del(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs, int64_t keys_bytes,
+              const int *trie_ids) {
+  err_.clear();
+  if (n < 0 || n > (1 << 26)) return fail(E_ARG, "batch size must be in [0, 2^26]");
+  if (n == 0) return OK;
+  if (!keys_hexs || !keys_indexs) return fail(E_ARG, "null batch array");
+  cudaSetDevice(dev_);
+  cudaError_t e = cudaSuccess;
+  if (keys_bytes < 0) {
+    if (device_inputs) return fail(E_ARG, "device deletes need keys_bytes");
+    keys_bytes = (int64_t)keys_indexs[2 * n - 1] + 1;
+  }
+  if (keys_bytes < 0) return fail(E_ARG, "bad index pairs");
+  int rc = sync_counters();
+  if (rc) return rc;
+  const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  uint8_t *dk = wsp<uint8_t>(ws_.g_keys, (size_t)keys_bytes + 64, e);
+  int *di = wsp<int>(ws_.g_idx, 2 * (size_t)n, e);
+  int *dtid = trie_ids ? wsp<int>(ws_.g_tid, (size_t)n, e) : nullptr;
+  const size_t nf = (size_t)n_full_ + 1;
+  uint64_t *hslot = wsp<uint64_t>(ws_.del_hslot, nf, e);
+  uint32_t *hext = wsp<uint32_t>(ws_.del_hext, nf, e);
+  uint8_t *stamp = wsp<uint8_t>(ws_.del_stamp, nf, e);
+  unsigned long long *dcnt = wsp<unsigned long long>(ws_.rw_tot, 8, e);  // [0] need, [1] key cursor
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, kind, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  if (e == cudaSuccess && dtid) e = cudaMemcpyAsync(dtid, trie_ids, sizeof(int) * (size_t)n, kind, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(stamp, 0, nf, st_);
+  if (e != cudaSuccess) return check_cuda(e, "delete copy");
+  DirtyList dl{dirty_ref_, dirty_depth_};
+  count_launch(), k_del_walk<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dl, dk, di, n, keys_bytes, dtid, hslot, hext,
+                                                                  stamp);
+  if ((rc = sync_counters())) return rc;
+  const uint32_t nd = h_ctr_->n_dirty;
+  if (nd == 0) return OK;
+  uint32_t *sorted = nullptr;
+  std::vector<uint32_t> off;
+  if ((rc = bucket_dirty(nd, &sorted, off))) return rc;
+  const uint32_t C = kHashClasses;
+  for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
+    const uint32_t a = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];  // branches at depth d
+    if (z == a) continue;
+    const int cnt = (int)(z - a);
+    // room for this level's new keys and short nodes, then collapse
+    if ((e = cudaMemsetAsync(dcnt, 0, 8, st_)) != cudaSuccess) return check_cuda(e, "delete need");
+    count_launch(), k_del_need<<<blocks_for(cnt), kThreads, 0, st_>>>(tv_, sorted + a, cnt, hext, stamp, dcnt);
+    if ((e = cudaMemcpyAsync(h_small_, dcnt, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "delete need");
+    const uint64_t need = h_small_[0];
+    if ((rc = sync_counters())) return rc;
+    if ((rc = ensure_capacity(0, (uint64_t)cnt, 0, 0, need + 64, 0))) return rc;
+    dl = DirtyList{dirty_ref_, dirty_depth_};  // the list may have grown with the short pool
+    h_small_[1] = key_used_;
+    if ((e = cudaMemcpyAsync(dcnt + 1, h_small_ + 1, 8, cudaMemcpyHostToDevice, st_)) != cudaSuccess)
+      return check_cuda(e, "delete cursor");
+    count_launch(), k_del_collapse<<<blocks_for(cnt), kThreads, 0, st_>>>(tv_, dl, sorted + a, cnt, hslot, hext, stamp,
+                                                                          dcnt + 1, cap_keys_);
+    if ((e = cudaMemcpyAsync(h_small_, dcnt + 1, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "delete collapse");
+    key_used_ = (h_small_[0] + 7) & ~7ull;
+    if ((e = cudaMemsetAsync(const_cast<uint8_t *>(tv_.keys) + h_small_[0], 0, 64, st_)) != cudaSuccess)
+      return check_cuda(e, "delete tail");
+  }
+  if ((rc = sync_counters())) return rc;
+  stats_.key_bytes = key_used_;
+  stats_.n_full = n_full_;
+  stats_.n_short = n_short_;
+  return OK;
+}
 
 int Trie::put_rw(const BatchIn &b, const uint8_t *rw, bool two_phase, uint64_t *read_hps, int *read_sizes,
                  int *read_num) {

@@ -99,6 +99,11 @@ class Trie {
   // (host arrays, or device arrays when b.device), *read_num = reads.
   int put_rw(const BatchIn &b, const uint8_t *rw, bool two_phase, uint64_t *read_hps, int *read_sizes,
              int *read_num);
+  // Delete keys (hex keys, as gets; trie ids or null for trie 0; device or
+  // host arrays).  Absent keys are ignored.  The trie becomes the canonical
+  // trie of the remaining keys after hash().
+  int del(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs, int64_t keys_bytes = -1,
+          const int *trie_ids = nullptr);
   int hash();
   int root(uint8_t out[32], int *len, int trie = 0);
   // roots of tries ids[0..n) (host array; null = tries 0..n-1): out32[32 i..]
@@ -227,6 +232,7 @@ class Trie {
     DevBlock dirty_cls;                                         // hash class of each dirty node
     DevBlock rw_flags, rw_a, rw_b, rw_c, rw_d, rw_e, rw_wpos;   // mixed read/write resolution
     DevBlock rw_hp, rw_len, rw_tot, rw_kept, rw_koff, rw_klen, rw_tid;
+    DevBlock del_hslot, del_hext, del_stamp;                    // deletes: how each path branch is linked
     DevBlock misc;
   } ws_;
   RadixSorter sorter_;
@@ -253,6 +259,7 @@ class Trie {
                       uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact = false);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
+  int bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off);
   int sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                  uint32_t **order_out, uint8_t **eqprev_out);
   int sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid, uint32_t **uord_out,

@@ -39,7 +39,7 @@ EXPORTS = [
     "gmpt_reserve_nodes", "gmpt_batch_features_device", "gmpt_puts_pipeline",
     "gmpt_puts_raw", "gmpt_puts_raw_device", "gmpt_puts_pipeline_raw",
     "gmpt_puts_latching_with_read", "gmpt_puts_2phase_with_read", "gmpt_puts_with_read_forest",
-    "gmpt_puts_with_read_device",
+    "gmpt_puts_with_read_device", "gmpt_deletes", "gmpt_deletes_device",
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
@@ -132,6 +132,8 @@ def lib():
     L.gmpt_puts_raw.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32]
     for f in ("gmpt_puts_latching_with_read", "gmpt_puts_2phase_with_read"):
         getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+    L.gmpt_deletes.argtypes = [vp, vp, vp, vp, i32]
+    L.gmpt_deletes_device.argtypes = [vp, vp, vp, vp, i32, i64]
     L.gmpt_puts_with_read_forest.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp]
     L.gmpt_puts_with_read_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, i64, i64, vp, vp, vp]
     L.gmpt_puts_raw_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32, i64, i64]
@@ -362,6 +364,16 @@ class MPT:
         tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
         f = self._L.gmpt_puts_2phase_forest if two_phase else self._L.gmpt_puts_latching_forest
         _check(f(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), _p(tid), len(ki) // 2))
+
+    def deletes(self, keys_hexs, keys_indexs, trie_ids=None):
+        """Remove keys (absent keys are ignored); hash_onepass_v2 afterwards."""
+        kh, ki, _, _ = _arrays(keys_hexs, keys_indexs)
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        _check(self._L.gmpt_deletes(self._h, _p(kh), _p(ki), _p(tid), len(ki) // 2))
+
+    def deletes_device(self, d_keys, d_kidx, n: int, keys_bytes: int, d_tids: int = 0):
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_deletes_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes)))
 
     def puts_with_read(self, two_phase: bool, keys_hexs, keys_indexs, rw_flags, values, values_indexs,
                        trie_ids=None, values_hps=None):

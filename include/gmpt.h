@@ -208,6 +208,19 @@ int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs,
                        const uint8_t *const *const *values_hps, const int *counts, const int *two_phase,
                        uint8_t *roots32, int *root_sizes);
 
+/* ---- deletes ----
+ * Remove keys (hex-nibble keys with terminator, index pairs as for the puts;
+ * trie_ids may be NULL: trie 0); absent keys are ignored.  After
+ * gmpt_hash_onepass the trie is the canonical trie of the remaining keys:
+ * a branch left with one child becomes a short node merged with the
+ * extension above it, an emptied branch disappears.  No counterpart in the
+ * reference, which has no delete path (go-ethereum deletes empty accounts
+ * and zeroed storage slots on commit). */
+int gmpt_deletes(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const int *trie_ids, int n);
+/* The same with DEVICE key / index / trie-id arrays; keys_bytes = key stream length. */
+int gmpt_deletes_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
+                        int n, int64_t keys_bytes);
+
 /* ---- mixed read/write batches ----
  * puts_latching_with_valuehp_v2_with_read (gpu_mpt.cuh:684-765) and
  * puts_2phase_with_valuehp_with_read (gpu_mpt.cuh:1609-1713): rw_flags[i] = 0
