@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--latch-ways", type=int, default=4, help="keys per LockNU thread (1, 2, 4)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-deletes", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=1 << 20)
     p.add_argument("--eth-accounts", type=int, default=30_000_000, help="state trie accounts (0 = skip)")
     p.add_argument("--eth-blocks", type=int, default=512)
@@ -664,6 +665,42 @@ def run_ours(args, world, rank, local):
                                 for k in range(len(dbat))]
     last = stats_all[-1]
 
+    # deletes: load the first batch alone, delete every 16th of its keys and
+    # rehash (timed), then put them back: the root must return exactly to the
+    # load's root (a size-independent check of the delete path at full size)
+    deletes = None
+    if not args.no_deletes:
+        b0, d0 = batches[0], dbat[0]
+        t.set_timing(False)
+        t.reset()
+        t.puts_device(True, d0["k"].data_ptr(), d0["ki"].data_ptr(), d0["v"].data_ptr(), d0["vi"].data_ptr(), d0["n"],
+                      d0["kb"], d0["vb"])
+        t.hash_onepass_v2()
+        root0 = t.get_root_hash()
+        assert root0 == roots_s[0], "load root differs from the timed step's"
+        sub = b0.subset(np.arange(0, b0.n, 16))
+        ds = dict(k=torch.from_numpy(sub.keys_hexs).to(dev), ki=torch.from_numpy(sub.keys_indexs).to(dev),
+                  v=torch.from_numpy(sub.values).to(dev), vi=torch.from_numpy(sub.values_indexs).to(dev))
+        torch.cuda.synchronize(dev)
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        t.deletes_device(ds["k"].data_ptr(), ds["ki"].data_ptr(), sub.n, sub.key_bytes())
+        t.hash_onepass_v2()
+        root_del = t.get_root_hash()
+        z.record(stream)
+        z.synchronize()
+        del_ms = a.elapsed_time(z)
+        t.puts_device(False, ds["k"].data_ptr(), ds["ki"].data_ptr(), ds["v"].data_ptr(), ds["vi"].data_ptr(), sub.n,
+                      sub.key_bytes(), sub.value_bytes())
+        t.hash_onepass_v2()
+        assert t.get_root_hash() == root0, "delete + re-insert did not restore the root"
+        assert root_del != root0
+        deletes = {"keys": int(sub.n), "from_trie_keys": int(b0.n), "ms": round(del_ms, 3),
+                   "mkeys_s": round(sub.n / (del_ms / 1e3) / 1e6, 3), "path": "gmpt_deletes_device + PhaseHC + root",
+                   "roundtrip_root_exact": True}
+        del ds
+
     # e2e: host C ABI from pinned buffers
     e2e = None
     if not args.no_e2e:
@@ -797,6 +834,7 @@ def run_ours(args, world, rank, local):
                    "hash_kernels_ms_per_step": round(hash_ms_step, 3)},
         "clocks": clocks,
         "e2e": e2e,
+        "deletes": deletes,
         "trie": {k: last[-1][1][k] for k in ("n_full", "n_short", "n_value", "last_dirty", "last_hashed")},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
