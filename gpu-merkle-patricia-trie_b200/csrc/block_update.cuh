@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(256, 2) k_block(TrieView tv0, DirtyList dl, Bl
   const int t_spread = lane * W + gw;
   // this warp's message buffer for hash_full_warp, after the staging words
   uint8_t *wmsg = reinterpret_cast<uint8_t *>(smem + 17 * blockDim.x) + (threadIdx.x >> 5) * kWarpMsgBytes;
-  // staging verdict: every CTA reads the same words, so all leave together
+  // staging outcome: every CTA reads the same words, so all leave together
   if (D->bad || D->noncontig || D->stream_terms != D->key_terms) {
     if (t == 0) atomicOr(&D->status, 2u);
     return;

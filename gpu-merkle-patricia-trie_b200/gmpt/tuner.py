@@ -157,7 +157,7 @@ def regret(times_ms: np.ndarray, choice) -> float:
 
 @dataclass
 class Selector:
-    """MLP schedule selector with the autotuned rule as fallback and judge:
+    """MLP schedule selector with the autotuned rule as fallback and yardstick:
     fit() holds out a quarter of the measured batches, and the network is
     used only if its regret there is no worse than the rule's (fit on the
     same three quarters); either way both are then refit on all batches."""

@@ -1,7 +1,7 @@
 """Mixed read/write batches (gmpt_puts_*_with_read) vs a sequential model.
 
 The reference's puts_*_with_read (gpu_mpt.cuh:684-765, 1609-1713) run the
-reads of a batch concurrently with its writes; this build defines the
+reads of a batch concurrently with its writes; the library defines the
 result as the batch applied in index order.  Expected results come from a
 plain dict applied op by op; roots from the oracle trie given the writes.
 """
