@@ -932,7 +932,7 @@ __global__ void __launch_bounds__(256) k_dirty_scatter(const uint32_t *ref, cons
     uint32_t slot = 0, off = 0;
     if (ok && lane == leader) {
       slot = (b * 0x9E3779B1u) >> 24;  // at most 256 bins per pass: a free slot exists
-      while (true) {
+      for (int probe = 0; probe < 256; ++probe) {
         const uint32_t prev = atomicCAS(&tbin[slot], kEmpty, b);
         if (prev == kEmpty || prev == b) break;
         slot = (slot + 1) & 255u;
