@@ -63,3 +63,21 @@ def test_cpp_facade_compiles_against_the_headers(tmp_path):
                         "-L", str(gmpt.LIB_PATH.parent), "-lgmpt_b200", "-o", str(exe)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_entry_points_reject_a_null_trie_without_touching_the_device():
+    # argument checks run before any CUDA call, so they hold on a GPU-less host
+    L = gmpt.lib()
+    E_ARG = 5
+    null = None
+    n = ctypes.c_int(0)
+    assert L.gmpt_deletes(null, null, null, null, 1) == E_ARG
+    assert L.gmpt_deletes_device(null, null, null, null, 1, 16) == E_ARG
+    assert L.gmpt_puts_raw(null, 0, null, null, null, null, null, null, 1) == E_ARG
+    assert L.gmpt_puts_raw_device(null, 1, null, null, null, null, null, null, 1, 8, 8) == E_ARG
+    assert L.gmpt_puts_with_read_forest(null, 0, null, null, null, null, null, null, null, 1, null, null,
+                                        ctypes.byref(n)) == E_ARG
+    assert L.gmpt_puts_latching_with_read(null, null, null, ctypes.byref(n), null, null, null, null, 1, null,
+                                          null) == E_ARG
+    assert L.gmpt_puts_pipeline_raw(null, 1, null, null, null, null, null, null, null, null, null) == E_ARG
+    assert b"null" in L.gmpt_last_error_message()
