@@ -375,8 +375,12 @@ __device__ __forceinline__ uint64_t dedup_home(uint64_t h, uint64_t mask) {
   return ((h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull >> 17) & mask;
 }
 
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+
+// slot_of[i] = the slot key i's hash landed in (kNoSlot if the table was
+// full), so the passes after it need not hash and probe again
 __global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
-                               DedupTable t) {
+                               DedupTable t, uint32_t *slot_of) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned long long h = dedup_hash(tv.keys + koff[i], klen[i], tid ? (uint32_t)tid[i] : 0u, t.hmask);
@@ -389,27 +393,22 @@ __global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t
     if (old == kDedupEmpty) old = atomicCAS(&t.hash[s], kDedupEmpty, h);
     if (old == kDedupEmpty || old == h) {
       if (__ldcg(&t.pos[s]) < (uint32_t)i) atomicMax(&t.pos[s], (uint32_t)i);
+      slot_of[i] = (uint32_t)s;
       return;
     }
   }
+  slot_of[i] = kNoSlot;
 }
 
 __global__ void k_dedup_mark(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
-                             DedupTable t, unsigned long long *keep, uint32_t *collision) {
+                             DedupTable t, const uint32_t *slot_of, unsigned long long *keep, uint32_t *collision) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
   const uint8_t *k = tv.keys + koff[i];
   const uint32_t len = klen[i];
-  const unsigned long long h = dedup_hash(k, len, tr, t.hmask);
-  uint64_t s = dedup_home(h, t.mask);
-  bool found = false;
-  for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask)
-    if (t.hash[s] == h) {
-      found = true;
-      break;
-    }
-  if (!found) {  // cannot happen after k_dedup_insert; walk every key then
+  const uint32_t s = slot_of[i];
+  if (s == kNoSlot) {  // cannot happen (the table has 2n slots); walk every key then
     atomicOr(collision, 1u);
     keep[i] = 1ull;
     return;
@@ -429,20 +428,15 @@ __global__ void k_dedup_mark(TrieView tv, const uint64_t *koff, const uint32_t *
 // equal keys in batch order.  A key unequal to its slot's representative (a
 // hash collision) sets *collision: the caller sorts by full keys instead.
 __global__ void k_rw_slots(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
-                           DedupTable t, uint64_t *skey, uint32_t *sval, uint32_t *collision) {
+                           DedupTable t, const uint32_t *slot_of, uint64_t *skey, uint32_t *sval,
+                           uint32_t *collision) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t tr = tid ? (uint32_t)tid[i] : 0u;
   const uint8_t *k = tv.keys + koff[i];
   const uint32_t len = klen[i];
-  const unsigned long long h = dedup_hash(k, len, tr, t.hmask);
-  uint64_t s = dedup_home(h, t.mask);
-  bool found = false;
-  for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask)
-    if (t.hash[s] == h) {
-      found = true;
-      break;
-    }
+  uint32_t s = slot_of[i];
+  const bool found = s != kNoSlot;
   if (!found) {
     atomicOr(collision, 1u);
     s = 0;

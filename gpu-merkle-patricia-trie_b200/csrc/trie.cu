@@ -102,7 +102,7 @@ Trie::~Trie() {
                         &ws_.sb_len, &ws_.sb_ref, &ws_.sb_d0, &ws_.sb_slot, &ws_.sb_code, &ws_.lcp,
                         &ws_.act2, &ws_.aseg, &ws_.aseg2, &ws_.kflags, &ws_.knib, &ws_.bins, &ws_.cursor,
                         &ws_.sorted_dirty, &ws_.g_keys, &ws_.g_idx, &ws_.g_hp, &ws_.g_len, &ws_.g_tid,
-                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.raw, &ws_.dirty_cls, &ws_.rw_flags,
+                        &ws_.tid, &ws_.dd_hash, &ws_.dd_pos, &ws_.dd_sel, &ws_.dd_slot, &ws_.raw, &ws_.dirty_cls, &ws_.rw_flags,
                         &ws_.rw_a, &ws_.rw_b, &ws_.rw_c, &ws_.rw_d, &ws_.rw_e, &ws_.rw_wpos, &ws_.rw_hp,
                         &ws_.rw_len, &ws_.rw_tot, &ws_.rw_kept, &ws_.rw_koff, &ws_.rw_klen, &ws_.rw_tid,
                         &ws_.del_hslot, &ws_.del_hext, &ws_.del_stamp,
@@ -494,8 +494,11 @@ int Trie::sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t ma
   if (e != cudaSuccess) return check_cuda(e, "rw group alloc");
   const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
   DedupTable tab{hash, hpos, size - 1, hmask};
-  count_launch(), k_dedup_insert<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab);
-  count_launch(), k_rw_slots<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, skey, sval, collision);
+  uint32_t *slot_of = wsp<uint32_t>(ws_.dd_slot, (size_t)n, e);
+  if (e != cudaSuccess) return check_cuda(e, "rw group alloc");
+  count_launch(), k_dedup_insert<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, slot_of);
+  count_launch(), k_rw_slots<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, slot_of, skey, sval,
+                                                                  collision);
   if ((e = cudaMemcpyAsync(h_small_, collision, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st_)) != cudaSuccess)
     return check_cuda(e, "rw group");
@@ -1110,8 +1113,10 @@ int Trie::put_latching(const BatchIn &b) {
     if (e != cudaSuccess) return check_cuda(e, "dedup alloc");
     const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
     DedupTable tab{hash, pos, size - 1, hmask};
-    count_launch(), k_dedup_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab);
-    count_launch(), k_dedup_mark<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab, keep,
+    uint32_t *slot_of = wsp<uint32_t>(ws_.dd_slot, (size_t)b.n, e);
+    if (e != cudaSuccess) return check_cuda(e, "dedup alloc");
+    count_launch(), k_dedup_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab, slot_of);
+    count_launch(), k_dedup_mark<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab, slot_of, keep,
                                                                         collision);
     if ((e = exclusive_scan<unsigned long long>(keep, rank, b.n, d_tot, scan_ws_, st_)) != cudaSuccess)
       return check_cuda(e, "dedup scan");

@@ -227,7 +227,7 @@ class Trie {
     DevBlock bins, cursor, sorted_dirty;                        // hash buckets
     DevBlock g_keys, g_idx, g_hp, g_len, g_tid;                 // gets
     DevBlock tid;                                               // trie ids of the batch
-    DevBlock dd_hash, dd_pos, dd_sel;                           // LockNU batch dedup
+    DevBlock dd_hash, dd_pos, dd_sel, dd_slot;                  // LockNU batch dedup
     DevBlock raw;                                               // raw key bytes of the batch
     DevBlock dirty_cls;                                         // hash class of each dirty node
     DevBlock rw_flags, rw_a, rw_b, rw_c, rw_d, rw_e, rw_wpos;   // mixed read/write resolution
