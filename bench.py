@@ -821,8 +821,8 @@ def run_ours(args, world, rank, local):
                      "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4),
                      "traffic": int(HASH_TRAFFIC_B_PER_NODE * nodes_per_launch),
-                     "traffic_source": "ncu dram__bytes_read+write per hashed node of the largest 1M-key YCSB level "
-                                       "(profiles/k_hash_level_ycsb1m.md) x hashed nodes per level here",
+                     "traffic_source": "ncu dram__bytes_read+write per hashed node of the largest level of a "
+                                       "1M-key YCSB load, scaled by the hashed nodes per level of this run",
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": int(alg_bytes_per_launch),
                      "avg_launch_us": round(avg_launch_s * 1e6, 2)},

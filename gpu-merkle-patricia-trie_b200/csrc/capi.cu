@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI (include/gmpt.h and the reference's include/libgmpt.h)
 // over gmpt::Trie.  No exceptions or exits cross the boundary.
 #include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -493,7 +494,9 @@ int gmpt_keccak256_batch(const uint8_t *data, const int64_t *indexs, int n, uint
   if (n == 0) return record(0, "");
   int64_t bytes = 0;
   for (int i = 0; i < n; ++i) {
-    if (indexs[2 * i] < 0 || indexs[2 * i + 1] < indexs[2 * i] - 1) return record(GMPT_E_ARG, "bad index pair");
+    // the end is bounded before the + 1 (an end near INT64_MAX would wrap)
+    if (indexs[2 * i] < 0 || indexs[2 * i + 1] < indexs[2 * i] - 1 || indexs[2 * i + 1] >= INT64_MAX - 64)
+      return record(GMPT_E_ARG, "bad index pair");
     bytes = std::max<int64_t>(bytes, indexs[2 * i + 1] + 1);
   }
   uint8_t *d_data = nullptr, *d_out = nullptr;

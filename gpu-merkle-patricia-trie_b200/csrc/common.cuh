@@ -91,6 +91,7 @@ struct TrieView {
   uint32_t epoch;         // put batch number (split claims)
   uint32_t gen;           // hash generation (dirty marks)
   int geth_mode;          // 1 = embed <32 B children, hash the root always
+  int account;            // 1 = hash kernels count encoding bytes / blocks / nodes (timing mode)
 };
 
 // ---------------------------------------------------------------------------

@@ -817,8 +817,8 @@ int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t>
   if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kHashBins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
-  count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(dirty_ref_, dirty_depth_, cls, (int)nd, cursor,
-                                                                        sorted);
+  count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(
+                      dirty_ref_, dirty_depth_, cls, (int)nd, cursor, sorted, ctr_);
   *sorted_out = sorted;
   return OK;
 }
@@ -850,6 +850,7 @@ int Trie::bucket_and_hash() {
     cudaEventRecord(ka, st_);
   }
   const size_t smem_warp = smem + 4 * kWarpMsgBytes;
+  tv_.account = timing_ ? 1 : 0;  // per-node accounting atomics only when measuring
   for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
     const uint32_t C = kHashClasses;
     uint32_t a = off[2 * d * C], m = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];
@@ -873,6 +874,7 @@ int Trie::bucket_and_hash() {
     cudaEventDestroy(ka);
     cudaEventDestroy(kz);
   }
+  tv_.account = 0;
   stats_.last_hash_levels = levels;
   stats_.hash_launches = levels;
   if ((e = cudaMemsetAsync(&ctr_->n_dirty, 0, 4, st_)) != cudaSuccess) return check_cuda(e, "hash reset");
@@ -1310,12 +1312,13 @@ int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, u
       err = "bad index pair";
       return E_ARG;
     }
+    // bounded before the + 1, so an end near INT64_MAX cannot wrap past the check
+    if (indexs[2 * i + 1] >= kNoAllocMaxBytes) {
+      err = "gmpt_keccak256_batch_noalloc: message bytes up to index " + std::to_string(indexs[2 * i + 1]) +
+            " exceed the limit of " + std::to_string(kNoAllocMaxBytes);
+      return E_ARG;
+    }
     bytes = std::max<int64_t>(bytes, indexs[2 * i + 1] + 1);
-  }
-  if (bytes > kNoAllocMaxBytes) {
-    err = "gmpt_keccak256_batch_noalloc: " + std::to_string(bytes) + " message bytes exceed the limit of " +
-          std::to_string(kNoAllocMaxBytes);
-    return E_ARG;
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -1339,16 +1342,22 @@ int keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, u
   uint8_t *d_data = base;
   int64_t *d_idx = reinterpret_cast<int64_t *>(base + kNoAllocIdxOff);
   uint8_t *d_out = base + kNoAllocOutOff;
-  // legacy default stream, synchronous copies from pageable memory
-  if (bytes) e = cudaMemcpy(d_data, data, (size_t)bytes, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(d_data + bytes, 0, kNoAllocTail);  // what the over-reads see
-  if (e == cudaSuccess) e = cudaMemcpy(d_idx, indexs, sizeof(int64_t) * 2 * (size_t)n, cudaMemcpyHostToDevice);
+  // The calling thread's per-thread default stream: it does not wait for the
+  // library's own or the caller's non-blocking streams (only for the legacy
+  // default stream, if the process uses that one too).
+  cudaStream_t st = cudaStreamPerThread;
+  if (bytes) e = cudaMemcpyAsync(d_data, data, (size_t)bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_data + bytes, 0, kNoAllocTail, st);  // what the over-reads see
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_idx, indexs, sizeof(int64_t) * 2 * (size_t)n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
     size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
-    count_launch(), k_keccak256_batch<<<blocks_for(n, kHashThreads), kHashThreads, smem>>>(d_data, d_idx, n, d_out);
+    count_launch(),
+        k_keccak256_batch<<<blocks_for(n, kHashThreads), kHashThreads, smem, st>>>(d_data, d_idx, n, d_out);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaMemcpy(out32, d_out, 32 * (size_t)n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out32, d_out, 32 * (size_t)n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("keccak no-alloc: ") + cudaGetErrorString(e);
     return E_CUDA;
@@ -1912,8 +1921,13 @@ int Trie::del(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool devi
     if ((e = cudaMemcpyAsync(h_small_, dcnt + 1, 8, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st_)) != cudaSuccess)
       return check_cuda(e, "delete collapse");
-    key_used_ = (h_small_[0] + 7) & ~7ull;
-    if ((e = cudaMemsetAsync(const_cast<uint8_t *>(tv_.keys) + h_small_[0], 0, 64, st_)) != cudaSuccess)
+    const uint64_t cursor = h_small_[0];
+    // k_del_collapse advances the cursor even when a level's key bytes did
+    // not fit (it then raises ERR_CAPACITY): check before the arena is touched
+    if ((rc = sync_counters())) return rc;
+    if (cursor + 64 > cap_keys_) return fail(E_CAPACITY, "key arena capacity exceeded by a delete collapse");
+    key_used_ = (cursor + 7) & ~7ull;
+    if ((e = cudaMemsetAsync(const_cast<uint8_t *>(tv_.keys) + cursor, 0, 64, st_)) != cudaSuccess)
       return check_cuda(e, "delete tail");
   }
   if ((rc = sync_counters())) return rc;

@@ -915,7 +915,7 @@ __global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *d
 // the bins the pass touches, so a hot bin (a level of millions of leaves)
 // takes one global atomic per CTA pass instead of one per warp.
 __global__ void __launch_bounds__(256) k_dirty_scatter(const uint32_t *ref, const uint16_t *depth, const uint8_t *cls,
-                                                       int n, uint32_t *cursor, uint32_t *out) {
+                                                       int n, uint32_t *cursor, uint32_t *out, Counters *ctr) {
   constexpr uint32_t kEmpty = 0xFFFFFFFFu;
   __shared__ uint32_t tbin[256], tcnt[256], tbase[256];
   const int lane = threadIdx.x & 31;
@@ -929,22 +929,31 @@ __global__ void __launch_bounds__(256) k_dirty_scatter(const uint32_t *ref, cons
     const uint32_t b = ok ? dirty_bin(depth[i], r, cls[i]) : kEmpty;
     const unsigned peers = __match_any_sync(0xffffffffu, b);
     const int leader = __ffs(peers) - 1;
-    uint32_t slot = 0, off = 0;
+    uint32_t slot = 0, off = 0, claimed = 0;
     if (ok && lane == leader) {
       slot = (b * 0x9E3779B1u) >> 24;  // at most 256 bins per pass: a free slot exists
       for (int probe = 0; probe < 256; ++probe) {
         const uint32_t prev = atomicCAS(&tbin[slot], kEmpty, b);
-        if (prev == kEmpty || prev == b) break;
+        if (prev == kEmpty || prev == b) {
+          claimed = 1;
+          break;
+        }
         slot = (slot + 1) & 255u;
       }
-      off = atomicAdd(&tcnt[slot], (uint32_t)__popc(peers));
+      // no slot of this bin (cannot happen with <= 256 bins per pass): report
+      // it and leave the entries out rather than count them in another bin
+      if (claimed)
+        off = atomicAdd(&tcnt[slot], (uint32_t)__popc(peers));
+      else
+        set_error(ctr, ERR_INTERNAL);
     }
     slot = __shfl_sync(0xffffffffu, slot, leader);
     off = __shfl_sync(0xffffffffu, off, leader);
+    claimed = __shfl_sync(0xffffffffu, claimed, leader);
     __syncthreads();
     if (tbin[threadIdx.x] != kEmpty) tbase[threadIdx.x] = atomicAdd(&cursor[tbin[threadIdx.x]], tcnt[threadIdx.x]);
     __syncthreads();
-    if (ok) out[tbase[slot] + off + __popc(peers & ((1u << lane) - 1u))] = r;
+    if (ok && claimed) out[tbase[slot] + off + __popc(peers & ((1u << lane) - 1u))] = r;
     __syncthreads();
   }
 }
@@ -1288,7 +1297,7 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
     if (last) break;
   }
   }
-  {  // accounting: encoding bytes and absorbed blocks of this pass
+  if (tv.account) {  // accounting (timing mode): encoding bytes and absorbed blocks of this pass
     unsigned am = __activemask();
     unsigned long long eb = __reduce_add_sync(am, (uint32_t)total);
     unsigned long long kb = __reduce_add_sync(am, raw ? 0u : (uint32_t)((total + 1 + 135) / 136));
@@ -1391,9 +1400,11 @@ __device__ __forceinline__ bool hash_full_warp(const TrieView &tv, uint32_t idx,
       o[3] = a[3];
       tv.full_hlen[idx] = 32;
     }
-    atomicAdd(&tv.ctr->enc_bytes, (unsigned long long)total);
-    atomicAdd(&tv.ctr->keccak_blocks, (unsigned long long)(raw ? 0u : nblk));
-    atomicAdd(&tv.ctr->hashed, 1u);
+    if (tv.account) {
+      atomicAdd(&tv.ctr->enc_bytes, (unsigned long long)total);
+      atomicAdd(&tv.ctr->keccak_blocks, (unsigned long long)(raw ? 0u : nblk));
+      atomicAdd(&tv.ctr->hashed, 1u);
+    }
   }
   __syncwarp();
   (void)stage;

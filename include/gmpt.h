@@ -49,7 +49,7 @@ typedef struct gmpt_stats {
   uint64_t device_bytes;
   uint32_t sort_passes, build_levels;
   float t_stage_ms, t_sort_ms, t_walk_ms, t_build_ms, t_hash_ms;
-  uint64_t last_hashed, last_enc_bytes, last_keccak_blocks; /* last PhaseHC pass */
+  uint64_t last_hashed, last_enc_bytes, last_keccak_blocks; /* last PhaseHC pass (timing mode only, else 0) */
   float t_hash_kernels_ms; /* encode+Keccak kernels of the last pass (timing mode) */
   uint32_t hash_launches, pad;
 } gmpt_stats;
@@ -215,7 +215,13 @@ int gmpt_puts_pipeline(gmpt_trie *t, int count, const uint8_t *const *keys_hexs,
  * a branch left with one child becomes a short node merged with the
  * extension above it, an emptied branch disappears.  No counterpart in the
  * reference, which has no delete path (go-ethereum deletes empty accounts
- * and zeroed storage slots on commit). */
+ * and zeroed storage slots on commit).
+ * Space is not reclaimed: unlinked branches, dead short nodes, the deleted
+ * keys' value records and the old key bytes stay in the pools and arenas,
+ * and every collapsed branch appends one short node plus its merged key
+ * (extension key + 1 + the child's key, in nibbles) to them.  A workload
+ * that deletes and re-inserts keys block after block grows the pools until
+ * gmpt_reset, or until the live keys are re-loaded into a fresh trie. */
 int gmpt_deletes(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs, const int *trie_ids, int n);
 /* The same with DEVICE key / index / trie-id arrays; keys_bytes = key stream length. */
 int gmpt_deletes_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
@@ -344,18 +350,26 @@ int gmpt_keccak256_batch_device(const uint8_t *d_data, const int64_t *d_indexs, 
  * reference.  For callers that cannot allocate device memory at the point of
  * the call: a process whose device memory is already owned by another
  * allocator (a framework's caching allocator that reserved the GPU), or code
- * that must not trigger cudaMalloc/cudaFree and the device-wide
- * synchronisation they can cause.  Same inputs, outputs and results as
- * gmpt_keccak256_batch (host arrays), but every device-side copy goes
- * through one fixed 3.5 MiB array inside the library that each GPU loading
- * the library keeps until the process exits.
- * Limits: at most 32768 messages and 2 MiB of message bytes per call
- * (larger calls fail with GMPT_E_ARG and a message naming the limit).
- * The first call on a device looks up that array's device address (set-up,
- * done once per device, on the current device); make that first call before
- * any stream capture.  All calls share the one array, so calls from this
- * process are serialised; work that overlaps a call on the same GPU through
- * other means races with it. */
+ * that must not call cudaMalloc/cudaFree there.  Same inputs, outputs and
+ * results as gmpt_keccak256_batch (host arrays), but every device-side copy
+ * goes through one fixed 3.5 MiB array inside the library that each GPU
+ * loading the library keeps until the process exits.
+ * Limits: at most 32768 messages and 2 MiB of message bytes per call (every
+ * end index below 2^21); larger calls fail with GMPT_E_ARG and a message
+ * naming the limit, before any device work.
+ * Memory: the array lives in the library's device module.  CUDA loads that
+ * module, and allocates its memory (the array included), on the first call
+ * on a device that uses any of the library's kernels -- this function's
+ * first call, or any earlier library call.  Callers whose device memory is
+ * later handed to another allocator should make one call before that.  The
+ * first call on a device also looks up the array's device address (set-up,
+ * once per device, on the current device); make that first call before any
+ * stream capture.
+ * Ordering: the copies and the kernel run on the calling thread's per-thread
+ * default stream (cudaStreamPerThread), and the call returns when they have
+ * finished; they do not wait for other non-blocking streams.  All calls share
+ * the one array, so calls from this process are serialised; work that
+ * overlaps a call on the same GPU through other means races with it. */
 int gmpt_keccak256_batch_noalloc(const uint8_t *data, const int64_t *indexs, int n, uint8_t *out32);
 /* Measurement aid: Keccak-f[1600] permutations per second of a
  * register-only loop on `device` (the integer-pipe ceiling of the hash

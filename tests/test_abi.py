@@ -81,3 +81,20 @@ def test_entry_points_reject_a_null_trie_without_touching_the_device():
                                           null) == E_ARG
     assert L.gmpt_puts_pipeline_raw(null, 1, null, null, null, null, null, null, null, null, null) == E_ARG
     assert b"null" in L.gmpt_last_error_message()
+
+
+def test_keccak_batches_reject_an_end_index_that_would_overflow():
+    # an end index near INT64_MAX must fail the argument check (before any
+    # CUDA call), not wrap to a small byte count in `end + 1`
+    L = gmpt.lib()
+    E_ARG = 5
+    data = (ctypes.c_uint8 * 16)()
+    out = (ctypes.c_uint8 * 32)()
+    for end in (2 ** 63 - 1, 2 ** 63 - 2, 2 ** 63 - 60):
+        idx = (ctypes.c_int64 * 2)(0, end)
+        assert L.gmpt_keccak256_batch(data, idx, 1, out) == E_ARG
+        assert L.gmpt_keccak256_batch_noalloc(data, idx, 1, out) == E_ARG
+    # the no-alloc limit is checked per pair, before any device work
+    idx = (ctypes.c_int64 * 2)(0, 2 << 20)
+    assert L.gmpt_keccak256_batch_noalloc(data, idx, 1, out) == E_ARG
+    assert b"limit" in L.gmpt_last_error_message()
