@@ -146,6 +146,17 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 
 
+def golden_roots(n):
+    """Oracle roots of the YCSB load + update configuration at n keys, when
+    the committed golden file has them (else None)."""
+    path = REPO / "tests" / "golden" / "config_roots.json"
+    if not path.exists():
+        return None
+    cases = json.loads(path.read_text())["cases"]
+    name = {1 << 24: "c2_ycsb_16m", 1 << 20: "c2_ycsb_1m"}.get(n)
+    return cases[name]["roots"] if name in cases else None
+
+
 def make_workload(n):
     load = W.ycsb_load(n, seed=0x5EED0002)
     upd = W.ycsb_zipf_updates(n, n, seed=0x5EED0003)
@@ -634,6 +645,11 @@ def run_ours(args, world, rank, local):
     barrier()
     clocks = sampler.stop()
     launches_per_step = (gmpt.launch_count() - launches0) / args.steps
+    # the full-size configuration's roots were computed by the oracle on the
+    # CPU (tests/golden/make_config_roots.py): the timed step must reach them
+    golden = golden_roots(args.n)
+    if golden is not None:
+        assert [r.hex() for r in roots_s] == golden, "roots differ from the oracle's for this configuration"
     step_ms = [a.elapsed_time(z) for a, z in ev]
     ms = statistics.mean(step_ms)
     if world > 1:
@@ -816,6 +832,7 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}"},
         "gpu_launches": int(round(launches_per_step)),
         "roots": [r.hex() for r in roots_s],
+        "roots_match_oracle": golden is not None,
         "phases_ms": phase,
         "roofline": {"bound": "hbm", "kernel": "k_hash_level (fused RLP encode + Keccak-256)",
                      "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",

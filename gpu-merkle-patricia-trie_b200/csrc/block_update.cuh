@@ -38,6 +38,7 @@ struct BlockDesc {
   int64_t kbytes, vbytes;          // stream lengths
   uint64_t key_base, val_base, vid_base;
   uint32_t gen, pad1;              // dirty generation of stage 0 (stage 1: gen + 1)
+  uint64_t barrier_ns;             // longest grid-barrier wait before giving up
   uint32_t bar_count, bar_gen;     // grid barrier
   // filled by k_block_stage
   uint32_t stream_terms, key_terms, noncontig, bad;  // bad: BLOCK_BAD_* bits
@@ -74,9 +75,10 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// A barrier wait longer than this gives up: the CTA raises ERR_BARRIER and
-// leaves the kernel, and so does every CTA at its next barrier.
-constexpr uint64_t kBarrierWaitNs = 2000000000ull;
+// A barrier wait longer than BlockDesc::barrier_ns (2 s unless the trie's
+// "block_barrier_ns" option says otherwise) gives up: the CTA raises
+// ERR_BARRIER and leaves the kernel, and so does every CTA at its next
+// barrier.
 
 // Grid-wide barrier of a cooperative launch (all CTAs co-resident).
 // Returns false when this CTA must stop.
@@ -95,10 +97,11 @@ __device__ bool grid_barrier(BlockDesc *D, Counters *ctr) {
       atomicAdd(&D->bar_gen, 1u);
     } else {
       const uint64_t t0 = global_ns();
+      const uint64_t limit = D->barrier_ns;
       uint32_t spins = 0;
       while (*vgen == g) {
         __nanosleep(64);
-        if ((++spins & 63) == 0 && global_ns() - t0 > kBarrierWaitNs) {
+        if ((++spins & 63) == 0 && global_ns() - t0 > limit) {
           ok = 0;
           break;
         }

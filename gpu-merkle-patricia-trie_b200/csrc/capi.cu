@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI (include/gmpt.h and the reference's include/libgmpt.h)
 // over gmpt::Trie.  No exceptions or exits cross the boundary.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -12,6 +13,7 @@
 #include "../../include/gmpt.h"
 #include "../../include/libgmpt.h"
 #include "mlp.h"
+#include "schedule.h"
 #include "trie.h"
 
 struct gmpt_trie {
@@ -20,6 +22,10 @@ struct gmpt_trie {
 
 struct gmpt_mlp {
   gmpt::Mlp *m;
+};
+
+struct gmpt_selector {
+  gmpt::Selector *s;
 };
 
 namespace {
@@ -476,6 +482,164 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out) {
   return record(0, "");
 }
 
+// ---- schedules and the selector ----
+
+int gmpt_schedule_count(void) { return gmpt::schedule_count(); }
+
+const char *gmpt_schedule_name(int k) {
+  const gmpt::Schedule *s = gmpt::schedule_at(k);
+  return s ? s->name : nullptr;
+}
+
+int gmpt_schedule_info(int k, int out[8]) {
+  const gmpt::Schedule *s = gmpt::schedule_at(k);
+  if (!s || !out) return record(GMPT_E_ARG, "schedule index out of range or null output");
+  out[0] = s->two_phase;
+  out[1] = s->persistent;
+  out[2] = s->local_build;
+  out[3] = s->local_sort;
+  out[4] = s->latch_ways;
+  out[5] = s->latch_dedup;
+  out[6] = s->block_grid;
+  out[7] = s->warp_full_max;
+  return record(0, "");
+}
+
+int gmpt_puts_schedule(gmpt_trie *t, int k, const uint8_t *keys_hexs, const int *keys_indexs,
+                       const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                       const int *trie_ids, int n) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (!gmpt::schedule_at(k)) return record(GMPT_E_ARG, "schedule index out of range");
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  return record_trie(gmpt::put_schedule(*t->t, k, b), t->t);
+}
+
+int gmpt_puts_schedule_device(gmpt_trie *t, int k, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                              const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids,
+                              int n, int64_t keys_bytes, int64_t values_bytes) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (!gmpt::schedule_at(k)) return record(GMPT_E_ARG, "schedule index out of range");
+  gmpt::BatchIn b = device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs, nullptr, n, keys_bytes,
+                                 values_bytes);
+  b.trie_ids = d_trie_ids;
+  return record_trie(gmpt::put_schedule(*t->t, k, b), t->t);
+}
+
+// tries_touched > 0 / trie_keys >= 0: the caller's counts for out[7] / out[4]
+// (a forest caller knows which tries a batch touches and how many keys they hold)
+static int features_call(gmpt_trie *t, const gmpt::BatchIn &b, int tries_touched, int64_t trie_keys, float *out) {
+  if (!t || !out) return record(GMPT_E_ARG, "null argument");
+  std::string err;
+  int rc = gmpt::batch_features(*t->t, b, out, err);
+  if (!rc && tries_touched > 0) out[7] = (float)std::log2((double)tries_touched);
+  if (!rc && trie_keys >= 0) out[4] = (float)std::log2((double)trie_keys + 1.0);
+  return record(rc, err);
+}
+
+int gmpt_batch_features(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                        const int64_t *values_indexs, const int *trie_ids, int n, float out[8]) {
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, nullptr, values_indexs, nullptr, n);
+  b.trie_ids = trie_ids;
+  return features_call(t, b, 0, -1, out);
+}
+
+int gmpt_batch_features_trie_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, int n,
+                                    int64_t keys_bytes, int64_t values_bytes, int tries_touched, int64_t trie_keys,
+                                    float out[8]) {
+  gmpt::BatchIn b = device_batch(d_keys_hexs, d_keys_indexs, nullptr, nullptr, nullptr, n, keys_bytes, values_bytes);
+  return features_call(t, b, tries_touched, trie_keys, out);
+}
+
+gmpt_selector *gmpt_selector_create(int device, const char *path) {
+  gmpt_selector *h = new (std::nothrow) gmpt_selector{nullptr};
+  if (!h || !(h->s = new (std::nothrow) gmpt::Selector(device))) {
+    delete h;
+    record(GMPT_E_CAPACITY, "out of host memory");
+    return nullptr;
+  }
+  if (path && h->s->load(path)) {
+    record(GMPT_E_ARG, h->s->error());
+    delete h->s;
+    delete h;
+    return nullptr;
+  }
+  record(0, "");
+  return h;
+}
+
+void gmpt_selector_destroy(gmpt_selector *s) {
+  if (!s) return;
+  delete s->s;
+  delete s;
+}
+
+int gmpt_selector_choose(gmpt_selector *s, const float features[8], int *schedule, int *used_net) {
+  if (!s || !features || !schedule) return record(GMPT_E_ARG, "null argument");
+  bool net = false;
+  int rc = s->s->choose(features, schedule, &net);
+  if (used_net) *used_net = net ? 1 : 0;
+  return record(rc, rc ? s->s->error() : std::string());
+}
+
+int gmpt_selector_counts(gmpt_selector *s, uint64_t out[2]) {
+  if (!s || !out) return record(GMPT_E_ARG, "null argument");
+  out[0] = s->s->choices();
+  out[1] = s->s->fallbacks();
+  return record(0, "");
+}
+
+// The library's own selector of each device (built-in rule, or the file
+// named by GMPT_SELECTOR), used when a caller passes none.
+static std::mutex g_sel_mu;
+static gmpt_selector *g_sel[64] = {};
+
+static gmpt_selector *default_selector(int device) {
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> g(g_sel_mu);
+  if (!g_sel[device]) g_sel[device] = gmpt_selector_create(device, std::getenv("GMPT_SELECTOR"));
+  return g_sel[device];
+}
+
+static int auto_call(gmpt_trie *t, gmpt_selector *sel, const gmpt::BatchIn &b, int tries_touched, int64_t trie_keys,
+                     int *chosen) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (chosen) *chosen = -1;
+  if (b.n == 0) return record(0, "");
+  if (!sel && !(sel = default_selector(t->t->device()))) return gmpt_last_error();
+  float f[8];
+  int rc = features_call(t, b, tries_touched, trie_keys, f);
+  if (rc) return rc;
+  int k = 0, net = 0;
+  if ((rc = gmpt_selector_choose(sel, f, &k, &net))) return rc;
+  if (chosen) *chosen = k;
+  return record_trie(gmpt::put_schedule(*t->t, k, b), t->t);
+}
+
+int gmpt_puts_auto(gmpt_trie *t, gmpt_selector *sel, const uint8_t *keys_hexs, const int *keys_indexs,
+                   const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                   const int *trie_ids, int n, int *chosen) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (n < 0 || (n > 0 && (!keys_hexs || !keys_indexs || !values_bytes || !values_indexs)))
+    return record(GMPT_E_ARG, "null batch array");
+  gmpt::BatchIn b = host_batch(keys_hexs, keys_indexs, values_bytes, values_indexs, values_hps, n);
+  b.trie_ids = trie_ids;
+  return auto_call(t, sel, b, 0, -1, chosen);
+}
+
+int gmpt_puts_auto_device(gmpt_trie *t, gmpt_selector *sel, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                          const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids, int n,
+                          int64_t keys_bytes, int64_t values_bytes, int tries_touched, int64_t trie_keys,
+                          int *chosen) {
+  if (!t) return record(GMPT_E_ARG, "null trie");
+  if (n < 0 || (n > 0 && (!d_keys_hexs || !d_keys_indexs || !d_values_bytes || !d_values_indexs)))
+    return record(GMPT_E_ARG, "null batch array");
+  gmpt::BatchIn b = device_batch(d_keys_hexs, d_keys_indexs, d_values_bytes, d_values_indexs, nullptr, n, keys_bytes,
+                                 values_bytes);
+  b.trie_ids = d_trie_ids;
+  return auto_call(t, sel, b, tries_touched, trie_keys, chosen);
+}
+
 int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value) {
   if (!t || !name) return record(GMPT_E_ARG, "null argument");
   return record_trie(t->t->set_option(name, value), t->t);
@@ -611,10 +775,18 @@ static const uint8_t *insert_hash_root(gmpt_trie *t, bool two_phase, const uint8
     record(GMPT_E_ARG, "null trie");
     return nullptr;
   }
-  int rc = two_phase ? gmpt_puts_2phase(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs,
-                                        values_hps, n)
-                     : gmpt_puts_latching(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs,
-                                          values_hps, n);
+  // GMPT_SCHEDULE=auto: the library's schedule selector picks PhaseNU,
+  // LockNU or the persistent launch (and their knobs) per batch
+  const char *sched = std::getenv("GMPT_SCHEDULE");
+  int rc;
+  if (sched && std::strcmp(sched, "auto") == 0)
+    rc = gmpt_puts_auto(t, nullptr, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs, values_hps,
+                        nullptr, n, nullptr);
+  else
+    rc = two_phase ? gmpt_puts_2phase(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs, values_hps,
+                                      n)
+                   : gmpt_puts_latching(t, keys_hexs, keys_hexs_indexs, values_bytes, values_bytes_indexs,
+                                        values_hps, n);
   if (rc) return nullptr;
   if (gmpt_hash_onepass(t)) return nullptr;
   uint8_t root[32];

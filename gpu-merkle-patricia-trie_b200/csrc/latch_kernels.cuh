@@ -327,8 +327,12 @@ __device__ __forceinline__ void latch_keys(const TrieView &tv, DirtyList dl, con
       latch_from(tv, dl, sp[w], x[w], ko[w], len[w], vid_base + (unsigned long long)key[w], retry_limit);
 }
 
+#ifndef GMPT_LATCH_CTAS
+#define GMPT_LATCH_CTAS 2
+#endif
+
 template <int kWays>
-__global__ void __launch_bounds__(256, 2) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
+__global__ void __launch_bounds__(256, GMPT_LATCH_CTAS) k_latch_insert(TrieView tv, DirtyList dl, const uint64_t *koff,
                                                       const uint32_t *klen, int n, uint64_t vid_base,
                                                       uint32_t retry_limit, const int *tid, KeySelect ks) {
   latch_keys<kWays>(tv, dl, koff, klen, n, vid_base, retry_limit, tid, blockIdx.x * blockDim.x + threadIdx.x,

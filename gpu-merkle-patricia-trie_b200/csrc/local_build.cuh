@@ -17,6 +17,10 @@ constexpr int kLocalCap = 2048;     // items per segment
 constexpr int kLocalThreads = 256;  // items [tid*8, tid*8+8) per thread
 constexpr int kLocalIpt = kLocalCap / kLocalThreads;
 constexpr int kLocalSegs = kLocalCap / 2;  // a segment has >= 2 items
+// resident CTAs per SM the register allocation is bounded for
+#ifndef GMPT_LOCAL_BUILD_CTAS
+#define GMPT_LOCAL_BUILD_CTAS 2
+#endif
 
 struct LocalSegs {
   uint64_t slot[kLocalSegs];  // where the segment's top node is linked
@@ -35,7 +39,7 @@ struct LocalSmem {
   uint32_t nseg;
 };
 
-__global__ void __launch_bounds__(kLocalThreads) k_local_build(TrieView tv, DirtyList dl, SortedItems si,
+__global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_build(TrieView tv, DirtyList dl, SortedItems si,
                                                                SegArrays gs, uint32_t gen) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   LocalSmem &L = *reinterpret_cast<LocalSmem *>(smem_raw);

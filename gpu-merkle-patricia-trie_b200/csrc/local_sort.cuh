@@ -21,7 +21,7 @@ constexpr int kSortLocalPerWarp = kSortLocalCap / kSortLocalWarps;  // 256 items
 struct LocalSortSmem {
   uint64_t key[2][kSortLocalCap];
   uint32_t val[2][kSortLocalCap];
-  uint32_t cnt[kSortLocalWarps][256];
+  uint16_t cnt[kSortLocalWarps][256];  // per-warp digit counts, then offsets (<= kSortLocalCap)
   uint32_t warp_tmp[kSortLocalWarps + 1];
   unsigned long long mask;
   uint32_t maxlen;
@@ -58,6 +58,7 @@ __device__ __forceinline__ uint32_t cta_excl_scan(uint32_t v, uint32_t *tmp, uin
 __device__ __forceinline__ void cta_radix_pass(LocalSortSmem &L, int src, int m, int shift) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortLocalWarps * 256; i += kSortLocalThreads) (&L.cnt[0][0])[i] = 0;
+  static_assert(kSortLocalCap < 65536, "digit offsets are 16-bit");
   __syncthreads();
   const unsigned lt = (1u << lane) - 1u;
   uint32_t rk[kSortLocalPerWarp / 32];
@@ -69,7 +70,7 @@ __device__ __forceinline__ void cta_radix_pass(LocalSortSmem &L, int src, int m,
     unsigned peers = __match_any_sync(0xffffffffu, d);
     uint32_t old = ok ? L.cnt[wid][d] : 0;
     __syncwarp();
-    if (ok && (int)lane == __ffs(peers) - 1) L.cnt[wid][d] = old + __popc(peers);
+    if (ok && (int)lane == __ffs(peers) - 1) L.cnt[wid][d] = (uint16_t)(old + __popc(peers));
     __syncwarp();
     rk[r] = old + __popc(peers & lt);
   }
@@ -83,7 +84,7 @@ __device__ __forceinline__ void cta_radix_pass(LocalSortSmem &L, int src, int m,
     uint32_t run = dbase;
     for (int w = 0; w < kSortLocalWarps; ++w) {
       uint32_t c = L.cnt[w][threadIdx.x];
-      L.cnt[w][threadIdx.x] = run;
+      L.cnt[w][threadIdx.x] = (uint16_t)run;
       run += c;
     }
   }

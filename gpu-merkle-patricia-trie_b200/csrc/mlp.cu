@@ -1,7 +1,7 @@
 // mlp.cu -- fp32 MLP kernels of the schedule selector (inference, masked-MSE
 // gradient, Adam training) and their host wrapper.
 //
-// The network is tiny (<= 16 inputs, <= 64 hidden, <= 8 outputs, < 6k
+// The network is tiny (<= 16 inputs, <= 64 hidden, <= 16 outputs, < 6.3k
 // parameters), so one CTA holds the parameters, the Adam moments, the
 // gradient and a 64-sample mini-batch's activations in shared memory and runs
 // whole training epochs in a single launch.  Each gradient element is owned by

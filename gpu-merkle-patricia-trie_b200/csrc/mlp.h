@@ -14,7 +14,7 @@
 
 namespace gmpt {
 
-constexpr int kMlpMaxIn = 16, kMlpMaxHidden = 64, kMlpMaxOut = 8;
+constexpr int kMlpMaxIn = 16, kMlpMaxHidden = 64, kMlpMaxOut = 16;
 
 class Mlp {
  public:

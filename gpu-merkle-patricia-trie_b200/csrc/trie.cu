@@ -29,8 +29,6 @@ constexpr int kThreads = 256;
 constexpr int kHashThreads = kHashLevelThreads;
 constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);          // (depth, kind)
 constexpr int kHashBins = kMaxDepthBins * (int)kHashClasses;       // (depth, kind, hash class)
-// levels with at most this many branch nodes hash them one warp each
-constexpr int kWarpFullMax = 4096;
 // LockNU batches of at least this many keys drop repeated keys first
 constexpr int kDedupMinKeys = 1 << 16;
 
@@ -194,8 +192,12 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   };
   uint64_t need_full = (uint64_t)n_full_ + add_full;
   if (need_full > kMaxNodes) return fail(E_CAPACITY, "branch node count exceeds 2^30");
+  // a branch-pool cap: the pool stops growing there and a kernel that runs
+  // out of branch nodes reports ERR_CAPACITY (the batch is then cut short)
+  if (opt_max_full_ && need_full > opt_max_full_) need_full = std::max<uint64_t>(opt_max_full_, n_full_);
   if (need_full > cap_full_) {
     uint64_t nc = std::min<uint64_t>(grow_to(need_full, cap_full_), kMaxNodes);
+    if (opt_max_full_) nc = std::min<uint64_t>(nc, std::max<uint64_t>(opt_max_full_, need_full));
     size_t o = n_full_;
     if (e == cudaSuccess) e = grow_array(tv_.full_child, o * 17, nc * 17, st_);
     if (e == cudaSuccess) e = grow_array(tv_.full_epoch, o, nc, st_);
@@ -421,7 +423,8 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
           (e = cudaStreamSynchronize(st_)) != cudaSuccess)
         return check_cuda(e, "sort runs");
       uint32_t maxrun = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
-      if (maxrun <= (uint32_t)kSortLocalCap) {
+      const uint32_t cap = opt_local_sort_cap_ > 0 ? (uint32_t)opt_local_sort_cap_ : (uint32_t)kSortLocalCap;
+      if (maxrun <= cap) {
         const size_t smem = sizeof(LocalSortSmem);
         if ((e = cudaFuncSetAttribute(k_local_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
@@ -623,7 +626,8 @@ int Trie::build_levels(int T) {
   while (K > 0) {
     ++levels;
     if (levels > kMaxKeyNibbles + 2) return fail(E_INTERNAL, "builder did not converge");
-    if (opt_local_build_ && maxseg <= (uint32_t)kLocalCap) {
+    const uint32_t lcap = opt_local_build_cap_ > 0 ? (uint32_t)opt_local_build_cap_ : (uint32_t)kLocalCap;
+    if (opt_local_build_ && maxseg <= lcap) {
       // every remaining segment fits one CTA: finish all subtries there
       const size_t smem = sizeof(LocalSmem);
       if ((e = cudaFuncSetAttribute(k_local_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
@@ -856,7 +860,7 @@ int Trie::bucket_and_hash() {
     uint32_t a = off[2 * d * C], m = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];
     if (z == a) continue;
     ++levels;
-    if (z - m > 0 && z - m <= (uint32_t)kWarpFullMax) {
+    if (z - m > 0 && z - m <= (uint32_t)opt_warp_full_max_) {
       // few branches: short nodes thread-wise, branches one warp each
       if (m > a)
         count_launch(), k_hash_level<<<blocks_for(m - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a,
@@ -1130,8 +1134,9 @@ int Trie::put_latching(const BatchIn &b) {
   const int ways = opt_latch_ways_;
   auto kern = ways == 1 ? k_latch_insert<1> : (ways == 2 ? k_latch_insert<2> : k_latch_insert<4>);
   count_launch(), kern<<<blocks_for((b.n + ways - 1) / ways), kThreads, 0, st_>>>(tv_, dl, koff, klen, b.n, vid_base,
-                                                                                 1u << 20, tid, ks);
+                                                                                 opt_retry_limit_, tid, ks);
   if ((rc = check_cuda(cudaGetLastError(), "latch launch"))) return rc;
+  empty_ = false;  // keys may be in even when the batch stops on an error
   if ((rc = sync_counters())) return rc;
   if (timing_) {
     cudaEventRecord(ev[2], st_);
@@ -1403,6 +1408,36 @@ int Trie::set_option(const std::string &name, int64_t value) {
     opt_block_graph_ = value != 0;
     return OK;
   }
+  if (name == "warp_full_max") {
+    if (value < 0 || value > 1 << 30) return fail(E_ARG, "warp_full_max must be in [0, 2^30]");
+    opt_warp_full_max_ = (int)value;
+    return OK;
+  }
+  if (name == "local_build_cap") {
+    if (value < 0 || value > kLocalCap) return fail(E_ARG, "local_build_cap must be in [0, 2048]");
+    opt_local_build_cap_ = (int)value;
+    return OK;
+  }
+  if (name == "local_sort_cap") {
+    if (value < 0 || value > kSortLocalCap) return fail(E_ARG, "local_sort_cap must be in [0, 2048]");
+    opt_local_sort_cap_ = (int)value;
+    return OK;
+  }
+  if (name == "block_barrier_ns") {
+    if (value < 1 || value > 60000000000ll) return fail(E_ARG, "block_barrier_ns must be in [1, 6e10]");
+    opt_barrier_ns_ = (uint64_t)value;
+    return OK;
+  }
+  if (name == "max_branch_nodes") {
+    if (value < 0 || value > (int64_t)kMaxNodes) return fail(E_ARG, "max_branch_nodes must be in [0, 2^30)");
+    opt_max_full_ = (uint32_t)value;
+    return OK;
+  }
+  if (name == "retry_limit") {
+    if (value < 1 || value > (1ll << 30)) return fail(E_ARG, "retry_limit must be in [1, 2^30]");
+    opt_retry_limit_ = (uint32_t)value;
+    return OK;
+  }
   return fail(E_ARG, "unknown option: " + name);
 }
 
@@ -1531,8 +1566,8 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   const int n = b.n;
   if (n < 0 || n > (1 << 26) || b.n0 < 0 || b.n0 > n || b.n_out < 0 || b.n_out > (1 << 26))
     return fail(E_ARG, "block sizes out of range");
-  if (n > 0 && (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs || !b.trie_ids))
-    return fail(E_ARG, "null block array");
+  if (n > 0 && (!b.keys_hexs || !b.keys_indexs || !b.values || !b.values_indexs))
+    return fail(E_ARG, "null block array");  // trie_ids may be null: every key in trie 0
   if ((b.patch_trie == nullptr) != (b.patch_off == nullptr)) return fail(E_ARG, "patch_trie and patch_off go together");
   if (b.n_out > 0 && (!b.out_ids || !out32 || !sizes)) return fail(E_ARG, "null output array");
   for (int i = 0; i < b.n_out; ++i)
@@ -1567,7 +1602,9 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.kidx.p, b.keys_indexs, 8 * (size_t)n, kind, st_);
     if (e == cudaSuccess && vb) e = cudaMemcpyAsync(blk_.vals.p, b.values, (size_t)vb, kind, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.vidx.p, b.values_indexs, 16 * (size_t)n, kind, st_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.tid.p, b.trie_ids, 4 * (size_t)n, kind, st_);
+    if (e == cudaSuccess)
+      e = b.trie_ids ? cudaMemcpyAsync(blk_.tid.p, b.trie_ids, 4 * (size_t)n, kind, st_)
+                     : cudaMemsetAsync(blk_.tid.p, 0, 4 * (size_t)n, st_);
     if (b.patch_trie) {
       if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.ptrie.p, b.patch_trie, 4 * (size_t)n, kind, st_);
       if (e == cudaSuccess) e = cudaMemcpyAsync(blk_.poff.p, b.patch_off, 4 * (size_t)n, kind, st_);
@@ -1590,6 +1627,7 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   h->val_base = val_base;
   h->vid_base = n_rec_;
   h->gen = gen_;
+  h->barrier_ns = opt_barrier_ns_;
   if (timing_) cudaEventRecord(ev[1], st_);
   if ((rc = block_launch())) return rc;
   if (timing_) cudaEventRecord(ev[2], st_);

@@ -125,8 +125,11 @@ class Trie {
   cudaStream_t stream() const { return st_; }
   int device() const { return dev_; }
   int max_tries() const { return (int)n_tries_; }
+  // value nodes in the pools (the keys stored, deleted ones included)
+  uint64_t value_nodes() const { return n_value_; }
   void set_timing(bool on) { timing_ = on; }
-  // tuning knobs (names: "local_build", "local_sort", "latch_ways", "block_grid", "block_graph")
+  // tuning knobs (names: "local_build", "local_sort", "latch_ways", "latch_dedup", "block_grid",
+  // "block_graph", "warp_full_max", "local_build_cap", "local_sort_cap", "retry_limit", ...)
   int set_option(const std::string &name, int64_t value);
   // persistent graph-replayed forest update; out32[32 i..] / sizes[i] = root
   // of trie out_ids[i] after the update
@@ -167,6 +170,12 @@ class Trie {
   int opt_latch_ways_ = 4;       // LockNU keys per thread (1, 2, 4)
   int opt_latch_dedup_ = 1;      // 0 off, 1 batches >= kDedupMinKeys, 2 always
   int opt_dedup_bits_ = 64;      // hash bits the dedup keeps (fewer only to test collisions)
+  int opt_warp_full_max_ = 4096; // hash levels with at most this many branches: a warp per branch
+  int opt_local_build_cap_ = 0;  // largest segment finished in one CTA (0 = the kernel's capacity)
+  int opt_local_sort_cap_ = 0;   // largest tied run finished in one CTA (0 = the kernel's capacity)
+  uint32_t opt_retry_limit_ = 1u << 20;  // failed CASes per LockNU key before GMPT_E_RETRY_LIMIT
+  uint64_t opt_barrier_ns_ = 2000000000ull;  // persistent kernel: longest grid-barrier wait
+  uint32_t opt_max_full_ = 0;    // branch pool cap (0 = none)
 
   // node pools (capacities in elements)
   TrieView tv_{};

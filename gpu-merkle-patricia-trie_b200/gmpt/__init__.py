@@ -43,6 +43,10 @@ EXPORTS = [
     "gmpt_mlp_create", "gmpt_mlp_destroy", "gmpt_mlp_num_params", "gmpt_mlp_get_params", "gmpt_mlp_set_params",
     "gmpt_mlp_forward", "gmpt_mlp_loss_grad", "gmpt_mlp_train",
     "gmpt_puts_forest_device", "gmpt_gets_forest_device", "gmpt_gen_ids", "gmpt_gen_keys", "gmpt_gen_values",
+    "gmpt_schedule_count", "gmpt_schedule_name", "gmpt_schedule_info", "gmpt_puts_schedule",
+    "gmpt_puts_schedule_device", "gmpt_batch_features", "gmpt_batch_features_trie_device", "gmpt_selector_create",
+    "gmpt_selector_destroy", "gmpt_selector_choose", "gmpt_selector_counts", "gmpt_puts_auto",
+    "gmpt_puts_auto_device",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -174,6 +178,20 @@ def lib():
     L.get_all_nodes.restype = NodeSet
     L.init_mpt.restype = vp
     L.free_mpt.argtypes = [vp]
+    L.gmpt_schedule_name.restype = C.c_char_p
+    L.gmpt_schedule_name.argtypes = [i32]
+    L.gmpt_schedule_info.argtypes = [i32, vp]
+    L.gmpt_puts_schedule.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, i32]
+    L.gmpt_puts_schedule_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, i32, i64, i64]
+    L.gmpt_batch_features.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+    L.gmpt_batch_features_trie_device.argtypes = [vp, vp, vp, i32, i64, i64, i32, i64, vp]
+    L.gmpt_selector_create.restype = vp
+    L.gmpt_selector_create.argtypes = [i32, C.c_char_p]
+    L.gmpt_selector_destroy.argtypes = [vp]
+    L.gmpt_selector_choose.argtypes = [vp, vp, vp, vp]
+    L.gmpt_selector_counts.argtypes = [vp, vp]
+    L.gmpt_puts_auto.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp]
+    L.gmpt_puts_auto_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, i64, i64, i32, i64, vp]
     _lib = L
     return L
 
@@ -322,6 +340,54 @@ class Net:
         return float(loss[0])
 
 
+def schedules() -> list:
+    """The library's insert schedules: [{name, two_phase, persistent,
+    local_build, local_sort, latch_ways, latch_dedup, block_grid,
+    warp_full_max}] in index order."""
+    L = lib()
+    out = []
+    keys = ("two_phase", "persistent", "local_build", "local_sort", "latch_ways", "latch_dedup", "block_grid",
+            "warp_full_max")
+    for k in range(L.gmpt_schedule_count()):
+        info = np.zeros(8, np.int32)
+        _check(L.gmpt_schedule_info(k, _p(info)))
+        d = {"name": L.gmpt_schedule_name(k).decode()}
+        d.update({kk: (bool(v) if kk in ("two_phase", "persistent") else int(v)) for kk, v in zip(keys, info)})
+        out.append(d)
+    return out
+
+
+class CSelector:
+    """The library's schedule selector (rule table + optional network),
+    loaded from a file written by gmpt.tuner.Selector.save (None: the
+    built-in rule)."""
+
+    def __init__(self, device: int = 0, path: str | None = None):
+        self._L = lib()
+        self._h = self._L.gmpt_selector_create(device, None if path is None else str(path).encode())
+        if not self._h:
+            raise GmptError(self._L.gmpt_last_error(), self._L.gmpt_last_error_message().decode())
+
+    def choose(self, features) -> tuple:
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        k, net = C.c_int(-1), C.c_int(0)
+        _check(self._L.gmpt_selector_choose(self._h, _p(f), C.byref(k), C.byref(net)))
+        return k.value, bool(net.value)
+
+    def counts(self) -> tuple:
+        out = np.zeros(2, np.uint64)
+        _check(self._L.gmpt_selector_counts(self._h, _p(out)))
+        return int(out[0]), int(out[1])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gmpt_selector_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 class MPT:
     """A device-resident trie (GpuMPT::Compress::MPT).
 
@@ -364,6 +430,55 @@ class MPT:
         tid = np.ascontiguousarray(trie_ids, dtype=np.int32)
         f = self._L.gmpt_puts_2phase_forest if two_phase else self._L.gmpt_puts_latching_forest
         _check(f(self._h, _p(kh), _p(ki), _p(vb), _p(vi), _p(hp), _p(tid), len(ki) // 2))
+
+    # -- schedules ---------------------------------------------------------
+    def puts_schedule(self, k: int, keys_hexs, keys_indexs, values, values_indexs, trie_ids=None):
+        """Insert under library schedule k (see schedules())."""
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        _check(self._L.gmpt_puts_schedule(self._h, int(k), _p(kh), _p(ki), _p(vb), _p(vi), None, _p(tid),
+                                          len(ki) // 2))
+
+    def puts_schedule_device(self, k: int, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int,
+                             values_bytes: int, d_tids: int = 0):
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_puts_schedule_device(self._h, int(k), v(d_keys), v(d_kidx), v(d_vals), v(d_vidx),
+                                                 v(d_tids), int(n), int(keys_bytes), int(values_bytes)))
+
+    def puts_auto(self, keys_hexs, keys_indexs, values, values_indexs, trie_ids=None, selector=None) -> int:
+        """Insert under the schedule the selector (None: the library's own)
+        picks; returns the schedule index run."""
+        kh, ki, vb, vi = _arrays(keys_hexs, keys_indexs, values, values_indexs)
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        k = C.c_int(-1)
+        _check(self._L.gmpt_puts_auto(self._h, selector._h if selector else None, _p(kh), _p(ki), _p(vb), _p(vi),
+                                      None, _p(tid), len(ki) // 2, C.byref(k)))
+        return k.value
+
+    def puts_auto_device(self, d_keys, d_kidx, d_vals, d_vidx, n: int, keys_bytes: int, values_bytes: int,
+                         d_tids: int = 0, tries_touched: int = 0, trie_keys: int = -1, selector=None) -> int:
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        k = C.c_int(-1)
+        _check(self._L.gmpt_puts_auto_device(self._h, selector._h if selector else None, v(d_keys), v(d_kidx),
+                                             v(d_vals), v(d_vidx), v(d_tids), int(n), int(keys_bytes),
+                                             int(values_bytes), int(tries_touched), int(trie_keys), C.byref(k)))
+        return k.value
+
+    def features(self, keys_hexs, keys_indexs, values_indexs, trie_ids=None) -> np.ndarray:
+        """The selector's 8 features of a host batch put into this trie."""
+        kh, ki, _, vi = _arrays(keys_hexs, keys_indexs, None, values_indexs)
+        tid = None if trie_ids is None else np.ascontiguousarray(trie_ids, dtype=np.int32)
+        out = np.zeros(8, np.float32)
+        _check(self._L.gmpt_batch_features(self._h, _p(kh), _p(ki), _p(vi), _p(tid), len(ki) // 2, _p(out)))
+        return out
+
+    def features_device(self, d_keys, d_kidx, n: int, keys_bytes: int, values_bytes: int,
+                        tries_touched: int = 0, trie_keys: int = -1) -> np.ndarray:
+        out = np.zeros(8, np.float32)
+        _check(self._L.gmpt_batch_features_trie_device(self._h, C.c_void_p(d_keys), C.c_void_p(d_kidx), int(n),
+                                                       int(keys_bytes), int(values_bytes), int(tries_touched),
+                                                       int(trie_keys), _p(out)))
+        return out
 
     def deletes(self, keys_hexs, keys_indexs, trie_ids=None):
         """Remove keys (absent keys are ignored); hash_onepass_v2 afterwards."""

@@ -25,6 +25,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+# The library's schedule table (csrc/schedule.cu kSchedules, gmpt.schedules()),
+# index for index; tests/test_tuner_host.py checks that the two agree.
 CONFIGS = [
     {"name": "phasenu", "two_phase": True, "local_build": 1, "local_sort": 1},
     {"name": "phasenu-global-build", "two_phase": True, "local_build": 0, "local_sort": 1},
@@ -36,6 +38,12 @@ CONFIGS = [
     # co-resident CTAs per SM (block_grid 0 = the device's maximum)
     {"name": "persistent-2cta", "two_phase": False, "persistent": True, "block_grid": 0},
     {"name": "persistent-1cta", "two_phase": False, "persistent": True, "block_grid": 148},
+    # LockNU without the repeated-key drop (latch_dedup 0)
+    {"name": "locknu-4-nodedup", "two_phase": False, "latch_ways": 4, "latch_dedup": 0},
+    # PhaseNU with every sort pass device-wide
+    {"name": "phasenu-global-sort", "two_phase": True, "local_build": 1, "local_sort": 0},
+    # PhaseNU, and PhaseHC hashes levels of up to 64K branches one warp each
+    {"name": "phasenu-warp-hash", "two_phase": True, "local_build": 1, "local_sort": 1, "warp_full_max": 65536},
 ]
 FIXED_PHASENU = 0
 FIXED_LOCKNU = 2  # the reference's fixed choice
@@ -45,14 +53,26 @@ FEATURES = ["log2_n", "key_nibbles", "key_nibbles_std", "dup_frac", "log2_trie_k
 
 
 def apply_config(mpt, k: int) -> bool:
-    """Set every knob of configuration k on the trie; returns two_phase."""
+    """Set every knob of configuration k on the trie (as the library's
+    apply_schedule does); returns two_phase."""
     c = CONFIGS[k]
     mpt.set_option("local_build", c.get("local_build", 1))
     mpt.set_option("local_sort", c.get("local_sort", 1))
     mpt.set_option("latch_ways", c.get("latch_ways", 4))
+    mpt.set_option("latch_dedup", c.get("latch_dedup", 1))
+    mpt.set_option("warp_full_max", c.get("warp_full_max", 4096))
     if c.get("persistent"):
         mpt.set_option("block_grid", c.get("block_grid", 0))
     return bool(c["two_phase"])
+
+
+def config_knobs(k: int) -> dict:
+    """Configuration k with every knob explicit (the library's defaults filled in)."""
+    c = CONFIGS[k]
+    return {"name": c["name"], "two_phase": bool(c["two_phase"]), "persistent": bool(c.get("persistent", False)),
+            "local_build": c.get("local_build", 1), "local_sort": c.get("local_sort", 1),
+            "latch_ways": c.get("latch_ways", 4), "latch_dedup": c.get("latch_dedup", 1),
+            "block_grid": c.get("block_grid", 0), "warp_full_max": c.get("warp_full_max", 4096)}
 
 
 def sample_stats(keys_hexs: np.ndarray, keys_indexs: np.ndarray, samples: int = 64) -> np.ndarray:
@@ -244,3 +264,39 @@ class Selector:
             self.fallbacks += 1
             return self.rule.choose(f)
         return self._net_choice(f)
+
+    def save(self, path) -> None:
+        """Write the selector for the library's C++ selector
+        (gmpt_selector_create): rule table, network, normalisation.  The
+        format is documented at Selector::load in csrc/schedule.cu."""
+        lines = ["gmpt-selector 1", f"schedules {len(CONFIGS)}", f"default {int(self.rule.default)}",
+                 f"rules {len(self.rule.table)}"]
+        for b, k in self.rule.table.items():
+            lines.append(f"{b[0]} {b[1]} {b[2]} {int(k)}")
+        if self.mean is None:
+            lines.append("net 0 0 0 0")
+        else:
+            p = self.net.params()
+            n_in, n_hidden, n_out = self.net.dims
+            lines.append(f"net {1 if self.use_net else 0} {n_in} {n_hidden} {n_out}")
+            lines.append(f"margin {self.ood_margin!r}")
+            for name, v in (("mean", self.mean), ("std", self.std), ("lo", self.lo), ("hi", self.hi)):
+                lines.append(name + " " + " ".join(repr(float(np.float32(x))) for x in v))
+            lines.append(f"cols {len(self.cols)} " + " ".join(str(int(c)) for c in self.cols))
+            lines.append(f"params {len(p)} " + " ".join(repr(float(x)) for x in p))
+        with open(path, "w") as f:
+            f.write("\n".join(lines) + "\n")
+
+    def to_library(self, device: int = 0, path=None):
+        """The same selector inside the library (gmpt.CSelector): choices are
+        then made by the C++ rule and the network's CUDA inference kernel."""
+        import os
+        import tempfile
+
+        from . import CSelector
+
+        if path is None:
+            fd, path = tempfile.mkstemp(suffix=".gmpt-selector")
+            os.close(fd)
+        self.save(path)
+        return CSelector(device, path)

@@ -324,13 +324,99 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
  *   "local_build" 1/0: finish build segments of <= 2048 keys inside one CTA
  *                      each (default 1) or keep every level device-wide;
  *   "local_sort"  1/0: same for the still-tied runs of the batch sort;
+ *   "local_build_cap", "local_sort_cap" N (<= 2048; 0 = 2048): the largest
+ *                      segment / run finished inside one CTA;
  *   "latch_ways"  1/2/4: keys each LockNU thread walks together (default 4:
  *                      more loads in flight; 1: more threads for small batches);
+ *   "latch_dedup" 0/1/2: LockNU drops repeated keys of a batch before the
+ *                      walk: never / batches of >= 64K keys (default) / always;
+ *   "warp_full_max" N: PhaseHC hashes a level's branches one warp each when
+ *                      the level has at most N branches (default 4096);
  *   "block_grid"  N:   CTAs of the persistent block kernel (0 = one per SM,
  *                      capped at what can be co-resident);
  *   "block_graph" 1/0: replay block launches from a captured CUDA graph
- *                      (default 1) or issue them one by one. */
+ *                      (default 1) or issue them one by one.
+ * Failure bounds (the reference instead spins without bound, util/lock.cuh:
+ * 17-21, and asserts on arena overflow, util/allocator.cuh:115-118):
+ *   "retry_limit" N:   failed CASes one LockNU key may take before the batch
+ *                      reports GMPT_E_RETRY_LIMIT (default 2^20).  Keys that
+ *                      hit it are left out and every other key is in; putting
+ *                      the batch again completes it;
+ *   "block_barrier_ns" N: longest grid-barrier wait of the persistent block
+ *                      kernel (default 2e9); a wait that runs out ends the
+ *                      launch with GMPT_E_INTERNAL ("grid barrier wait gave
+ *                      up") with the block partly applied: gmpt_reset and
+ *                      reload the trie;
+ *   "max_branch_nodes" N: the branch pool stops growing at N nodes (0 = no
+ *                      cap); a batch that needs more fails with
+ *                      GMPT_E_CAPACITY from the kernel that ran out, partly
+ *                      applied: gmpt_reset and reload the trie. */
 int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value);
+
+/* ---- schedules and the schedule selector ----
+ * A put batch can run under several schedules -- PhaseNU or LockNU with
+ * their knobs, or the persistent launch (LockNU insert + PhaseHC in one
+ * graph-replayed kernel) -- and every one gives the same trie, so choosing
+ * only changes time.  No counterpart in the reference, which fixes LockNU
+ * (lib/libgmpt.cu:107-111) and fits its cost model offline
+ * (test/experiments.cu:3250-3348).
+ * gmpt_schedule_info(k, out): out = {PhaseNU, persistent, local_build,
+ * local_sort, latch_ways, latch_dedup, block_grid, warp_full_max}. */
+int gmpt_schedule_count(void);
+const char *gmpt_schedule_name(int k);
+int gmpt_schedule_info(int k, int out[8]);
+/* Insert a batch under schedule k (host arrays; trie_ids may be NULL).  A
+ * persistent schedule also hashes the trie; a batch it cannot take (caller
+ * host pointers, index pairs that do not tile the key stream) runs as LockNU. */
+int gmpt_puts_schedule(gmpt_trie *t, int k, const uint8_t *keys_hexs, const int *keys_indexs,
+                       const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                       const int *trie_ids, int n);
+/* The same with device arrays (d_trie_ids may be NULL). */
+int gmpt_puts_schedule_device(gmpt_trie *t, int k, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                              const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids,
+                              int n, int64_t keys_bytes, int64_t values_bytes);
+/* The selector's features of a put batch into t:
+ *   out[0] log2(n + 1)          out[4] log2(value nodes in t + 1)
+ *   out[1] mean key nibbles/64  out[5] log2(mean value bytes + 1)
+ *   out[2] key-length spread/64 out[6] mean longest common prefix of a
+ *   out[3] repeated-key share          sampled key with the others / mean length
+ *                               out[7] log2(tries the batch touches)
+ * out[2], out[3], out[6] come from 64 evenly spaced keys (host arrays: on the
+ * host; device arrays: the kernel of gmpt_batch_features_device). */
+int gmpt_batch_features(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_indexs,
+                        const int64_t *values_indexs, const int *trie_ids, int n, float out[8]);
+/* Device key arrays, stream totals given.  tries_touched > 0 fills out[7]
+ * and trie_keys >= 0 (keys of the tries the batch touches) out[4]; otherwise
+ * they come from the whole trie object. */
+int gmpt_batch_features_trie_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, int n,
+                                    int64_t keys_bytes, int64_t values_bytes, int tries_touched, int64_t trie_keys,
+                                    float out[8]);
+/* A schedule selector: an autotuned rule table (coarse buckets of batch
+ * size, trie size and repeated-key share -> the schedule measured fastest
+ * there) and optionally the MLP of gmpt_mlp_* predicting every schedule's
+ * log time (inference on the device), with the rule as fallback outside the
+ * network's training range.  path = a file written by the Python trainer
+ * (gmpt.tuner.Selector.save); NULL = the built-in rule (empty trie: PhaseNU;
+ * up to 64K keys: persistent launch; else LockNU, 4 keys per thread). */
+typedef struct gmpt_selector gmpt_selector;
+gmpt_selector *gmpt_selector_create(int device, const char *path);
+void gmpt_selector_destroy(gmpt_selector *s);
+int gmpt_selector_choose(gmpt_selector *s, const float features[8], int *schedule, int *used_net);
+/* out[0] = choices so far, out[1] = of which the rule made (fallbacks) */
+int gmpt_selector_counts(gmpt_selector *s, uint64_t out[2]);
+/* Insert a batch under the schedule the selector picks for it (sel NULL: the
+ * library's selector of the trie's device -- the file named by the
+ * GMPT_SELECTOR environment variable, else the built-in rule).  *chosen
+ * (may be NULL) = the schedule run.  Setting GMPT_SCHEDULE=auto makes the
+ * reference ABI's build_mpt_* / insert_mpt_* calls (libgmpt.h) go this way. */
+int gmpt_puts_auto(gmpt_trie *t, gmpt_selector *sel, const uint8_t *keys_hexs, const int *keys_indexs,
+                   const uint8_t *values_bytes, const int64_t *values_indexs, const uint8_t *const *values_hps,
+                   const int *trie_ids, int n, int *chosen);
+/* Device arrays; tries_touched / trie_keys as for gmpt_batch_features_trie_device. */
+int gmpt_puts_auto_device(gmpt_trie *t, gmpt_selector *sel, const uint8_t *d_keys_hexs, const int *d_keys_indexs,
+                          const uint8_t *d_values_bytes, const int64_t *d_values_indexs, const int *d_trie_ids, int n,
+                          int64_t keys_bytes, int64_t values_bytes, int tries_touched, int64_t trie_keys,
+                          int *chosen);
 /* per-phase CUDA-event timing into gmpt_stats (adds synchronisation) */
 int gmpt_set_timing(gmpt_trie *t, int on);
 
@@ -379,7 +465,7 @@ int gmpt_keccak_peak(int device, double *perm_per_s);
 uint64_t gmpt_launch_count(void);
 
 /* ---- schedule selector network --------------------------------------
- * A two-hidden-layer ReLU MLP (n_in <= 16, n_hidden <= 64, n_out <= 8, fp32)
+ * A two-hidden-layer ReLU MLP (n_in <= 16, n_hidden <= 64, n_out <= 16, fp32)
  * with hand-written CUDA inference, gradient and Adam training kernels; the
  * library's schedule selector predicts per-configuration batch times with it.
  * No counterpart in the reference, whose insert strategy is fixed

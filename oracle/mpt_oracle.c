@@ -85,6 +85,10 @@ void omt_sha3_256(const uint8_t *in, size_t len, uint8_t out[32]) {
   sponge256(in, len, 0x06, out);
 }
 
+void omt_keccak256_rows(const uint8_t *in, size_t rows, size_t width, uint8_t *out) {
+  for (size_t r = 0; r < rows; ++r) sponge256(in + r * width, width, 0x01, out + 32 * r);
+}
+
 /* ------------------------------------------------------------------------ */
 /* RLP (util/rlp.cuh:9-155) and compact keys (util/utils.cuh:340-396)        */
 /* ------------------------------------------------------------------------ */

@@ -64,6 +64,9 @@ void omt_keccak_f1600(uint64_t st[25]);
 void omt_keccak256(const uint8_t *in, size_t len, uint8_t out[32]);
 /* FIPS-202 SHA3-256 (pad 0x06): same permutation; used to pin it. */
 void omt_sha3_256(const uint8_t *in, size_t len, uint8_t out[32]);
+/* Keccak-256 of each of `rows` messages of `width` bytes laid out back to
+ * back -> out[32 * rows]. */
+void omt_keccak256_rows(const uint8_t *in, size_t rows, size_t width, uint8_t *out);
 
 /* --- helpers (util/utils.cuh) ------------------------------------------- */
 int omt_key_bytes_to_hex(const uint8_t *key, int len, uint8_t *hex);

@@ -63,6 +63,7 @@ def lib():
         L.omt_keccak256.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
         L.omt_sha3_256.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
         L.omt_keccak_f1600.argtypes = [C.c_void_p]
+        L.omt_keccak256_rows.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]
         _lib = L
     return _lib
 
@@ -101,6 +102,16 @@ def keccak256(data: bytes) -> bytes:
     out = np.zeros(32, np.uint8)
     lib().omt_keccak256(_ptr(buf), len(data), _ptr(out))
     return out.tobytes()
+
+
+def keccak256_rows(msgs: np.ndarray) -> np.ndarray:
+    """Keccak-256 of every row of a 2-D uint8 array -> [rows, 32] (CPU; the
+    same contract as gmpt.keccak256_rows)."""
+    m = np.ascontiguousarray(msgs, dtype=np.uint8)
+    rows, width = m.shape
+    out = np.empty((rows, 32), dtype=np.uint8)
+    lib().omt_keccak256_rows(_ptr(m), rows, width, _ptr(out))
+    return out
 
 
 def sha3_256(data: bytes) -> bytes:

@@ -54,6 +54,45 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def config_roots():
+    """Oracle roots of the benchmark configurations at full size
+    (tests/golden/make_config_roots.py)."""
+    return json.loads((REPO / "tests" / "golden" / "config_roots.json").read_text())["cases"]
+
+
+def last_occurrence(batch, idx):
+    """For sampled key positions idx, the batch position of the last
+    occurrence of the same key (keys of any length): a 64-bit hash of every
+    key groups the candidates, whose bytes are then compared."""
+    ki = batch.keys_indexs.reshape(-1, 2).astype(np.int64)
+    lens = ki[:, 1] - ki[:, 0] + 1
+    n = len(ki)
+    kh = batch.keys_hexs.astype(np.uint64)
+    total = int(lens.sum())
+    starts = np.zeros(n, dtype=np.int64)
+    np.cumsum(lens[:-1], out=starts[1:])
+    if total != len(kh) or np.any(ki[:, 0] != starts):
+        raise ValueError("keys must tile the stream")
+    pos = np.arange(total, dtype=np.uint64) - np.repeat(starts, lens).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        w = (pos + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        w ^= w >> np.uint64(29)
+        h = np.add.reduceat((kh + np.uint64(1)) * w, starts) ^ (lens.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F))
+    order = np.argsort(h, kind="stable")
+    hs = h[order]
+    out = []
+    for i in np.asarray(idx, dtype=np.int64):
+        a = np.searchsorted(hs, h[i], side="left")
+        z = np.searchsorted(hs, h[i], side="right")
+        best = -1
+        for j in order[a:z]:
+            if batch.key(int(j)) == batch.key(int(i)):
+                best = max(best, int(j))
+        out.append(best)
+    return np.array(out, dtype=np.int64)
+
+
+@pytest.fixture(scope="session")
 def gpu_lib():
     """The CUDA library; GPU tests fail loudly if it is missing."""
     import torch

@@ -43,21 +43,27 @@ def test_ycsb_load_then_zipf_updates_matches_oracle_at_256k(gpu_lib):
             assert t.get_root_hash() == r, strategies
 
 
-def test_ycsb_16m_strategies_agree_and_order_does_not_matter(gpu_lib):
-    # size-independent properties at the full 16M configuration: both insert
-    # strategies give the same root, inserting the batch in a permuted order
+def test_ycsb_16m_matches_oracle_roots_and_order_does_not_matter(gpu_lib, config_roots):
+    # The full 16M configuration: the load root and the load + update root
+    # equal the oracle's (tests/golden/config_roots.json, made by
+    # tests/golden/make_config_roots.py) for both insert strategies; then
+    # size-independent properties: inserting the batch in a permuted order
     # gives the same root (canonical trie), and sampled lookups return the
     # last written value.
     n = 1 << 24
+    want = [bytes.fromhex(r) for r in config_roots["c2_ycsb_16m"]["roots"]]
     load = W.ycsb_load(n, seed=0x5EED0002)
     upd = W.ycsb_zipf_updates(n, n, seed=0x5EED0003)
     roots = {}
     for s in ("2phase", "latching"):
         t = gpu_lib.MPT()
+        got = []
         for b in (load, upd):
             f = t.puts_2phase_with_valuehp if s == "2phase" else t.puts_latching_with_valuehp_v2
             f(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
             t.hash_onepass_v2()
+            got.append(t.get_root_hash())
+        assert got == want, s
         roots[s] = t.get_root_hash()
         if s == "2phase":
             idx = W.sample_indices(n, 4096, seed=9)

@@ -123,3 +123,30 @@ def test_oracle_rejects_malformed_keys():
 
 def _flat(b):
     return b.keys_hexs, b.keys_indexs, b.values, b.values_indexs
+
+
+def test_oracle_reaches_the_committed_config_roots_at_1m():
+    # tests/golden/config_roots.json was made by make_config_roots.py with
+    # this oracle (and its 1M cases checked against the reference build):
+    # the YCSB load + zipf update case at 2^20 keys is re-run here
+    import json
+    from pathlib import Path
+
+    from gmpt import workloads as W
+
+    cases = json.loads((Path(__file__).resolve().parent / "golden" / "config_roots.json").read_text())["cases"]
+    n = 1 << 20
+    t = O.OracleTrie()
+    got = []
+    for b in (W.ycsb_load(n, seed=0x5EED0002), W.ycsb_zipf_updates(n, n, seed=0x5EED0003)):
+        t.puts(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+        t.hash()
+        got.append(t.root().hex())
+    assert got == cases["c2_ycsb_1m"]["roots"]
+    assert cases["c2_ycsb_1m"]["reference_build_agrees"]
+
+
+def test_cpu_keccak_rows_matches_single_messages():
+    rows = np.random.default_rng(1).integers(0, 256, (37, 20), dtype=np.uint8)
+    out = O.keccak256_rows(rows)
+    assert [O.keccak256(r.tobytes()) for r in rows] == [o.tobytes() for o in out]

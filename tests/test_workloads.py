@@ -167,3 +167,16 @@ def test_hexs_to_keys_inverts_keys_to_hexs():
         assert np.array_equal(ri[1::2] - ri[0::2] + 1, lens)
     with pytest.raises(ValueError):
         W.hexs_to_keys(np.array([1, 2, 3, 16], np.uint8), np.array([0, 3], np.int32))
+
+
+def test_last_occurrence_helper_matches_a_dictionary():
+    from conftest import last_occurrence
+
+    b = W.vocab_keys(20000, vmin=1, vmax=8, vmu=1.0)
+    last = {}
+    for i in range(b.n):
+        last[b.key(i)] = i
+    idx = W.sample_indices(b.n, 500, seed=5)
+    got = last_occurrence(b, idx)
+    assert [last[b.key(int(i))] for i in idx] == got.tolist()
+    assert any(g != i for g, i in zip(got, idx))  # the sample holds repeated keys
