@@ -57,15 +57,18 @@ def parse():
     p.add_argument("--eth-blocks", type=int, default=512)
     p.add_argument("--eth-compare-blocks", type=int, default=32,
                    help="blocks also run through the per-trie and forest multi-launch paths")
-    p.add_argument("--req-tenants", default="0,262144,1048576,4194304",
+    p.add_argument("--req-tenants", default="0,1048576,4194304,16777216",
                    help="pre-existing keys of each tenant trie of the request loop (empty = skip)")
     p.add_argument("--req-train", type=int, default=1200, help="requests of the selector's training streams")
     p.add_argument("--req-train-episode", type=int, default=300, help="requests per training episode")
     p.add_argument("--req-eval", type=int, default=300, help="requests of each evaluation stream")
     p.add_argument("--req-min", type=int, default=1000)
-    p.add_argument("--req-max", type=int, default=1 << 20)
+    p.add_argument("--req-max", type=int, default=1 << 22)
     p.add_argument("--req-util", type=float, default=0.85, help="load of the plain server (arrival rate)")
     p.add_argument("--req-load", type=float, default=0.25, help="share of puts that fill a new empty tenant trie")
+    p.add_argument("--vocab-n", type=int, default=8 << 20,
+                   help="keys of the variable-length vocabulary-key section (0 = skip)")
+    p.add_argument("--no-gets", action="store_true")
     return p.parse_args()
 
 
@@ -249,6 +252,171 @@ def cpu_baseline(args, batches):
             "sample": f"first {n} keys of the load and of the update batch; {desc}"}
 
 
+def phase_roofline(batches, stats_all, hbm_peak, perm_peak):
+    """Per-phase HBM rooflines of the timed steps and the put + hash
+    composite (algorithmic bytes and ops as defined in DESIGN.md section 5):
+      stage   2 (|k| + |v|) + 56 B per key (read the streams and index
+              pairs, write the arenas, value records and key records)
+      sort    |k| + 4 B per key (read every key once, write its rank)
+      build   |k| per key + the new nodes' pool records (branch 75 B, short
+              node 24 B, value node 8 B)
+      insert  |k| + 8 B per key (read every key once, write its record id)
+      hash    Keccak-f permutations over the measured permutation peak
+    composite = max(B_alg / HBM peak, permutations / permutation peak) over
+    the measured put + hash time, B_alg = sum(|k| + |v| + 16) +
+    sum over hashed nodes (encoding + 32)."""
+    steps = len(stats_all)
+    out = {}
+
+    def add(name, nbytes, ms):
+        gbs = nbytes / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"ms": round(ms, 3), "alg_bytes": int(nbytes), "achieved_gbs": round(gbs, 1),
+                     "frac": round(gbs / hbm_peak, 4)}
+
+    prev = {"n_full": 0, "n_short": 0, "n_value": 0}
+    tot_alg = tot_ms = tot_perm = 0.0
+    for k, b in enumerate(batches):
+        put = [info[k][0] for info in stats_all]
+        hs = [info[k][1] for info in stats_all]
+        mean = lambda key, src: statistics.mean(x[key] for x in src)  # noqa: E731
+        kbytes, vbytes, n = b.key_bytes(), b.value_bytes(), b.n
+        tag = f"b{k}"
+        add(f"{tag}_stage", 2 * (kbytes + vbytes) + 56 * n, mean("t_stage_ms", put))
+        if mean("t_sort_ms", put) > 0:
+            add(f"{tag}_sort", kbytes + 4 * n, mean("t_sort_ms", put))
+            nf = put[-1]["n_full"] - prev["n_full"]
+            ns = put[-1]["n_short"] - prev["n_short"]
+            nv = put[-1]["n_value"] - prev["n_value"]
+            add(f"{tag}_build", kbytes + 75 * nf + 24 * ns + 8 * nv, mean("t_build_ms", put) + mean("t_walk_ms", put))
+        else:
+            add(f"{tag}_insert", kbytes + 8 * n, mean("t_build_ms", put))
+        prev = {kk: put[-1][kk] for kk in prev}
+        perms = mean("last_keccak_blocks", hs)
+        hk = mean("t_hash_kernels_ms", hs)
+        out[f"{tag}_hash"] = {"ms": round(mean("t_hash_ms", hs), 3), "kernels_ms": round(hk, 3),
+                              "permutations": int(perms),
+                              "int_frac": round(perms / (hk / 1e3) / perm_peak, 4) if hk > 0 else None}
+        tot_alg += kbytes + vbytes + 16 * n + mean("last_enc_bytes", hs) + 32 * mean("last_hashed", hs)
+        tot_perm += perms
+        tot_ms += sum(mean(key, put) for key in ("t_stage_ms", "t_sort_ms", "t_walk_ms", "t_build_ms"))
+        tot_ms += mean("t_hash_ms", hs)
+    bound_ms = max(tot_alg / (hbm_peak * 1e9), tot_perm / perm_peak) * 1e3
+    out["composite"] = {"alg_bytes": int(tot_alg), "permutations": int(tot_perm),
+                        "hbm_bound_ms": round(tot_alg / (hbm_peak * 1e9) * 1e3, 3),
+                        "int_bound_ms": round(tot_perm / perm_peak * 1e3, 3), "measured_ms": round(tot_ms, 3),
+                        "frac": round(bound_ms / tot_ms, 4),
+                        "bound": "int (Keccak-f)" if tot_perm / perm_peak > tot_alg / (hbm_peak * 1e9) else "hbm"}
+    return out
+
+
+def run_gets(t, d, n, dev, stream, hbm_peak):
+    """gets_parallel throughput: n lookups of device-resident keys into the
+    trie with device-resident results (every key is present)."""
+    import torch
+
+    hp = torch.empty(n, dtype=torch.int64, device=dev)
+    ln = torch.empty(n, dtype=torch.int32, device=dev)
+    ms = []
+    for it in range(4):
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        t.gets_device(d["k"].data_ptr(), d["ki"].data_ptr(), n, d["kb"], hp.data_ptr(), ln.data_ptr())
+        z.record(stream)
+        z.synchronize()
+        if it:
+            ms.append(a.elapsed_time(z))
+    found = int((ln > 0).sum().item())
+    m = statistics.median(ms)
+    alg = d["kb"] + 8 * n + 12 * n  # read each key and its index pair, write hp + size
+    gbs = alg / (m / 1e3) / 1e9
+    return {"keys": n, "found": found, "ms": round(m, 3), "mkeys_s": round(n / (m / 1e3) / 1e6, 2),
+            "alg_bytes": int(alg), "achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm_peak, 4),
+            "path": "gmpt_gets_device (keys copied next to a zero tail, k_gets, device results)"}
+
+
+def run_vocab(args, local, dev, hbm_peak, perm_peak):
+    """Variable-length vocabulary keys (8-96 B) with 128 B - 4 KB values into
+    an empty trie, each insert strategy + PhaseHC + root; roots against the
+    oracle's (tests/golden/config_roots.json)."""
+    import torch
+
+    import gmpt
+
+    n = args.vocab_n
+    t0 = time.time()
+    b = W.vocab_keys(n)
+    gen_s = time.time() - t0
+    d = dict(k=torch.from_numpy(b.keys_hexs).to(dev), ki=torch.from_numpy(b.keys_indexs).to(dev),
+             v=torch.from_numpy(b.values).to(dev), vi=torch.from_numpy(b.values_indexs).to(dev))
+    t = gmpt.MPT(device=local)
+    t.reserve(n, b.key_bytes(), b.value_bytes())
+    stream = torch.cuda.ExternalStream(t.stream_ptr(), device=dev)
+    res = {}
+    roots = set()
+    for strat in ("2phase", "latching"):
+        ms, info = [], []
+        for it in range(4):
+            t.reset()
+            t.set_timing(it == 3)
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            z = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            t.puts_device(strat == "2phase", d["k"].data_ptr(), d["ki"].data_ptr(), d["v"].data_ptr(),
+                          d["vi"].data_ptr(), n, b.key_bytes(), b.value_bytes())
+            t.hash_onepass_v2()
+            roots.add(t.get_root_hash())
+            z.record(stream)
+            z.synchronize()
+            if 0 < it < 3:
+                ms.append(a.elapsed_time(z))
+            if it == 3:
+                info = t.stats()
+        m = statistics.mean(ms)
+        res[strat] = {"ms": round(m, 3), "mkeys_s": round(n / (m / 1e3) / 1e6, 2),
+                      "hash_kernels_ms": round(info["t_hash_kernels_ms"], 3),
+                      "keccak_int_frac": round(info["last_keccak_blocks"] / (info["t_hash_kernels_ms"] / 1e3) /
+                                               perm_peak, 4),
+                      "permutations": int(info["last_keccak_blocks"]), "hashed_nodes": int(info["last_hashed"])}
+    t.set_timing(False)
+    t.close()
+    golden = None
+    path = REPO / "tests" / "golden" / "config_roots.json"
+    if path.exists():
+        c = json.loads(path.read_text())["cases"].get({8 << 20: "c3_vocab_8m", 1 << 20: "c3_vocab_1m"}.get(n, ""))
+        golden = c["roots"][0] if c else None
+    assert len(roots) == 1, "the two strategies disagree"
+    root = roots.pop()
+    if golden is not None:
+        assert root.hex() == golden, "vocabulary-key root differs from the oracle's"
+    sizes = b.values_indexs[1::2] - b.values_indexs[0::2] + 1
+    klens = (b.keys_indexs[1::2] - b.keys_indexs[0::2]) // 2
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle as O
+
+        m = min(n, 1 << 18)
+        sub = b.subset(np.arange(m))
+        if O.ref_lib(big=True) is not None:
+            threads = os.cpu_count() or 1
+            rt = O.RefTrie(big=True, threads=threads)
+            tt = time.perf_counter()
+            rt.puts_lock_and_hash(sub.keys_hexs, sub.keys_indexs, sub.values, sub.values_indexs)
+            dt = time.perf_counter() - tt
+            rt.close()
+            cpu = {"value": round(m / dt / 1e6, 4), "unit": "Mkeys/s", "cores": threads, "kind": "reference",
+                   "sample": f"first {m} keys; reference CpuMPT puts_lock + hashs_onepass"}
+    del d
+    torch.cuda.empty_cache()
+    return {"workload": f"{n} vocabulary keys of {int(klens.min())}-{int(klens.max())} B (lognormal mu 3.0 sigma "
+                        f"0.5, seeded 10k-word vocabulary), values {int(sizes.min())}-{int(sizes.max())} B "
+                        "(lognormal), one batch into an empty trie + PhaseHC + root",
+            "strategies": res, "root": root.hex(), "root_matches_oracle": golden is not None,
+            "value_bytes": int(b.value_bytes()), "generate_s": round(gen_s, 1), "cpu_baseline": cpu}
+
+
 GRIDS = (74, 148, 296)  # persistent-kernel grids the block autotuner tries
 TUNE_ROUNDS = 4
 
@@ -416,7 +584,7 @@ def run_eth(args, local, dev):
     }
 
 
-MERGE_KEYS = 1 << 22  # largest merged batch of the queue-draining server
+MERGE_KEYS = 1 << 23  # largest merged batch of the queue-draining server
 
 
 def run_requests(args, local, dev):
@@ -466,12 +634,15 @@ def run_requests(args, local, dev):
     loss = sel.fit(Ftr, Ttr, max_epochs=600, lr=3e-3)
     train_s = time.time() - tt
     rule = sel.rule
+    csel = sel.to_library(local)
     out = {"workload": f"request loop over tenant tries (pre-existing keys {sizes}, plus a new empty tenant per "
                        f"load request = {args.req_load:.2f} of puts; keys 20-96 B, values 16-128 B per tenant); "
                        f"batches log-uniform [{args.req_min}, {args.req_max}] keys, zipf theta U[0,1.2], puts mix "
                        "fresh keys (share U[0,1]) and zipf updates; Poisson arrivals at "
                        f"{args.req_util:.2f} load of the plain server",
            "configs": [c["name"] for c in TU.CONFIGS],
+           "selector": "in the library: gmpt_selector (C++ rule table + the network's CUDA inference kernel), "
+                       "trained by gmpt.tuner with the library's MLP kernels",
            "train": {"requests": episodes * args.req_train_episode, "episodes": episodes, "puts": int(len(Ftr)),
                      "mlp": f"{len(TU.FEATURES)}-32-32-{len(TU.CONFIGS)}", "final_loss": round(loss, 4),
                      "train_kernel_s": round(train_s, 3), "validation": sel.validation,
@@ -497,7 +668,7 @@ def run_requests(args, local, dev):
             rn.reset(tenants)
             if batching:
                 rn.reserve_for(ev, merged_keys=MERGE_KEYS)
-            fb0 = sel.fallbacks
+            fb0 = csel.counts()[1]
             gc.collect()
             gc.disable()  # service times are host wall clock: no collector pauses inside
             r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS, mixed=mixed)
@@ -506,7 +677,7 @@ def run_requests(args, local, dev):
             res[name] = {"mkeys_s": round(r.keys / (r.busy_ms / 1e3) / 1e6, 3),
                          "p50_ms": round(float(np.percentile(r.latency_ms, 50)), 3),
                          "p99_ms": round(float(np.percentile(r.latency_ms, 99)), 3),
-                         "groups": r.groups, "rule_fallbacks": sel.fallbacks - fb0, "slowest_calls": r.slowest,
+                         "groups": r.groups, "rule_fallbacks": csel.counts()[1] - fb0, "slowest_calls": r.slowest,
                          "choices": {TU.CONFIGS[k]["name"]: v for k, v in sorted(r.choices.items())}}
             return r
 
@@ -514,7 +685,8 @@ def run_requests(args, local, dev):
             return TU.FIXED_LOCKNU
 
         def learned_policy(runner, run, n, kb, vb):
-            return sel.choose(runner.features(run, n, kb, vb))
+            # the library's selector: C++ rule table + the network's CUDA inference
+            return csel.choose(runner.features(run, n, kb, vb))[0]
 
         # the plain server (fixed LockNU, one request at a time): its service
         # times do not depend on arrivals, so it sets the arrival rate
@@ -680,6 +852,13 @@ def run_ours(args, world, rank, local):
     phase["hash_kernels_ms"] = [round(statistics.mean(info[k][1]["t_hash_kernels_ms"] for info in stats_all), 3)
                                 for k in range(len(dbat))]
     last = stats_all[-1]
+    phases = phase_roofline(batches, stats_all, hbm_peak, kpeak)
+
+    # lookups: every key of the load batch in the final trie of the last step
+    gets = None
+    if not args.no_gets:
+        gets = run_gets(t, dbat[0], dbat[0]["n"], dev, stream, hbm_peak)
+        assert gets["found"] == dbat[0]["n"], "a loaded key was not found"
 
     # deletes: load the first batch alone, delete every 16th of its keys and
     # rehash (timed), then put them back: the root must return exactly to the
@@ -842,13 +1021,24 @@ def run_ours(args, world, rank, local):
                                        "1M-key YCSB load, scaled by the hashed nodes per level of this run",
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": int(alg_bytes_per_launch),
-                     "avg_launch_us": round(avg_launch_s * 1e6, 2)},
+                     "avg_launch_us": round(avg_launch_s * 1e6, 2),
+                     # the hash kernels are integer-pipe bound: Keccak-f permutations per second
+                     # over the measured rate of the same permutation in a register-only loop
+                     "int_pipe": {"kernel": "k_hash_level + k_hash_full_warp",
+                                  "permutations_per_step": int(sum(perms) / len(stats_all)),
+                                  "achieved_perm_per_s": round(sum(perms) / (sum(hk_ms) / 1e3), 1),
+                                  "peak_perm_per_s": round(kpeak, 1),
+                                  "frac": round(sum(perms) / (sum(hk_ms) / 1e3) / kpeak, 4),
+                                  "peak_kind": "measured live: register-only Keccak-f[1600] loop (gmpt_keccak_peak)"},
+                     "composite": phases.pop("composite"),
+                     "phases": phases},
         "keccak": {"permutations_per_step": int(sum(perms) / len(stats_all)),
                    "perm_per_s": round(sum(perms) / (sum(hk_ms) / 1e3), 1),
                    "peak_perm_per_s": round(kpeak, 1),
                    "frac": round(sum(perms) / (sum(hk_ms) / 1e3) / kpeak, 4),
                    "peak_kind": "measured live: register-only Keccak-f[1600] loop (gmpt_keccak_peak)",
                    "hash_kernels_ms_per_step": round(hash_ms_step, 3)},
+        "gets": gets,
         "clocks": clocks,
         "e2e": e2e,
         "deletes": deletes,
@@ -856,9 +1046,12 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, batches)
-    if world == 1 and (args.eth_accounts > 0 or args.req_tenants):
+    if world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0):
         t.close()
         del dbat
+        torch.cuda.empty_cache()
+    if world == 1 and args.vocab_n > 0:
+        line["vocab"] = run_vocab(args, local, dev, hbm_peak, kpeak)
         torch.cuda.empty_cache()
     if world == 1 and args.eth_accounts > 0:
         line["batched"] = run_eth(args, local, dev)
@@ -867,7 +1060,7 @@ def run_ours(args, world, rank, local):
         line["learned"] = run_requests(args, local, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if not (world == 1 and (args.eth_accounts > 0 or args.req_tenants)):
+    if not (world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0)):
         t.close()
     if world > 1:
         import torch.distributed as dist

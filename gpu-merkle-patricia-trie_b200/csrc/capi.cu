@@ -300,6 +300,15 @@ int gmpt_gets_forest_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int 
                      t->t);
 }
 
+int gmpt_gets_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids, int n,
+                     int64_t keys_bytes, uint64_t *d_values_hps, int *d_values_sizes) {
+  if (!t || (n > 0 && (!d_keys_hexs || !d_keys_indexs || !d_values_hps || !d_values_sizes)) || keys_bytes < 0)
+    return record(GMPT_E_ARG, "null argument");
+  return record_trie(
+      t->t->gets(d_keys_hexs, d_keys_indexs, n, true, d_values_hps, d_values_sizes, keys_bytes, d_trie_ids, true),
+      t->t);
+}
+
 int gmpt_gen_ids(uint64_t seed, int64_t n, int64_t n_existing, int64_t next_new, double p_new, double theta,
                  int64_t *d_ids, int64_t *n_new, void *stream) {
   std::string err;
@@ -638,6 +647,35 @@ int gmpt_puts_auto_device(gmpt_trie *t, gmpt_selector *sel, const uint8_t *d_key
                                  values_bytes);
   b.trie_ids = d_trie_ids;
   return auto_call(t, sel, b, tries_touched, trie_keys, chosen);
+}
+
+int gmpt_flush_dirty(gmpt_trie *t, const uint8_t **hashs, const uint8_t **encs,
+                     const unsigned long long **encs_indexs, unsigned long long *num) {
+  if (!t || !hashs || !encs || !encs_indexs || !num) return record(GMPT_E_ARG, "null argument");
+  *hashs = *encs = nullptr;
+  *encs_indexs = nullptr;
+  *num = 0;
+  std::vector<uint8_t> h, e;
+  std::vector<unsigned long long> ix;
+  int rc = t->t->flush_dirty(h, e, ix);
+  if (rc) return record_trie(rc, t->t);
+  uint8_t *hb = static_cast<uint8_t *>(std::malloc(h.size() + 1));
+  uint8_t *eb = static_cast<uint8_t *>(std::malloc(e.size() + 1));
+  unsigned long long *ib = static_cast<unsigned long long *>(std::malloc(sizeof(unsigned long long) * ix.size() + 8));
+  if (!hb || !eb || !ib) {
+    std::free(hb);
+    std::free(eb);
+    std::free(ib);
+    return record(GMPT_E_CAPACITY, "out of host memory");
+  }
+  if (!h.empty()) std::memcpy(hb, h.data(), h.size());
+  if (!e.empty()) std::memcpy(eb, e.data(), e.size());
+  if (!ix.empty()) std::memcpy(ib, ix.data(), sizeof(unsigned long long) * ix.size());
+  *hashs = hb;
+  *encs = eb;
+  *encs_indexs = ib;
+  *num = h.size() / 32;
+  return record(0, "");
 }
 
 int gmpt_set_option(gmpt_trie *t, const char *name, int64_t value) {

@@ -65,6 +65,7 @@ struct TrieView {
   uint16_t *full_depth;   // nibble depth of the node's path
   uint8_t *full_hash;     // [cap_full * 32]
   uint8_t *full_hlen;
+  uint8_t *full_dead;     // 1: unlinked by a delete (no longer in any trie)
   // short nodes
   uint64_t *short_key;    // nibble offset into the key arena
   uint32_t *short_klen;

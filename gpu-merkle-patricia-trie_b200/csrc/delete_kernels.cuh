@@ -135,6 +135,7 @@ __global__ void k_del_collapse(TrieView tv, DirtyList dl, const uint32_t *refs, 
   if (cnt >= 2) return;
   const uint64_t hs = hslot[id];
   const uint32_t e = hext[id];
+  tv.full_dead[id] = 1;  // unlinked below, or replaced by a short node
   if (cnt == 0) {  // nothing left below: unlink the branch and its extension
     if (e != kNoExt) tv.short_dead[e] = 1;
     write_slot(tv, hs, 0u);

@@ -43,6 +43,31 @@ __global__ void k_flush_collect(TrieView tv, const uint8_t *keys, const int *idx
   }
 }
 
+__global__ void k_widen_u32(const uint32_t *in, int64_t n, uint64_t *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i];
+}
+
+// Sorted refs of the nodes hashed since the last flush -> flags[i] = 1 for
+// the first copy of a node that is still in a trie (not unlinked by a split
+// or a delete) and referenced by hash (encoding of 32 bytes hashed) or a
+// root (nibble depth 0: exactly the roots of the forest's tries).
+__global__ void k_flush_dirty_flags(TrieView tv, const uint64_t *refs, int n, unsigned long long *flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t r = (uint32_t)refs[i];
+  const uint32_t id = ref_idx(r);
+  bool keep = i == 0 || refs[i] != refs[i - 1];
+  if (keep) {
+    if (ref_kind(r) == KIND_FULL)
+      keep = !tv.full_dead[id] && (tv.full_hlen[id] == 32 || tv.full_depth[id] == 0);
+    else
+      keep = ref_kind(r) == KIND_SHORT && !tv.short_dead[id] &&
+             (tv.short_hlen[id] == 32 || tv.short_depth[id] == 0);
+  }
+  flags[i] = keep ? 1ull : 0ull;
+}
+
 __global__ void k_flush_unique_flags(const uint64_t *refs, int n, unsigned long long *flags) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;

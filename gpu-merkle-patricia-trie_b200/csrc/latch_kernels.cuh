@@ -125,6 +125,7 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
     tv.full_depth[br] = (uint16_t)bd;
     tv.full_epoch[br] = gen;
     tv.full_hlen[br] = 0;
+    tv.full_dead[br] = 0;
     // the old node's remainder
     uint32_t rest = schild;
     bool use_left = sl - mm - 1 > 0;

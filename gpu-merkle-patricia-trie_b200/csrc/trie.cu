@@ -85,7 +85,7 @@ Trie::Trie(int device, int geth_mode, int max_tries)
 Trie::~Trie() {
   cudaSetDevice(dev_);
   if (st_) cudaStreamSynchronize(st_);
-  void *ptrs[] = {tv_.full_child, tv_.full_epoch, tv_.full_depth, tv_.full_hash, tv_.full_hlen,
+  void *ptrs[] = {tv_.full_child, tv_.full_epoch, tv_.full_depth, tv_.full_hash, tv_.full_hlen, tv_.full_dead, fl_refs_,
                   tv_.short_key, tv_.short_klen, tv_.short_child, tv_.short_epoch, tv_.short_depth,
                   tv_.short_dead, tv_.short_hash, tv_.short_hlen, tv_.short_claim, tv_.short_pseudo,
                   tv_.value_vid, tv_.rec_off, tv_.rec_len, tv_.rec_hp, (void *)tv_.keys, (void *)tv_.vals,
@@ -204,6 +204,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
     if (e == cudaSuccess) e = grow_array(tv_.full_depth, o, nc, st_);
     if (e == cudaSuccess) e = grow_array(tv_.full_hash, o * 32, nc * 32, st_);
     if (e == cudaSuccess) e = grow_array(tv_.full_hlen, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_dead, o, nc, st_);
     if (e != cudaSuccess) return check_cuda(e, "grow branch pool");
     cap_full_ = (uint32_t)nc;
   }
@@ -275,7 +276,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   tv_.cap_full = cap_full_;
   tv_.cap_short = cap_short_;
   tv_.cap_value = cap_value_;
-  stats_.device_bytes = (uint64_t)cap_full_ * (68 + 4 + 2 + 32 + 1) + (uint64_t)cap_short_ * (8 + 4 + 4 + 4 + 2 + 1 + 32 + 1 + 8) +
+  stats_.device_bytes = (uint64_t)cap_full_ * (68 + 4 + 2 + 32 + 1 + 1) + (uint64_t)cap_short_ * (8 + 4 + 4 + 4 + 2 + 1 + 32 + 1 + 8) +
                         (uint64_t)cap_value_ * 8 + cap_rec_ * 20 + cap_keys_ + cap_vals_ + cap_dirty_ * 6;
   return OK;
 }
@@ -879,6 +880,17 @@ int Trie::bucket_and_hash() {
     cudaEventDestroy(kz);
   }
   tv_.account = 0;
+  if (track_dirty_) {  // keep this pass's nodes for flush_dirty
+    if (fl_n_ + nd > fl_cap_) {
+      uint64_t nc = std::max<uint64_t>(fl_n_ + nd, fl_cap_ + fl_cap_ / 2 + 1024);
+      if ((e = grow_array(fl_refs_, fl_n_, nc, st_)) != cudaSuccess) return check_cuda(e, "grow flush record");
+      fl_cap_ = nc;
+    }
+    if ((e = cudaMemcpyAsync(fl_refs_ + fl_n_, dirty_ref_, 4 * (size_t)nd, cudaMemcpyDeviceToDevice, st_)) !=
+        cudaSuccess)
+      return check_cuda(e, "flush record");
+    fl_n_ += nd;
+  }
   stats_.last_hash_levels = levels;
   stats_.hash_launches = levels;
   if ((e = cudaMemsetAsync(&ctr_->n_dirty, 0, 4, st_)) != cudaSuccess) return check_cuda(e, "hash reset");
@@ -959,7 +971,7 @@ int Trie::roots(const int *ids, int n, uint8_t *out32, int *sizes) {
 }
 
 int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs, uint64_t *out_hp,
-               int *out_len, int64_t keys_bytes, const int *trie_ids) {
+               int *out_len, int64_t keys_bytes, const int *trie_ids, bool device_outputs) {
   err_.clear();
   if (n <= 0) return OK;
   cudaSetDevice(dev_);
@@ -974,12 +986,25 @@ int Trie::gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool dev
   uint64_t *dhp = wsp<uint64_t>(ws_.g_hp, (size_t)n, e);
   int *dlen = wsp<int>(ws_.g_len, (size_t)n, e);
   int *dtid = trie_ids ? wsp<int>(ws_.g_tid, (size_t)n, e) : nullptr;
+  // the keys are copied next to a zeroed 64-byte tail (the 8-byte key loads
+  // may read past a key's last byte); index pairs and trie ids of device
+  // batches are read where they are
   if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys_hexs, (size_t)keys_bytes, kind, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(dk + keys_bytes, 0, 64, st_);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
-  if (e == cudaSuccess && dtid) e = cudaMemcpyAsync(dtid, trie_ids, sizeof(int) * (size_t)n, kind, st_);
+  const int *ki = device_inputs ? keys_indexs : di;
+  const int *ti = device_inputs ? trie_ids : dtid;
+  if (e == cudaSuccess && !device_inputs)
+    e = cudaMemcpyAsync(di, keys_indexs, sizeof(int) * 2 * (size_t)n, kind, st_);
+  if (e == cudaSuccess && dtid && !device_inputs)
+    e = cudaMemcpyAsync(dtid, trie_ids, sizeof(int) * (size_t)n, kind, st_);
   if (e != cudaSuccess) return check_cuda(e, "gets copy");
-  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, di, n, keys_bytes, dhp, dlen, nullptr, dtid);
+  if (device_outputs) {
+    count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, ki, n, keys_bytes, out_hp, out_len, nullptr,
+                                                                ti);
+    e = cudaStreamSynchronize(st_);
+    return check_cuda(e, "gets");
+  }
+  count_launch(), k_gets<<<blocks_for(n), kThreads, 0, st_>>>(tv_, dk, ki, n, keys_bytes, dhp, dlen, nullptr, ti);
   e = cudaMemcpyAsync(out_hp, dhp, sizeof(uint64_t) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(out_len, dlen, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
@@ -1048,6 +1073,7 @@ int Trie::reset() {
   if (e != cudaSuccess) return check_cuda(e, "reset");
   n_full_ = n_short_ = n_value_ = 0;
   n_rec_ = key_used_ = val_used_ = 0;
+  fl_n_ = 0;
   empty_ = true;
   ++gen_;
   tv_.gen = gen_;
@@ -1221,6 +1247,57 @@ int Trie::flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, s
     return check_cuda(e, "flush read");
   }
   return fail(E_INTERNAL, "flush: node count changed between passes");
+}
+
+int Trie::flush_dirty(std::vector<uint8_t> &hashs, std::vector<uint8_t> &encs,
+                       std::vector<unsigned long long> &encs_indexs) {
+  err_.clear();
+  hashs.clear();
+  encs.clear();
+  encs_indexs.clear();
+  if (!track_dirty_) return fail(E_ARG, "flush_dirty needs the track_dirty option (set before the puts)");
+  cudaSetDevice(dev_);
+  const uint64_t cnt = fl_n_;
+  if (cnt == 0) return OK;
+  if (cnt > 0x7FFFFFFFull) return fail(E_CAPACITY, "flush record exceeds 2^31 nodes");
+  cudaError_t e = cudaSuccess;
+  uint64_t *refs = wsp<uint64_t>(ws_.skey, cnt, e);
+  uint32_t *dummy = wsp<uint32_t>(ws_.sval, cnt, e);
+  unsigned long long *flags = wsp<unsigned long long>(ws_.flags, cnt, e);
+  unsigned long long *pos = wsp<unsigned long long>(ws_.pos, cnt, e);
+  uint32_t *uref = wsp<uint32_t>(ws_.act, cnt, e);
+  unsigned long long *sizes = wsp<unsigned long long>(ws_.it_key, cnt, e);
+  unsigned long long *offs = wsp<unsigned long long>(ws_.it_base, cnt, e);
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 64, e) + 4;
+  if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(cnt));
+  if (e != cudaSuccess) return check_cuda(e, "flush dirty alloc");
+  count_launch(), k_widen_u32<<<blocks_for((int64_t)cnt), kThreads, 0, st_>>>(fl_refs_, (int64_t)cnt, refs);
+  if ((e = sorter_.sort(refs, dummy, (int)cnt, st_)) != cudaSuccess) return check_cuda(e, "flush dirty sort");
+  count_launch(), k_flush_dirty_flags<<<blocks_for((int64_t)cnt), kThreads, 0, st_>>>(tv_, refs, (int)cnt, flags);
+  if ((e = exclusive_scan<unsigned long long>(flags, pos, cnt, d_tot, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "flush dirty scan");
+  const int m = (int)read_u64(d_tot);
+  fl_n_ = 0;
+  if (m == 0) return OK;
+  count_launch(), k_flush_sizes<<<blocks_for((int64_t)cnt), kThreads, 0, st_>>>(tv_, refs, flags, pos, (int)cnt, uref,
+                                                                               sizes);
+  if ((e = exclusive_scan<unsigned long long>(sizes, offs, m, d_tot, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "flush dirty scan2");
+  const uint64_t total = read_u64(d_tot);
+  uint8_t *d_encs = wsp<uint8_t>(ws_.sb_base, total + 64, e);
+  unsigned long long *d_idx = wsp<unsigned long long>(ws_.sb_slot, 2 * (size_t)m, e);
+  uint8_t *d_hash = wsp<uint8_t>(ws_.sb_code, 32 * (size_t)m, e);
+  if (e != cudaSuccess) return check_cuda(e, "flush dirty alloc2");
+  count_launch(), k_flush_write<<<blocks_for(m), kThreads, 0, st_>>>(tv_, uref, offs, m, d_encs, d_idx, d_hash);
+  hashs.resize(32 * (size_t)m);
+  encs.resize(total);
+  encs_indexs.resize(2 * (size_t)m);
+  e = cudaMemcpyAsync(hashs.data(), d_hash, hashs.size(), cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess && total) e = cudaMemcpyAsync(encs.data(), d_encs, total, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(encs_indexs.data(), d_idx, 8 * encs_indexs.size(), cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  return check_cuda(e, "flush dirty read");
 }
 
 }  // namespace gmpt
@@ -1421,6 +1498,11 @@ int Trie::set_option(const std::string &name, int64_t value) {
   if (name == "local_sort_cap") {
     if (value < 0 || value > kSortLocalCap) return fail(E_ARG, "local_sort_cap must be in [0, 2048]");
     opt_local_sort_cap_ = (int)value;
+    return OK;
+  }
+  if (name == "track_dirty") {
+    track_dirty_ = value != 0;
+    if (!track_dirty_) fl_n_ = 0;
     return OK;
   }
   if (name == "block_barrier_ns") {

@@ -110,8 +110,10 @@ class Trie {
   // zero-padded, sizes[i] = length (0 = empty trie)
   int roots(const int *ids, int n, uint8_t *out32, int *sizes);
   // out_hp[i] = host pointer given with the value (0 when absent), out_len[i] its size
+  // (device_outputs: out_hp / out_len are device arrays, written by the kernel)
   int gets(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool device_inputs,
-           uint64_t *out_hp, int *out_len, int64_t keys_bytes = -1, const int *trie_ids = nullptr);
+           uint64_t *out_hp, int *out_len, int64_t keys_bytes = -1, const int *trie_ids = nullptr,
+           bool device_outputs = false);
   // value bytes of the stored value for each key (test/export helper)
   int get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &vals,
                  std::vector<int64_t> &offs);
@@ -120,6 +122,12 @@ class Trie {
   const uint32_t *pending_dirty(int *n) const;
   int flush_nodes(const uint8_t *keys_hexs, const int *keys_indexs, int n, std::vector<uint8_t> &hashs,
                   std::vector<uint8_t> &encs, std::vector<unsigned long long> &encs_indexs);
+  // (hash, encoding) of every node hashed since the last flush_dirty that is
+  // still in a trie and referenced by hash (encoding >= 32 bytes, or a root),
+  // in its current state, ordered by node reference; needs the "track_dirty"
+  // option (set before the puts).  Clears the record.
+  int flush_dirty(std::vector<uint8_t> &hashs, std::vector<uint8_t> &encs,
+                  std::vector<unsigned long long> &encs_indexs);
   const TrieStats &stats() const { return stats_; }
   const std::string &error() const { return err_; }
   cudaStream_t stream() const { return st_; }
@@ -191,6 +199,11 @@ class Trie {
   uint32_t epoch_ = 0;         // per put batch (split claims)
   uint32_t gen_ = 1;           // per hash pass (dirty marks)
   bool empty_ = true;
+
+  // nodes hashed since the last flush_dirty (when tracking is on)
+  bool track_dirty_ = false;
+  uint32_t *fl_refs_ = nullptr;
+  uint64_t fl_n_ = 0, fl_cap_ = 0;
 
   // dirty list pending for hash()
   uint32_t *dirty_ref_ = nullptr;

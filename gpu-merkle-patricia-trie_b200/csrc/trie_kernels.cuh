@@ -73,6 +73,7 @@ __device__ __forceinline__ uint32_t new_full(const TrieView &tv, DirtyList d, ui
   tv.full_depth[f] = (uint16_t)depth;
   tv.full_epoch[f] = gen;
   tv.full_hlen[f] = 0;
+  tv.full_dead[f] = 0;
   dirty_push(tv.ctr, d, make_ref(KIND_FULL, f), depth);
   return f;
 }
@@ -1127,7 +1128,8 @@ template <bool kCoh>
 __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint64_t *stage, uint32_t stride) {
   uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
   bool full = kind == KIND_FULL;
-  if (!full && ldn<kCoh>(tv.short_dead + idx)) return;
+  // nodes a split or a delete unlinked are not hashed
+  if (ldn<kCoh>((full ? tv.full_dead : tv.short_dead) + idx)) return;
   // depth 0 holds exactly the roots of the forest's tries; go-ethereum
   // hashes a root whatever its size
   bool force = tv.geth_mode && (full ? ldn<kCoh>(tv.full_depth + idx) : ldn<kCoh>(tv.short_depth + idx)) == 0;
@@ -1340,6 +1342,7 @@ template <bool kCoh>
 __device__ __forceinline__ bool hash_full_warp(const TrieView &tv, uint32_t idx, uint8_t *msg, uint64_t *stage,
                                                uint32_t stride) {
   const int lane = threadIdx.x & 31;
+  if (ldn<kCoh>(tv.full_dead + idx)) return true;  // unlinked by a delete: nothing to hash
   EncItem it{0, 0, 0, nullptr, 0};
   if (lane < 17) it = child_item<kCoh>(tv, ldn<kCoh>(tv.full_child + (size_t)idx * 17 + lane));
   const uint32_t sz = lane < 17 ? it.pren + it.blen : 0u;

@@ -46,7 +46,7 @@ EXPORTS = [
     "gmpt_schedule_count", "gmpt_schedule_name", "gmpt_schedule_info", "gmpt_puts_schedule",
     "gmpt_puts_schedule_device", "gmpt_batch_features", "gmpt_batch_features_trie_device", "gmpt_selector_create",
     "gmpt_selector_destroy", "gmpt_selector_choose", "gmpt_selector_counts", "gmpt_puts_auto",
-    "gmpt_puts_auto_device",
+    "gmpt_puts_auto_device", "gmpt_gets_device", "gmpt_flush_dirty",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -191,6 +191,8 @@ def lib():
     L.gmpt_selector_choose.argtypes = [vp, vp, vp, vp]
     L.gmpt_selector_counts.argtypes = [vp, vp]
     L.gmpt_puts_auto.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp]
+    L.gmpt_gets_device.argtypes = [vp, vp, vp, vp, i32, i64, vp, vp]
+    L.gmpt_flush_dirty.argtypes = [vp, vp, vp, vp, vp]
     L.gmpt_puts_auto_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, i64, i64, i32, i64, vp]
     _lib = L
     return L
@@ -608,6 +610,31 @@ class MPT:
         _check(self._L.gmpt_gets_forest_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes),
                                                _p(hps), _p(sizes)))
         return hps[:n], sizes[:n]
+
+    def flush_dirty(self) -> list:
+        """gmpt_flush_dirty: [(hash, encoding)] of the nodes hashed since the
+        last flush (needs set_option("track_dirty", 1) before the puts)."""
+        h, e, ix = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        num = C.c_ulonglong(0)
+        _check(self._L.gmpt_flush_dirty(self._h, C.byref(h), C.byref(e), C.byref(ix), C.byref(num)))
+        n = num.value
+        out = []
+        try:
+            idx = np.ctypeslib.as_array(C.cast(ix, C.POINTER(C.c_ulonglong)), shape=(2 * n,)) if n else []
+            for i in range(n):
+                hb = C.string_at(h.value + 32 * i, 32)
+                a, z = int(idx[2 * i]), int(idx[2 * i + 1])
+                out.append((hb, C.string_at(e.value + a, z - a + 1)))
+        finally:
+            for p in (h, e, ix):
+                self._L.gmpt_free_buffer(p)
+        return out
+
+    def gets_device(self, d_keys, d_kidx, n: int, keys_bytes: int, d_out_hp, d_out_len, d_tids: int = 0):
+        """Lookups of device-resident keys with device-resident results."""
+        v = lambda a: C.c_void_p(a) if a else None  # noqa: E731
+        _check(self._L.gmpt_gets_device(self._h, v(d_keys), v(d_kidx), v(d_tids), int(n), int(keys_bytes),
+                                        v(d_out_hp), v(d_out_len)))
 
     def puts_raw(self, two_phase: bool, keys, keys_indexs, values, values_indexs, trie_ids=None, hps=None):
         """Put with RAW key bytes (keys_indexs: inclusive byte ranges, end =

@@ -287,13 +287,13 @@ class Runner:
         return n, kb, voff
 
     def features(self, reqs, n, kb, vb):
-        """Selector features: exact totals plus one sampling kernel over the
-        staged keys (gmpt_batch_features_device)."""
+        """Selector features from the library (gmpt_batch_features_trie_device:
+        exact totals plus one sampling kernel over the staged keys), with the
+        touched tenants' key count and number."""
         s = self.stage
-        st = self.g.batch_features_device(s.keys.data_ptr(), s.kidx.data_ptr(), n, kb)
         touched = set(r.tenant for r in reqs)
         trie_keys = sum(self.count[t] for t in touched)
-        return TU.features_from_stats(n, kb, st, vb / max(n, 1), trie_keys, len(touched))
+        return self.mpt.features_device(s.keys.data_ptr(), s.kidx.data_ptr(), n, kb, vb, len(touched), trie_keys)
 
     def snapshot(self, n, kb, vb):
         """Host copy of the staged batch (keys, values, trie ids)."""
@@ -304,14 +304,12 @@ class Runner:
     def put(self, reqs, k: int, n, kb, vb):
         if self.record is not None:
             self.record.append(self.snapshot(n, kb, vb))
-        two = TU.apply_config(self.mpt, k)
         s = self.stage
         touched = sorted(set(r.tenant for r in reqs))
-        if TU.CONFIGS[k].get("persistent"):
-            return self.mpt.block_update_device(s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(),
-                                                s.vidx.data_ptr(), s.tids.data_ptr(), 0, 0, n, n, kb, vb, touched)
-        self.mpt.puts_forest_device(two, s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(), s.vidx.data_ptr(),
-                                    s.tids.data_ptr(), n, kb, vb)
+        # the library runs schedule k (a persistent schedule hashes in the
+        # same launch, and the hash call then has nothing left to do)
+        self.mpt.puts_schedule_device(k, s.keys.data_ptr(), s.kidx.data_ptr(), s.vals.data_ptr(), s.vidx.data_ptr(),
+                                      n, kb, vb, d_tids=s.tids.data_ptr())
         self.mpt.hash_onepass_v2()
         return self.mpt.get_roots(touched)
 

@@ -170,6 +170,12 @@ int gmpt_puts_forest_device(gmpt_trie *t, int two_phase, const uint8_t *d_keys_h
  * results land in the host arrays as for gmpt_gets_parallel. */
 int gmpt_gets_forest_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids,
                             int n, int64_t keys_bytes, const uint8_t **values_hps, int *values_sizes);
+/* The same with DEVICE result arrays: d_values_hps[i] (the host pointer
+ * given with the value, as a uint64) and d_values_sizes[i] are written by the
+ * lookup kernel; nothing crosses to the host.  Synchronous on the trie's
+ * stream. */
+int gmpt_gets_device(gmpt_trie *t, const uint8_t *d_keys_hexs, const int *d_keys_indexs, const int *d_trie_ids, int n,
+                     int64_t keys_bytes, uint64_t *d_values_hps, int *d_values_sizes);
 
 /* ---- synthetic request batches in device memory (bench and tests) ----
  * gmpt_gen_ids: n ids; each is fresh (next_new, next_new + 1, ... in batch
@@ -320,6 +326,22 @@ int gmpt_get_values(gmpt_trie *t, const uint8_t *keys_hexs, const int *keys_inde
                     uint8_t *out, int64_t out_cap, int64_t *out_indexs, int64_t *out_len);
 
 int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
+
+/* The commit nodeset: (hash, RLP encoding) of every node hashed since the
+ * previous gmpt_flush_dirty (or since tracking began) that is still in a
+ * trie and is referenced by hash -- encoding of 32 bytes or more, or a root
+ * -- in its current state, each once, ordered by node reference.  hashs =
+ * 32 bytes per node (a root shorter than 32 bytes: its raw encoding,
+ * zero-padded), encs + inclusive [start, end] pairs encs_indexs[2 * num];
+ * the three arrays are malloc'd, release them with gmpt_free_buffer.  Needs
+ * the "track_dirty" option set to 1 before the puts whose nodes are to be
+ * exported (hash passes then keep a record of their nodes, 4 bytes per node,
+ * until the flush; persistent block updates are not recorded).  The
+ * reference exports every node on a set of key paths instead
+ * (MPT::flush_dirty_nodes, gpu_mpt.cuh:1039-1122, behind get_all_nodes,
+ * lib/libgmpt.cu:216-238); go-ethereum commits only the changed nodes. */
+int gmpt_flush_dirty(gmpt_trie *t, const uint8_t **hashs, const uint8_t **encs,
+                     const unsigned long long **encs_indexs, unsigned long long *num);
 /* Tuning knobs of the batch pipeline (results never depend on them):
  *   "local_build" 1/0: finish build segments of <= 2048 keys inside one CTA
  *                      each (default 1) or keep every level device-wide;
@@ -335,7 +357,9 @@ int gmpt_get_stats(gmpt_trie *t, gmpt_stats *out);
  *   "block_grid"  N:   CTAs of the persistent block kernel (0 = one per SM,
  *                      capped at what can be co-resident);
  *   "block_graph" 1/0: replay block launches from a captured CUDA graph
- *                      (default 1) or issue them one by one.
+ *                      (default 1) or issue them one by one;
+ *   "track_dirty" 1/0: record the nodes each hash pass rehashes for
+ *                      gmpt_flush_dirty (default 0).
  * Failure bounds (the reference instead spins without bound, util/lock.cuh:
  * 17-21, and asserts on arena overflow, util/allocator.cuh:115-118):
  *   "retry_limit" N:   failed CASes one LockNU key may take before the batch

@@ -185,6 +185,7 @@ enum { T_FULL = 1, T_SHORT = 2, T_VALUE = 3 };
 typedef struct onode {
   uint8_t type;
   uint8_t dirty;
+  uint8_t touched;    /* on a put path since the last omt_flush */
   uint8_t hlen;       /* length of hash[] (full/short nodes) */
   uint8_t hash[32];   /* Keccak-256, or the raw encoding if it is < 32 B */
   /* full */
@@ -271,6 +272,7 @@ static int prefix_len(const uint8_t *a, int alen, const uint8_t *b, int blen) {
  * *err is set on malformed (prefix) keys. */
 static onode *put_rec(omt_trie *t, onode *node, const uint8_t *key, int klen,
                       onode *value, int *dirty, int *err) {
+  if (node && node->type != T_VALUE) node->touched = 1;
   if (klen == 0) {
     if (node && node->type == T_VALUE) {
       *dirty = !(node->vlen == value->vlen &&
@@ -290,6 +292,7 @@ static onode *put_rec(omt_trie *t, onode *node, const uint8_t *key, int klen,
     s->key = key;
     s->klen = klen;
     s->val = value;
+    s->touched = 1;
     *dirty = 1;
     return s;
   }
@@ -312,6 +315,7 @@ static onode *put_rec(omt_trie *t, onode *node, const uint8_t *key, int klen,
       *err = OMT_ERR_NOMEM;
       return node;
     }
+    br->touched = 1;
     int d1 = 0, d2 = 0;
     br->child[node->key[m]] = put_rec(t, NULL, node->key + m + 1,
                                       node->klen - m - 1, node->val, &d1, err);
@@ -424,13 +428,11 @@ static void finish_hash(omt_trie *t, onode *node, const uint8_t *enc, int len,
   }
 }
 
-static void hash_rec(omt_trie *t, onode *node, int is_root) {
-  if (!node) return;
-  if (node->type == T_VALUE) return; /* hash := raw value bytes */
-  if (!node->dirty) return;
-  int force = is_root && t->mode == OMT_MODE_GETH;
+/* RLP encoding of a full or short node from its children's current
+ * references (node.cuh:46-112, 226-270) into the scratch buffer; returns
+ * its length. */
+static int encode_node(omt_trie *t, const onode *node, uint8_t **out) {
   if (node->type == T_SHORT) {
-    hash_rec(t, node->val, 0);
     uint8_t kcbuf[256];
     uint8_t *kc = node->klen / 2 + 1 <= (int)sizeof(kcbuf)
                       ? kcbuf
@@ -443,27 +445,101 @@ static void hash_rec(omt_trie *t, onode *node, int is_root) {
     o += rlp_str(e + o, kc, kn);
     o += child_item(t, e + o, node->val);
     (void)o;
-    t->stats.hashed_short++;
-    finish_hash(t, node, e, len, force);
-  } else {
-    for (int i = 0; i < 17; ++i) hash_rec(t, node->child[i], 0);
-    uint64_t payload = 0;
-    for (int i = 0; i < 17; ++i)
-      payload += node->child[i] ? (uint64_t)child_item_size(t, node->child[i]) : 1;
-    int len = rlp_list_head_size(payload) + (int)payload;
-    uint8_t *e = enc_buf(t, (size_t)len);
-    int o = rlp_list_head(e, payload);
-    for (int i = 0; i < 17; ++i) {
-      if (node->child[i])
-        o += child_item(t, e + o, node->child[i]);
-      else
-        e[o++] = 0x80;
-    }
-    t->stats.hashed_full++;
-    finish_hash(t, node, e, len, force);
+    *out = e;
+    return len;
   }
+  uint64_t payload = 0;
+  for (int i = 0; i < 17; ++i)
+    payload += node->child[i] ? (uint64_t)child_item_size(t, node->child[i]) : 1;
+  int len = rlp_list_head_size(payload) + (int)payload;
+  uint8_t *e = enc_buf(t, (size_t)len);
+  int o = rlp_list_head(e, payload);
+  for (int i = 0; i < 17; ++i) {
+    if (node->child[i])
+      o += child_item(t, e + o, node->child[i]);
+    else
+      e[o++] = 0x80;
+  }
+  *out = e;
+  return len;
+}
+
+static void hash_rec(omt_trie *t, onode *node, int is_root) {
+  if (!node) return;
+  if (node->type == T_VALUE) return; /* hash := raw value bytes */
+  if (!node->dirty) return;
+  int force = is_root && t->mode == OMT_MODE_GETH;
+  if (node->type == T_SHORT)
+    hash_rec(t, node->val, 0);
+  else
+    for (int i = 0; i < 17; ++i) hash_rec(t, node->child[i], 0);
+  uint8_t *e;
+  int len = encode_node(t, node, &e);
+  if (node->type == T_SHORT)
+    t->stats.hashed_short++;
+  else
+    t->stats.hashed_full++;
+  finish_hash(t, node, e, len, force);
   node->dirty = 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Commit nodeset: reachable nodes on put paths since the last flush          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct flushbuf {
+  uint8_t *hashs, *encs;
+  uint64_t *idx;
+  uint64_t num, cap, ebytes, ecap;
+} flushbuf;
+
+static int flush_rec(omt_trie *t, onode *node, int is_root, flushbuf *f) {
+  if (!node || node->type == T_VALUE) return 0;
+  if (node->type == T_SHORT) {
+    if (flush_rec(t, node->val, 0, f)) return 1;
+  } else {
+    for (int i = 0; i < 17; ++i)
+      if (flush_rec(t, node->child[i], 0, f)) return 1;
+  }
+  if (!node->touched) return 0;
+  node->touched = 0;
+  if (node->hlen != 32 && !is_root) return 0; /* embedded in its parent */
+  uint8_t *e;
+  int len = encode_node(t, node, &e);
+  if (f->num == f->cap) {
+    f->cap = f->cap ? 2 * f->cap : 1024;
+    f->hashs = (uint8_t *)realloc(f->hashs, 32 * f->cap);
+    f->idx = (uint64_t *)realloc(f->idx, 16 * f->cap);
+    if (!f->hashs || !f->idx) return 1;
+  }
+  if (f->ebytes + (uint64_t)len > f->ecap) {
+    f->ecap = 2 * (f->ebytes + (uint64_t)len) + 4096;
+    f->encs = (uint8_t *)realloc(f->encs, f->ecap);
+    if (!f->encs) return 1;
+  }
+  memset(f->hashs + 32 * f->num, 0, 32);
+  memcpy(f->hashs + 32 * f->num, node->hash, node->hlen);
+  memcpy(f->encs + f->ebytes, e, (size_t)len);
+  f->idx[2 * f->num] = f->ebytes;
+  f->idx[2 * f->num + 1] = f->ebytes + (uint64_t)len - 1;
+  f->ebytes += (uint64_t)len;
+  f->num++;
+  return 0;
+}
+
+int omt_flush(omt_trie *t, uint8_t **hashs, uint8_t **encs, uint64_t **encs_indexs,
+              uint64_t *num) {
+  flushbuf f;
+  memset(&f, 0, sizeof(f));
+  int rc = flush_rec(t, t->root, 1, &f);
+  *hashs = f.hashs;
+  *encs = f.encs;
+  *encs_indexs = f.idx;
+  *num = f.num;
+  return rc ? OMT_ERR_NOMEM : OMT_OK;
+}
+
+void omt_free_buffer(void *p) { free(p); }
 
 void omt_hash(omt_trie *t) {
   omt_stats keep = t->stats;

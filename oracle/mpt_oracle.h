@@ -90,6 +90,15 @@ void omt_gets(const omt_trie *t, const uint8_t *keys_hexs,
               const int *keys_indexs, int n, uint64_t *out_ptr,
               int *out_len);
 void omt_get_stats(const omt_trie *t, omt_stats *out);
+/* Commit nodeset (call after omt_hash): (hash, encoding) of every node
+ * reachable from the root that a put visited or created since the last
+ * omt_flush and that is referenced by hash (hash length 32) or is the root;
+ * hashs[32 * num] (zero-padded), encs + inclusive pairs encs_indexs[2 * num],
+ * children before parents.  Clears the marks.  Free the arrays with
+ * omt_free_buffer. */
+int omt_flush(omt_trie *t, uint8_t **hashs, uint8_t **encs, uint64_t **encs_indexs,
+              uint64_t *num);
+void omt_free_buffer(void *p);
 uint64_t omt_count_stats(omt_trie *t); /* refresh live node counts; returns total */
 
 #ifdef __cplusplus

@@ -64,6 +64,9 @@ def lib():
         L.omt_sha3_256.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
         L.omt_keccak_f1600.argtypes = [C.c_void_p]
         L.omt_keccak256_rows.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]
+        L.omt_flush.restype = C.c_int
+        L.omt_flush.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.omt_free_buffer.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -180,6 +183,26 @@ class OracleTrie:
         ln = np.zeros(n, np.int32)
         self._L.omt_gets(self._t, _ptr(kh), _ptr(ki), n, _ptr(ptr), _ptr(ln))
         return [None if p == 0 else C.string_at(int(p), int(l)) for p, l in zip(ptr, ln)]
+
+    def flush(self) -> list:
+        """[(hash32, encoding)] of the nodes on put paths since the last
+        flush that are referenced by hash or are the root (omt_flush)."""
+        h, e, ix = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        num = C.c_uint64(0)
+        if self._L.omt_flush(self._t, C.byref(h), C.byref(e), C.byref(ix), C.byref(num)) != 0:
+            raise MemoryError("oracle flush")
+        out = []
+        try:
+            n = num.value
+            idx = np.ctypeslib.as_array(C.cast(ix, C.POINTER(C.c_uint64)), shape=(2 * n,)) if n else []
+            for i in range(n):
+                a, z = int(idx[2 * i]), int(idx[2 * i + 1])
+                out.append((C.string_at(h.value + 32 * i, 32), C.string_at(e.value + a, z - a + 1)))
+        finally:
+            for p in (h, e, ix):
+                if p.value:
+                    self._L.omt_free_buffer(p)
+        return out
 
     def stats(self) -> dict:
         self._L.omt_count_stats(self._t)

@@ -150,3 +150,25 @@ def test_cpu_keccak_rows_matches_single_messages():
     rows = np.random.default_rng(1).integers(0, 256, (37, 20), dtype=np.uint8)
     out = O.keccak256_rows(rows)
     assert [O.keccak256(r.tobytes()) for r in rows] == [o.tobytes() for o in out]
+
+
+def test_oracle_flush_exports_the_changed_paths_once():
+    # two batches: the flush after each exports the nodes on that batch's
+    # paths, every exported hash is Keccak-256 of its encoding (or the root's
+    # raw encoding), and a flush with no puts in between exports nothing
+    b1 = W.random_keys(3000, 32, 40, seed=21)
+    b2 = W.random_keys(500, 32, 40, seed=22)
+    t = O.OracleTrie()
+    t.puts(b1.keys_hexs, b1.keys_indexs, b1.values, b1.values_indexs)
+    t.hash()
+    f1 = t.flush()
+    assert len(f1) == len({h for h, _ in f1})
+    for h, enc in f1:
+        assert O.keccak256(enc) == h
+    root = t.root()
+    assert f1[-1][0] == root  # children first: the root comes last
+    assert t.flush() == []
+    t.puts(b2.keys_hexs, b2.keys_indexs, b2.values, b2.values_indexs)
+    t.hash()
+    f2 = t.flush()
+    assert 0 < len(f2) < len(f1) and f2[-1][0] == t.root()
