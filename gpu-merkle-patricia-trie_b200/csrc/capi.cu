@@ -71,9 +71,13 @@ extern "C" {
 
 int gmpt_version(void) { return 1; }
 
-gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries) {
+gmpt_trie *gmpt_create_ex(int device, int encode_mode, int max_tries, unsigned flags) {
   if (max_tries < 1 || max_tries > (1 << 30)) {
     record(GMPT_E_ARG, "max_tries must be in [1, 2^30]");
+    return nullptr;
+  }
+  if (flags & ~(unsigned)GMPT_CREATE_UNIFIED_MEMORY) {
+    record(GMPT_E_ARG, "unknown creation flag");
     return nullptr;
   }
   gmpt_trie *h = new (std::nothrow) gmpt_trie{nullptr};
@@ -81,7 +85,7 @@ gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries) {
     record(GMPT_E_CAPACITY, "out of host memory");
     return nullptr;
   }
-  h->t = new (std::nothrow) gmpt::Trie(device, encode_mode, max_tries);
+  h->t = new (std::nothrow) gmpt::Trie(device, encode_mode, max_tries, (flags & GMPT_CREATE_UNIFIED_MEMORY) != 0);
   if (!h->t || !h->t->error().empty()) {
     record(GMPT_E_CUDA, h->t ? h->t->error() : "out of host memory");
     delete h->t;
@@ -90,6 +94,10 @@ gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries) {
   }
   record(0, "");
   return h;
+}
+
+gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries) {
+  return gmpt_create_ex(device, encode_mode, max_tries, 0);
 }
 
 gmpt_trie *gmpt_create(int device, int encode_mode) { return gmpt_create_forest(device, encode_mode, 1); }

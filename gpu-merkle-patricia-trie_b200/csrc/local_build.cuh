@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_
       }
       const bool cs = (k == S.start[q]) || L.lcp[k] == D;
       const bool ce = (k + 1 == S.end[q]) || L.lcp[k + 1] == D;
-      nb[r] = tv.keys[si.base[base + k] + D];
+      if (cs) nb[r] = tv.keys[si.base[base + k] + D];  // a child run's slot nibble
       if (cs && ce) {
         make_leaf(tv, dl, si, base + k, D + 1, ((uint64_t)f << 5) | nb[r], gen);
         L.seg[k] = 0xFFFF;

@@ -133,15 +133,17 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     // (thread t owns items [t*8, t*8+8))
     constexpr int ipt = kSortLocalCap / kSortLocalThreads;
     uint32_t starts = 0;
-    uint8_t st[ipt];
+    uint8_t st[ipt], tp[ipt + 1];
 #pragma unroll
-    for (int r = 0; r < ipt; ++r) {
-      int k = threadIdx.x * ipt + r;
+    for (int r = 0; r <= ipt; ++r) {
+      int k = threadIdx.x * ipt + r;  // r == ipt: the next thread's first item
       bool tied_prev;
       if (c == c0)
-        tied_prev = k > 0;
+        tied_prev = k > 0 && k < m;
       else
         tied_prev = k > 0 && k < m && L.key[src][k] == L.key[src][k - 1];
+      tp[r] = tied_prev ? 1 : 0;
+      if (r == ipt) break;
       st[r] = (k < m && !tied_prev) ? 1 : 0;
       starts += st[r];
     }
@@ -158,7 +160,10 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
       if (k >= m) continue;
       rank += st[r];
       uint32_t it = L.val[src][k];
-      uint32_t ch = c < nchunks ? key_chunk(tv.keys, koff[it], klen[it], c) : klen[it];
+      // an item already alone in its group keeps its place whatever its
+      // chunk: skip the gather of its key bytes
+      const bool single = !tp[r] && !tp[r + 1];
+      uint32_t ch = single ? 0u : (c < nchunks ? key_chunk(tv.keys, koff[it], klen[it], c) : klen[it]);
       uint64_t key = ((uint64_t)(rank - 1) << 32) | ch;
       L.key[src][k] = key;
     }

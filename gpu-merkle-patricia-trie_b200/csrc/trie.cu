@@ -34,11 +34,23 @@ constexpr int kDedupMinKeys = 1 << 16;
 
 inline unsigned blocks_for(int64_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
+// managed: unified memory (the trie may then exceed the device's memory,
+// pages migrating on demand -- the reference's UMMPT, mpt/um_mpt.cuh:13-52),
+// preferring the device the trie lives on
 template <typename T>
-cudaError_t grow_array(T *&p, size_t old_n, size_t new_n, cudaStream_t st) {
+cudaError_t grow_array(T *&p, size_t old_n, size_t new_n, cudaStream_t st, bool managed = false, int dev = 0) {
   T *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, new_n * sizeof(T) + 64);
+  const size_t bytes = new_n * sizeof(T) + 64;
+  cudaError_t e = managed ? cudaMallocManaged(&q, bytes) : cudaMalloc(&q, bytes);
   if (e != cudaSuccess) return e;
+  if (managed) {
+    e = cudaMemAdvise(q, bytes, cudaMemAdviseSetPreferredLocation, dev);
+    if (e == cudaSuccess) e = cudaMemAdvise(q, bytes, cudaMemAdviseSetAccessedBy, dev);
+    if (e != cudaSuccess) {
+      cudaFree(q);
+      return e;
+    }
+  }
   if (p && old_n) {
     e = cudaMemcpyAsync(q, p, old_n * sizeof(T), cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return e;
@@ -61,8 +73,9 @@ T *wsp(DevBlock &b, size_t n, cudaError_t &e) {
 
 // ---------------------------------------------------------------------------
 
-Trie::Trie(int device, int geth_mode, int max_tries)
-    : dev_(device), geth_(geth_mode ? 1 : 0), n_tries_(max_tries > 1 ? (uint32_t)max_tries : 1u) {
+Trie::Trie(int device, int geth_mode, int max_tries, bool unified)
+    : dev_(device), geth_(geth_mode ? 1 : 0), managed_(unified),
+      n_tries_(max_tries > 1 ? (uint32_t)max_tries : 1u) {
   cudaError_t e = cudaSetDevice(dev_);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&roots_, sizeof(uint32_t) * n_tries_ + 64);
@@ -199,12 +212,12 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
     uint64_t nc = std::min<uint64_t>(grow_to(need_full, cap_full_), kMaxNodes);
     if (opt_max_full_) nc = std::min<uint64_t>(nc, std::max<uint64_t>(opt_max_full_, need_full));
     size_t o = n_full_;
-    if (e == cudaSuccess) e = grow_array(tv_.full_child, o * 17, nc * 17, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.full_epoch, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.full_depth, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.full_hash, o * 32, nc * 32, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.full_hlen, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.full_dead, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_child, o * 17, nc * 17, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_epoch, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_depth, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_hash, o * 32, nc * 32, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_hlen, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.full_dead, o, nc, st_, managed_, dev_);
     if (e != cudaSuccess) return check_cuda(e, "grow branch pool");
     cap_full_ = (uint32_t)nc;
   }
@@ -213,16 +226,16 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   if (need_short > cap_short_) {
     uint64_t nc = std::min<uint64_t>(grow_to(need_short, cap_short_), kMaxNodes);
     size_t o = n_short_;
-    if (e == cudaSuccess) e = grow_array(tv_.short_key, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_klen, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_child, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_epoch, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_depth, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_dead, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_hash, o * 32, nc * 32, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_hlen, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_claim, o, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.short_pseudo, o, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_key, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_klen, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_child, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_epoch, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_depth, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_dead, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_hash, o * 32, nc * 32, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_hlen, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_claim, o, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.short_pseudo, o, nc, st_, managed_, dev_);
     if (e != cudaSuccess) return check_cuda(e, "grow short pool");
     cap_short_ = (uint32_t)nc;
   }
@@ -230,15 +243,15 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   if (need_value > kMaxNodes) return fail(E_CAPACITY, "value node count exceeds 2^30");
   if (need_value > cap_value_) {
     uint64_t nc = std::min<uint64_t>(grow_to(need_value, cap_value_), kMaxNodes);
-    if ((e = grow_array(tv_.value_vid, n_value_, nc, st_)) != cudaSuccess) return check_cuda(e, "grow values");
+    if ((e = grow_array(tv_.value_vid, n_value_, nc, st_, managed_, dev_)) != cudaSuccess) return check_cuda(e, "grow values");
     cap_value_ = (uint32_t)nc;
   }
   uint64_t need_rec = n_rec_ + add_rec;
   if (need_rec > cap_rec_) {
     uint64_t nc = grow_to(need_rec, cap_rec_);
-    if (e == cudaSuccess) e = grow_array(tv_.rec_off, n_rec_, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.rec_len, n_rec_, nc, st_);
-    if (e == cudaSuccess) e = grow_array(tv_.rec_hp, n_rec_, nc, st_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_off, n_rec_, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_len, n_rec_, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec_hp, n_rec_, nc, st_, managed_, dev_);
     if (e != cudaSuccess) return check_cuda(e, "grow value records");
     cap_rec_ = nc;
   }
@@ -246,7 +259,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   if (need_keys > cap_keys_) {
     uint64_t nc = grow_to(need_keys, cap_keys_);
     uint8_t *p = const_cast<uint8_t *>(tv_.keys);
-    if ((e = grow_array(p, key_used_, nc + 64, st_)) != cudaSuccess) return check_cuda(e, "grow key arena");
+    if ((e = grow_array(p, key_used_, nc + 64, st_, managed_, dev_)) != cudaSuccess) return check_cuda(e, "grow key arena");
     tv_.keys = p;
     cap_keys_ = nc;
   }
@@ -254,7 +267,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   if (need_vals > cap_vals_) {
     uint64_t nc = grow_to(need_vals, cap_vals_);
     uint8_t *p = const_cast<uint8_t *>(tv_.vals);
-    if ((e = grow_array(p, val_used_, nc + 64, st_)) != cudaSuccess) return check_cuda(e, "grow value arena");
+    if ((e = grow_array(p, val_used_, nc + 64, st_, managed_, dev_)) != cudaSuccess) return check_cuda(e, "grow value arena");
     tv_.vals = p;
     cap_vals_ = nc;
   }
@@ -268,8 +281,8 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
       cudaStreamSynchronize(st_);
       nd = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
     }
-    if (e == cudaSuccess) e = grow_array(dirty_ref_, nd, nc, st_);
-    if (e == cudaSuccess) e = grow_array(dirty_depth_, nd, nc, st_);
+    if (e == cudaSuccess) e = grow_array(dirty_ref_, nd, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(dirty_depth_, nd, nc, st_, managed_, dev_);
     if (e != cudaSuccess) return check_cuda(e, "grow dirty list");
     cap_dirty_ = nc;
   }
@@ -883,7 +896,8 @@ int Trie::bucket_and_hash() {
   if (track_dirty_) {  // keep this pass's nodes for flush_dirty
     if (fl_n_ + nd > fl_cap_) {
       uint64_t nc = std::max<uint64_t>(fl_n_ + nd, fl_cap_ + fl_cap_ / 2 + 1024);
-      if ((e = grow_array(fl_refs_, fl_n_, nc, st_)) != cudaSuccess) return check_cuda(e, "grow flush record");
+      if ((e = grow_array(fl_refs_, fl_n_, nc, st_, managed_, dev_)) != cudaSuccess)
+        return check_cuda(e, "grow flush record");
       fl_cap_ = nc;
     }
     if ((e = cudaMemcpyAsync(fl_refs_ + fl_n_, dirty_ref_, 4 * (size_t)nd, cudaMemcpyDeviceToDevice, st_)) !=

@@ -85,7 +85,8 @@ class Trie {
  public:
   // max_tries > 1 makes a forest: independent tries sharing the node pools
   // and arenas, addressed by trie id 0..max_tries-1
-  Trie(int device, int geth_mode, int max_tries = 1);
+  // unified: node pools, arenas and the dirty list in unified memory
+  Trie(int device, int geth_mode, int max_tries = 1, bool unified = false);
   ~Trie();
   Trie(const Trie &) = delete;
   Trie &operator=(const Trie &) = delete;
@@ -133,6 +134,7 @@ class Trie {
   cudaStream_t stream() const { return st_; }
   int device() const { return dev_; }
   int max_tries() const { return (int)n_tries_; }
+  bool unified() const { return managed_; }
   // value nodes in the pools (the keys stored, deleted ones included)
   uint64_t value_nodes() const { return n_value_; }
   void set_timing(bool on) { timing_ = on; }
@@ -169,6 +171,7 @@ class Trie {
  private:
   int dev_ = 0;
   int geth_ = 0;
+  bool managed_ = false;
   cudaStream_t st_ = nullptr;
   std::string err_;
   TrieStats stats_{};

@@ -820,7 +820,9 @@ __global__ void k_level_children(TrieView tv, DirtyList dl, SortedItems si, cons
   }
   bool cs = (i == sg.start[s]) || si.lcp[i] == D;
   bool ce = (i + 1 == sg.end[s]) || si.lcp[i + 1] == D;
-  uint8_t nib = tv.keys[si.base[i] + D];
+  // only the first item of a child run names the child slot: the other
+  // items skip the gather of their key's nibble
+  uint8_t nib = cs ? tv.keys[si.base[i] + D] : 0;
   uint64_t slot = ((uint64_t)f << 5) | nib;
   if (cs && ce) {
     make_leaf(tv, dl, si, i, D + 1, slot, gen);

@@ -46,7 +46,7 @@ EXPORTS = [
     "gmpt_schedule_count", "gmpt_schedule_name", "gmpt_schedule_info", "gmpt_puts_schedule",
     "gmpt_puts_schedule_device", "gmpt_batch_features", "gmpt_batch_features_trie_device", "gmpt_selector_create",
     "gmpt_selector_destroy", "gmpt_selector_choose", "gmpt_selector_counts", "gmpt_puts_auto",
-    "gmpt_puts_auto_device", "gmpt_gets_device", "gmpt_flush_dirty",
+    "gmpt_puts_auto_device", "gmpt_gets_device", "gmpt_flush_dirty", "gmpt_create_ex",
     "preprocess", "build_mpt_2phase", "build_mpt_olc", "get_all_nodes", "init_mpt", "insert_mpt_2phase",
     "insert_mpt_olc", "free_mpt",
 ]
@@ -100,6 +100,8 @@ def lib():
     L.gmpt_create.argtypes = [i32, i32]
     L.gmpt_create_forest.restype = vp
     L.gmpt_create_forest.argtypes = [i32, i32, i32]
+    L.gmpt_create_ex.restype = vp
+    L.gmpt_create_ex.argtypes = [i32, i32, i32, C.c_uint]
     L.gmpt_max_tries.argtypes = [vp]
     for f in ("gmpt_puts_2phase_forest", "gmpt_puts_latching_forest"):
         getattr(L, f).argtypes = [vp, vp, vp, vp, vp, vp, vp, i32]
@@ -397,9 +399,9 @@ class MPT:
     pools; the ``*_forest`` methods take a trie id per key and every other
     method addresses trie 0."""
 
-    def __init__(self, device: int = 0, mode: int = MODE_REF, max_tries: int = 1):
+    def __init__(self, device: int = 0, mode: int = MODE_REF, max_tries: int = 1, unified: bool = False):
         self._L = lib()
-        self._h = self._L.gmpt_create_forest(device, mode, int(max_tries))
+        self._h = self._L.gmpt_create_ex(device, mode, int(max_tries), 1 if unified else 0)
         if not self._h:
             raise GmptError(self._L.gmpt_last_error(), self._L.gmpt_last_error_message().decode())
 

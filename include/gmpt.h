@@ -67,6 +67,14 @@ void gmpt_destroy(gmpt_trie *t);
  * object (gpu_mpt.cuh:162-173); trie 0 of a forest is what every
  * single-trie call below addresses. */
 gmpt_trie *gmpt_create_forest(int device, int encode_mode, int max_tries);
+/* gmpt_create_forest with flags.  GMPT_CREATE_UNIFIED_MEMORY: the node
+ * pools, key / value arenas and dirty list live in unified memory
+ * (cudaMallocManaged, preferred location and accessed-by the device), so a
+ * trie may grow past the device's memory with pages migrating on demand --
+ * the reference's out-of-core UMMPT (mpt/um_mpt.cuh:13-52).  Results are
+ * the same; speed drops once pages migrate. */
+enum { GMPT_CREATE_UNIFIED_MEMORY = 1 };
+gmpt_trie *gmpt_create_ex(int device, int encode_mode, int max_tries, unsigned flags);
 int gmpt_max_tries(gmpt_trie *t);
 /* drop every node (capacity is kept) */
 int gmpt_reset(gmpt_trie *t);
