@@ -66,10 +66,21 @@ def parse():
     p.add_argument("--req-max", type=int, default=1 << 22)
     p.add_argument("--req-util", type=float, default=0.85, help="load of the plain server (arrival rate)")
     p.add_argument("--req-load", type=float, default=0.25, help="share of puts that fill a new empty tenant trie")
+    p.add_argument("--req-configs", default="",
+                   help="schedules timed in the request loop's matrix (comma-separated names; empty = all)")
+    p.add_argument("--req-full", action="store_true",
+                   help="the request loop at its configured ranges: tenants up to 64M keys, batches 1K-16M, "
+                        "2000 requests per stream (a dedicated run of several minutes)")
     p.add_argument("--vocab-n", type=int, default=8 << 20,
                    help="keys of the variable-length vocabulary-key section (0 = skip)")
     p.add_argument("--no-gets", action="store_true")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.req_full:
+        a.req_tenants = "0,2097152,16777216,67108864"
+        a.req_min, a.req_max = 1000, 1 << 24
+        a.req_eval, a.req_train, a.req_train_episode = 2000, 1000, 500
+        a.req_configs = a.req_configs or "phasenu,locknu-4,locknu-2,persistent-1cta"
+    return a
 
 
 # --------------------------------------------------------------------------
@@ -248,8 +259,24 @@ def cpu_baseline(args, batches):
             t.hash()
         dt = time.perf_counter() - t0
         kind, cores, desc = "port", 1, "C restatement of the reference CPU MPT, one thread"
-    return {"value": round(2 * n / dt / 1e6, 4), "unit": "Mkeys/s", "cores": cores, "kind": kind,
-            "sample": f"first {n} keys of the load and of the update batch; {desc}"}
+    out = {"value": round(2 * n / dt / 1e6, 4), "unit": "Mkeys/s", "cores": cores, "kind": kind,
+           "sample": f"first {n} keys of the load and of the update batch; {desc}"}
+    if kind == "reference":
+        # the reference's single-thread CPU_baseline: puts_baseline +
+        # hashs_dirty_flag (cpu_mpt.cuh:359-378, 498-505) on a quarter sample
+        m = max(n // 4, 1)
+        one = [b.subset(np.arange(m)) for b in batches]
+        t = O.RefTrie(big=True, threads=1)
+        t0 = time.perf_counter()
+        for b in one:
+            t.puts_baseline(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+            t.hash()
+        dt1 = time.perf_counter() - t0
+        t.close()
+        out["single_thread"] = {"value": round(2 * m / dt1 / 1e6, 4), "unit": "Mkeys/s", "cores": 1,
+                                "sample": f"first {m} keys of each batch; reference CpuMPT puts_baseline + "
+                                          "hashs_dirty_flag"}
+    return out
 
 
 def phase_roofline(batches, stats_all, hbm_peak, perm_peak):
@@ -608,8 +635,10 @@ def run_requests(args, local, dev):
         return tenants, S.make_stream(seed, count, tenants, ratio, args.req_min, args.req_max, load_frac=args.req_load)
 
     # training data: episodes of fresh tenant sets, every configuration timed
+    names = [c["name"] for c in TU.CONFIGS]
+    cfg = [names.index(x) for x in args.req_configs.split(",")] if args.req_configs else list(range(len(names)))
     tenants, st = stream(0x5EED0C60, args.req_train_episode, 0.2)
-    reps = [S.Runner(gmpt, tenants, local, dev, max_tries=4096) for _ in TU.CONFIGS]
+    reps = [S.Runner(gmpt, tenants, local, dev, max_tries=4096) for _ in cfg]
     Fs, Ts = [], []
     episodes = max(1, args.req_train // args.req_train_episode)
     for e in range(episodes):
@@ -623,7 +652,7 @@ def run_requests(args, local, dev):
             n0, kb0, vb0 = reps[0].build([x for x in st if x.kind == "put"][:1])
             reps[0].features([x for x in st if x.kind == "put"][:1], n0, kb0, vb0)
             reps[0].reset(tenants)
-        T, _, F = S.time_matrix(reps, st)
+        T, _, F = S.time_matrix(reps, st, configs=cfg)
         puts = np.array([r.kind == "put" for r in st])
         Fs.append(F[puts])
         Ts.append(T[puts])
@@ -640,7 +669,7 @@ def run_requests(args, local, dev):
                        f"batches log-uniform [{args.req_min}, {args.req_max}] keys, zipf theta U[0,1.2], puts mix "
                        "fresh keys (share U[0,1]) and zipf updates; Poisson arrivals at "
                        f"{args.req_util:.2f} load of the plain server",
-           "configs": [c["name"] for c in TU.CONFIGS],
+           "configs": [names[k] for k in cfg],
            "selector": "in the library: gmpt_selector (C++ rule table + the network's CUDA inference kernel), "
                        "trained by gmpt.tuner with the library's MLP kernels",
            "train": {"requests": episodes * args.req_train_episode, "episodes": episodes, "puts": int(len(Ftr)),
@@ -656,7 +685,7 @@ def run_requests(args, local, dev):
             r.reserve_for(ev)
         gc.collect()
         gc.disable()
-        T, G, F = S.time_matrix(reps, ev)
+        T, G, F = S.time_matrix(reps, ev, configs=cfg)
         gc.enable()
         final = reps[0].roots()
         isput = np.array([r.kind == "put" for r in ev])

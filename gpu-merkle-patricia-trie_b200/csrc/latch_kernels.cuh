@@ -350,13 +350,17 @@ __global__ void __launch_bounds__(256, GMPT_LATCH_CTAS) k_latch_insert(TrieView 
 // makes the insert walk every key as if there were no dedup.  Results never
 // depend on the hash.
 
-constexpr unsigned long long kDedupEmpty = ~0ull;
+constexpr unsigned long long kDedupEmpty = 0ull;
 
+// Slot s is two 8-byte words, [2s] the key hash (0 = free) and [2s + 1] the
+// largest batch position with that hash (low 32 bits), so a probe touches one
+// 16-byte pair: one DRAM sector per key instead of one per array.
 struct DedupTable {
-  unsigned long long *hash;  // [size], kDedupEmpty = free
-  uint32_t *pos;             // [size] largest batch position with that hash
+  unsigned long long *slot;  // [2 * size], zeroed = every slot free
   uint64_t mask;             // size - 1 (size a power of two)
   uint64_t hmask;            // hash bits kept (narrower only to test collisions)
+  __device__ __forceinline__ unsigned long long *hash(uint64_t s) const { return slot + 2 * s; }
+  __device__ __forceinline__ uint32_t *pos(uint64_t s) const { return reinterpret_cast<uint32_t *>(slot + 2 * s + 1); }
 };
 
 __device__ __forceinline__ uint64_t dedup_hash(const uint8_t *k, uint32_t len, uint32_t trie, uint64_t hmask) {
@@ -373,7 +377,7 @@ __device__ __forceinline__ uint64_t dedup_hash(const uint8_t *k, uint32_t len, u
   h = (h ^ (h >> 31)) * 0x94D049BB133111EBull;
   h ^= h >> 32;
   h &= hmask;
-  return h == kDedupEmpty ? 0ull : h;
+  return h == kDedupEmpty ? 1ull : h;
 }
 
 __device__ __forceinline__ uint64_t dedup_home(uint64_t h, uint64_t mask) {
@@ -394,10 +398,10 @@ __global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t
     // read before the atomics: a zipf-hot key repeats up to millions of
     // times, and a CAS or max that cannot change the slot would serialise
     // every one of them on the same address
-    unsigned long long old = __ldcg(&t.hash[s]);
-    if (old == kDedupEmpty) old = atomicCAS(&t.hash[s], kDedupEmpty, h);
+    unsigned long long old = __ldcg(t.hash(s));
+    if (old == kDedupEmpty) old = atomicCAS(t.hash(s), kDedupEmpty, h);
     if (old == kDedupEmpty || old == h) {
-      if (__ldcg(&t.pos[s]) < (uint32_t)i) atomicMax(&t.pos[s], (uint32_t)i);
+      if (__ldcg(t.pos(s)) < (uint32_t)i) atomicMax(t.pos(s), (uint32_t)i);
       slot_of[i] = (uint32_t)s;
       return;
     }
@@ -418,7 +422,7 @@ __global__ void k_dedup_mark(TrieView tv, const uint64_t *koff, const uint32_t *
     keep[i] = 1ull;
     return;
   }
-  const uint32_t w = t.pos[s];
+  const uint32_t w = *t.pos(s);
   bool kept = w == (uint32_t)i;
   if (!kept) {
     const bool same = klen[w] == len && (tid ? (uint32_t)tid[w] == tr : true) &&
@@ -446,7 +450,7 @@ __global__ void k_rw_slots(TrieView tv, const uint64_t *koff, const uint32_t *kl
     atomicOr(collision, 1u);
     s = 0;
   } else {
-    const uint32_t w = t.pos[s];
+    const uint32_t w = *t.pos(s);
     if (w != (uint32_t)i) {
       const bool same = klen[w] == len && (tid ? (uint32_t)tid[w] == tr : true) &&
                         match_nibbles(tv.keys + koff[w], k, (int)len) == (int)len;

@@ -497,20 +497,18 @@ int Trie::sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t ma
   cudaError_t e = cudaSuccess;
   uint64_t size = 1024;
   while (size < 2ull * (uint64_t)n) size <<= 1;
-  unsigned long long *hash = wsp<unsigned long long>(ws_.dd_hash, size, e);
-  uint32_t *hpos = wsp<uint32_t>(ws_.dd_pos, size, e);
+  unsigned long long *table = wsp<unsigned long long>(ws_.dd_hash, 2 * size, e);
   uint64_t *skey = wsp<uint64_t>(ws_.skey, (size_t)n, e);
   uint32_t *sval = wsp<uint32_t>(ws_.sval, (size_t)n, e);
   uint32_t *order = wsp<uint32_t>(ws_.order, (size_t)n, e);
   uint8_t *eqprev = wsp<uint8_t>(ws_.eqprev, (size_t)n + 1, e);
   unsigned long long *tot = wsp<unsigned long long>(ws_.rw_tot, 8, e);
   uint32_t *collision = reinterpret_cast<uint32_t *>(tot + 5);
-  if (e == cudaSuccess) e = cudaMemsetAsync(hash, 0xFF, sizeof(unsigned long long) * size, st_);
-  if (e == cudaSuccess) e = cudaMemsetAsync(hpos, 0, sizeof(uint32_t) * size, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(table, 0, 2 * sizeof(unsigned long long) * size, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(tot, 0, 64, st_);
   if (e != cudaSuccess) return check_cuda(e, "rw group alloc");
   const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
-  DedupTable tab{hash, hpos, size - 1, hmask};
+  DedupTable tab{table, size - 1, hmask};
   uint32_t *slot_of = wsp<uint32_t>(ws_.dd_slot, (size_t)n, e);
   if (e != cudaSuccess) return check_cuda(e, "rw group alloc");
   count_launch(), k_dedup_insert<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, slot_of);
@@ -1145,20 +1143,18 @@ int Trie::put_latching(const BatchIn &b) {
     cudaError_t e = cudaSuccess;
     uint64_t size = 1024;
     while (size < 2ull * (uint64_t)b.n) size <<= 1;
-    unsigned long long *hash = wsp<unsigned long long>(ws_.dd_hash, size, e);
-    uint32_t *pos = wsp<uint32_t>(ws_.dd_pos, size, e);
+    unsigned long long *table = wsp<unsigned long long>(ws_.dd_hash, 2 * size, e);
     uint32_t *sel = wsp<uint32_t>(ws_.dd_sel, (size_t)b.n, e);
     unsigned long long *keep = wsp<unsigned long long>(ws_.flags, (size_t)b.n, e);
     unsigned long long *rank = wsp<unsigned long long>(ws_.pos, (size_t)b.n, e);
     unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
     uint32_t *collision = reinterpret_cast<uint32_t *>(d_tot + 1);
     if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(b.n));
-    if (e == cudaSuccess) e = cudaMemsetAsync(hash, 0xFF, sizeof(unsigned long long) * size, st_);
-    if (e == cudaSuccess) e = cudaMemsetAsync(pos, 0, sizeof(uint32_t) * size, st_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(table, 0, 2 * sizeof(unsigned long long) * size, st_);
     if (e == cudaSuccess) e = cudaMemsetAsync(collision, 0, 4, st_);
     if (e != cudaSuccess) return check_cuda(e, "dedup alloc");
     const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
-    DedupTable tab{hash, pos, size - 1, hmask};
+    DedupTable tab{table, size - 1, hmask};
     uint32_t *slot_of = wsp<uint32_t>(ws_.dd_slot, (size_t)b.n, e);
     if (e != cudaSuccess) return check_cuda(e, "dedup alloc");
     count_launch(), k_dedup_insert<<<blocks_for(b.n), kThreads, 0, st_>>>(tv_, koff, klen, tid, b.n, tab, slot_of);
