@@ -589,6 +589,38 @@ int Trie::resolve_rw(int n, const uint32_t *order, const uint8_t *eqprev, const 
   return sync_counters();  // a bad flag rejects the batch before any insert
 }
 
+// A mixed batch was staged whole into the key arena, but after the reads
+// are answered only the kept writes' keys are referenced (by the leaves the
+// insert makes): move them to the start of the batch's region and give the
+// rest back, so a read-heavy stream does not fill the arena with keys
+// nothing points to.
+int Trie::compact_rw_keys(int m, const uint32_t *kept, uint64_t *koff, const uint32_t *klen, uint64_t key_base) {
+  cudaError_t e = cudaSuccess;
+  uint8_t *arena = const_cast<uint8_t *>(tv_.keys);
+  uint64_t total = 0;
+  if (m > 0) {
+    unsigned long long *sizes = wsp<unsigned long long>(ws_.rw_a, (size_t)m, e);
+    unsigned long long *offs = wsp<unsigned long long>(ws_.rw_b, (size_t)m, e);
+    unsigned long long *d_tot = wsp<unsigned long long>(ws_.rw_tot, 8, e) + 6;
+    if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(m));
+    if (e != cudaSuccess) return check_cuda(e, "rw compact alloc");
+    count_launch(), k_rw_kept_sizes<<<blocks_for(m), kThreads, 0, st_>>>(kept, m, klen, sizes);
+    if ((e = exclusive_scan<unsigned long long>(sizes, offs, m, d_tot, scan_ws_, st_)) != cudaSuccess)
+      return check_cuda(e, "rw compact scan");
+    total = read_u64(d_tot);
+    uint8_t *tmp = wsp<uint8_t>(ws_.raw, (size_t)total + 8, e);
+    if (e != cudaSuccess) return check_cuda(e, "rw compact alloc");
+    count_launch(), k_rw_kept_copy<<<blocks_for(m), kThreads, 0, st_>>>(tv_.keys, koff, klen, kept, offs, m, tmp);
+    if ((e = cudaMemcpyAsync(arena + key_base, tmp, (size_t)total, cudaMemcpyDeviceToDevice, st_)) != cudaSuccess)
+      return check_cuda(e, "rw compact copy");
+    count_launch(), k_rw_kept_offsets<<<blocks_for(m), kThreads, 0, st_>>>(kept, offs, m, key_base, koff);
+  }
+  if ((e = cudaMemsetAsync(arena + key_base + total, 0, 64, st_)) != cudaSuccess) return check_cuda(e, "rw compact tail");
+  key_used_ = key_base + ((total + 7) & ~7ull);
+  stats_.key_bytes = key_used_;
+  return OK;
+}
+
 // Level-synchronous construction over the T sorted items in ws_.sb_*.
 int Trie::build_levels(int T) {
   cudaError_t e = cudaSuccess;
@@ -701,6 +733,7 @@ int Trie::put_2phase(const BatchIn &b) {
   int m = 0;
   if (rw_) rw_->vid_base = vid_base;
   if ((rc = sort_unique(n, koff, klen, maxlen, tid, &uord, &m))) return rc;
+  if (rw_ && (rc = compact_rw_keys(m, uord, koff, klen, key_base))) return rc;
   stats_.last_unique = (uint64_t)m;
   if (timing_) cudaEventRecord(ev[2], st_);
   cudaError_t e = cudaSuccess;
@@ -1130,6 +1163,7 @@ int Trie::put_latching(const BatchIn &b) {
     int m = 0;
     if ((rc = sort_unique(b.n, koff, klen, maxlen, tid, &uord, &m))) return rc;
     if ((rc = sync_counters())) return rc;
+    if ((rc = compact_rw_keys(m, uord, koff, klen, key_base))) return rc;
     if (m == 0) {
       if (timing_)
         for (auto &x : ev) cudaEventDestroy(x);

@@ -294,6 +294,8 @@ class Trie {
   int sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                   uint32_t **uord, int *m);
   int build_levels(int T);
+  // mixed batch: keep only the m kept writes' key bytes in the arena
+  int compact_rw_keys(int m, const uint32_t *kept, uint64_t *koff, const uint32_t *klen, uint64_t key_base);
   int bucket_and_hash();
   uint64_t read_u64(const void *dptr);
 };

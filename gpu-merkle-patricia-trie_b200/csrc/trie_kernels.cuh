@@ -360,6 +360,31 @@ __global__ void k_rw_map(const uint32_t *order, const uint32_t *kept, int m, uin
   if (j < m) uord[j] = kept[order[j]];
 }
 
+// Key bytes of the kept writes of a mixed batch, moved together to the start
+// of the batch's region of the key arena (the reads' keys are referenced by
+// nothing once the reads are answered).  sizes -> scan -> copy out -> copy
+// back -> offsets.
+__global__ void k_rw_kept_sizes(const uint32_t *kept, int m, const uint32_t *klen, unsigned long long *sizes) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) sizes[j] = klen[kept[j]];
+}
+
+__global__ void k_rw_kept_copy(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, const uint32_t *kept,
+                               const unsigned long long *offs, int m, uint8_t *out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t i = kept[j];
+  const uint8_t *src = keys + koff[i];
+  uint8_t *dst = out + offs[j];
+  for (uint32_t b = 0; b < klen[i]; ++b) dst[b] = src[b];
+}
+
+__global__ void k_rw_kept_offsets(const uint32_t *kept, const unsigned long long *offs, int m, uint64_t base,
+                                  uint64_t *koff) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) koff[kept[j]] = base + offs[j];
+}
+
 __global__ void k_rw_read_flags(TrieView tv, const uint8_t *rw, int n, unsigned long long *is_read) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;

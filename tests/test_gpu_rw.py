@@ -185,3 +185,33 @@ def test_mixed_batch_hash_collisions_fall_back_exactly(gpu_lib, two_phase):
     t.hash_onepass_v2()
     assert t.get_root_hash() == oracle_root(O.MODE_REF, state)
     t.close()
+
+
+@pytest.mark.parametrize("two_phase", [False, True])
+def test_mixed_batches_keep_only_the_kept_writes_keys(gpu_lib, two_phase):
+    # the key arena grows by the kept writes' key bytes only: reads (and
+    # overwritten writes) give their bytes back after the batch
+    rng = W.Xoshiro256ss(91)
+    pool = keyset(rng, 3000, 24, 256)
+    t = gpu_lib.MPT()
+    load = make_batch([nib(k) for k in pool], [b"v" * 8] * len(pool))
+    t.puts_2phase_with_valuehp(load.keys_hexs, load.keys_indexs, load.values, load.values_indexs)
+    t.hash_onepass_v2()
+    state = {(0, k): (0, b"v" * 8) for k in pool}
+    for rnd in range(3):
+        before = t.stats()["key_bytes"]
+        keys, flags, vals, hps = mixed_ops(rng, pool, 5000, 0.3 if rnd < 2 else 0.0, [])
+        b = make_batch([nib(k) for k in keys], [v if f else b"" for v, f in zip(vals, flags)])
+        hp, sz = t.puts_with_read(two_phase, b.keys_hexs, b.keys_indexs, flags, b.values, b.values_indexs,
+                                  values_hps=hps)
+        t.hash_onepass_v2()
+        want = expect(state, keys, flags, vals, hps)
+        assert list(zip(hp.tolist(), sz.tolist())) == want
+        last = {}
+        for k, f in zip(keys, flags):
+            if f:
+                last[k] = len(nib(k))
+        grown = t.stats()["key_bytes"] - before
+        assert grown == (sum(last.values()) + 7) // 8 * 8
+        assert t.get_root_hash() == oracle_root(O.MODE_REF, state)
+    t.close()
