@@ -37,6 +37,7 @@ struct LocalSmem {
   uint16_t seg[kLocalCap];  // segment of each item at this level, 0xFFFF = done
   uint32_t warp_sums[kLocalThreads / 32 + 1];
   uint32_t nseg;
+  uint32_t leaf_base, dirty_base, leaf_ok;  // this level's leaf short nodes
 };
 
 __global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_build(TrieView tv, DirtyList dl, SortedItems si,
@@ -98,15 +99,20 @@ __global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_
       write_slot(tv, S.slot[q], top);
     }
     __syncthreads();
-    // 3a. children of each branch: leaves now; count next-level segment starts
+    // 3a. children of each branch: singleton children become leaves (made in
+    // 3b, their short nodes allocated once for the whole CTA: one global
+    // atomic per level instead of one per warp); count next-level segment
+    // starts and leaves
     uint8_t fl[kLocalIpt];
     uint8_t nb[kLocalIpt];
-    uint32_t my_starts = 0;
+    uint16_t lq[kLocalIpt];
+    uint32_t leafbits = 0, my_starts = 0, my_leaves = 0;
 #pragma unroll
     for (int r = 0; r < kLocalIpt; ++r) {
       const int k = tid * kLocalIpt + r;
       fl[r] = 0;
       nb[r] = 0;
+      lq[r] = 0;
       if (k >= m) continue;
       const uint16_t q = L.seg[k];
       if (q == 0xFFFF) continue;
@@ -119,15 +125,19 @@ __global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_
       const bool ce = (k + 1 == S.end[q]) || L.lcp[k + 1] == D;
       if (cs) nb[r] = tv.keys[si.base[base + k] + D];  // a child run's slot nibble
       if (cs && ce) {
-        make_leaf(tv, dl, si, base + k, D + 1, ((uint64_t)f << 5) | nb[r], gen);
+        leafbits |= 1u << r;
+        lq[r] = q;
+        if (D + 1 < si.len[base + k]) ++my_leaves;  // else the value links straight in
         L.seg[k] = 0xFFFF;
         continue;
       }
       fl[r] = 1 | (cs ? 2 : 0) | (ce ? 4 : 0);
       my_starts += cs ? 1u : 0u;
     }
-    // block-wide exclusive scan of the starts (items are in thread order)
-    uint32_t incl = my_starts;
+    // block-wide exclusive scan of (leaves << 16 | starts) (items are in
+    // thread order; each count is at most kLocalCap < 2^16)
+    const uint32_t mine = (my_leaves << 16) | my_starts;
+    uint32_t incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -142,11 +152,51 @@ __global__ void __launch_bounds__(kLocalThreads, GMPT_LOCAL_BUILD_CTAS) k_local_
         L.warp_sums[w] = run;
         run += c;
       }
-      L.warp_sums[kLocalThreads / 32] = run;
+      L.warp_sums[kLocalThreads / 32] = run & 0xFFFFu;
+      const uint32_t tl = run >> 16;
+      L.leaf_ok = 1;
+      if (tl) {
+        const uint32_t b0 = atomicAdd(&tv.ctr->n_short, tl);
+        if (b0 + tl > tv.cap_short) {  // nothing pushed to the dirty list then
+          set_error(tv.ctr, ERR_CAPACITY);
+          L.leaf_ok = 0;
+        } else {
+          L.leaf_base = b0;
+          L.dirty_base = atomicAdd(&tv.ctr->n_dirty, tl);
+        }
+      }
     }
     __syncthreads();
-    // 3b. an item's next-level segment is the latest start at or before it
-    uint32_t run = L.warp_sums[wid] + incl - my_starts;  // starts before this thread
+    // 3b. leaves; an item's next-level segment is the latest start at or before it
+    const uint32_t before = L.warp_sums[wid] + incl - mine;
+    uint32_t run = before & 0xFFFFu;  // starts before this thread
+    uint32_t lb = before >> 16;       // leaf short nodes before this thread
+#pragma unroll
+    for (int r = 0; r < kLocalIpt; ++r) {
+      if (!((leafbits >> r) & 1u)) continue;
+      const uint32_t q = lq[r], i = base + tid * kLocalIpt + r;
+      const uint32_t x = S.D[q] + 1, len = si.len[i];
+      const uint64_t slot = ((uint64_t)S.branch[q] << 5) | nb[r];
+      if (x >= len) {
+        write_slot(tv, slot, si.ref[i]);
+        continue;
+      }
+      const uint32_t j = lb++;
+      if (!L.leaf_ok) continue;
+      const uint32_t sn = L.leaf_base + j;
+      tv.short_key[sn] = si.base[i] + x;
+      tv.short_klen[sn] = len - x;
+      tv.short_child[sn] = si.ref[i];
+      tv.short_depth[sn] = (uint16_t)x;
+      tv.short_epoch[sn] = gen;
+      tv.short_dead[sn] = 0;
+      tv.short_claim[sn] = 0;
+      tv.short_hlen[sn] = 0;
+      const uint32_t ref = make_ref(KIND_SHORT, sn);
+      dl.ref[L.dirty_base + j] = ref;
+      dl.depth[L.dirty_base + j] = (uint16_t)x;
+      write_slot(tv, slot, ref);
+    }
 #pragma unroll
     for (int r = 0; r < kLocalIpt; ++r) {
       const int k = tid * kLocalIpt + r;
