@@ -24,8 +24,10 @@ __device__ __forceinline__ uint32_t load_slot(const uint32_t *p) {
   return *reinterpret_cast<const volatile uint32_t *>(p);
 }
 
+// Pool slots are taken warp-aggregated among the lanes that allocate
+// together (one atomic per warp on the pool counter, not one per lane).
 __device__ __forceinline__ uint32_t alloc_short(const TrieView &tv) {
-  uint32_t s = atomicAdd(&tv.ctr->n_short, 1u);
+  uint32_t s = warp_alloc(&tv.ctr->n_short, 1u);
   if (s >= tv.cap_short) {
     set_error(tv.ctr, ERR_CAPACITY);
     return 0xFFFFFFFFu;
@@ -34,7 +36,7 @@ __device__ __forceinline__ uint32_t alloc_short(const TrieView &tv) {
 }
 
 __device__ __forceinline__ uint32_t alloc_full(const TrieView &tv) {
-  uint32_t f = atomicAdd(&tv.ctr->n_full, 1u);
+  uint32_t f = warp_alloc(&tv.ctr->n_full, 1u);
   if (f >= tv.cap_full) {
     set_error(tv.ctr, ERR_CAPACITY);
     return 0xFFFFFFFFu;
@@ -67,7 +69,7 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
     uint32_t kind = ref_kind(ref), idx = ref_idx(ref);
     if (kind == KIND_NULL) {
       if (vnode == 0xFFFFFFFFu) {
-        vnode = atomicAdd(&tv.ctr->n_value, 1u);
+        vnode = warp_alloc(&tv.ctr->n_value, 1u);
         if (vnode >= tv.cap_value) {
           set_error(tv.ctr, ERR_CAPACITY);
           return;
@@ -137,7 +139,7 @@ __device__ __noinline__ void latch_from(TrieView tv, DirtyList dl, uint32_t *sp,
     ch[sk[mm]] = rest;
     // this key's leaf
     if (vnode == 0xFFFFFFFFu) {
-      vnode = atomicAdd(&tv.ctr->n_value, 1u);
+      vnode = warp_alloc(&tv.ctr->n_value, 1u);
       if (vnode >= tv.cap_value) {
         set_error(tv.ctr, ERR_CAPACITY);
         return;
