@@ -45,7 +45,9 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours",
+                   help="reference: the reference's CPU MPT on the host cores (the reference arm); "
+                        "reference-gpu: the reference's own GPU library on this GPU (a separate measurement)")
     p.add_argument("--n", type=int, default=1 << 24, help="keys per batch")
     p.add_argument("--strategy", default="auto", help="auto | 2phase | latching | 2phase,latching")
     p.add_argument("--latch-ways", type=int, default=4, help="keys per LockNU thread (1, 2, 4)")
@@ -232,6 +234,73 @@ def run_reference(args, world, rank):
         "e2e": {"value": round(v, 4), "unit": "Mkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "root": root.hex(),
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu(args, world, rank):
+    """The reference's own GPU library (oracle/_ref/libgmpt_ref_gpu.so:
+    lib/libgmpt.cu compiled unmodified for sm_100a by oracle/Makefile) through
+    its public C ABI: init_mpt, then insert_mpt_olc (LockNU +
+    hash_onepass_v2 + get_root_hash, lib/libgmpt.cu:248-321) per batch, host
+    arrays in and the root out, as go-ethereum calls it; wall clock per step
+    (its host-to-device copies inside, as its API makes them).  A fresh trie
+    per step; the reference frees nothing, so each step keeps its 17 GB of
+    arenas until the process exits."""
+    if rank != 0:
+        return
+    import ctypes as C
+
+    path = REPO / "oracle" / "_ref" / "libgmpt_ref_gpu.so"
+    if not path.exists():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/libgmpt_ref_gpu.so not built"}))
+        return
+    L = C.CDLL(str(path))
+    L.init_mpt.restype = C.c_void_p
+    L.insert_mpt_olc.restype = C.c_void_p
+    L.insert_mpt_olc.argtypes = [C.c_void_p] * 6 + [C.c_int]
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    batches = make_workload(args.n)
+    arrs = [(np.ascontiguousarray(b.keys_hexs), np.ascontiguousarray(b.keys_indexs, np.int32),
+             np.ascontiguousarray(b.values), np.ascontiguousarray(b.values_indexs, np.int64), b.n) for b in batches]
+    times, roots = [], []
+    for it in range(args.warmup + args.steps):
+        h = L.init_mpt()
+        t0 = time.perf_counter()
+        rs = []
+        for kh, ki, vb, vi, n in arrs:
+            r = L.insert_mpt_olc(h, P(kh), P(ki), P(vb), P(vi), None, n)
+            rs.append(C.string_at(r, 32).hex() if r else "")
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+            roots.append(rs)
+    # a batch of distinct keys (the 2^20 random-key configuration) for a
+    # clean root comparison: the reference's LockNU keeps an arbitrary one of
+    # a key's repeated writes (gpu_mpt_kernels.cuh:1004-1027)
+    c1 = W.random_keys(1 << 20)
+    h = L.init_mpt()
+    t0 = time.perf_counter()
+    r = L.insert_mpt_olc(h, P(c1.keys_hexs), P(np.ascontiguousarray(c1.keys_indexs, np.int32)), P(c1.values),
+                         P(np.ascontiguousarray(c1.values_indexs, np.int64)), None, c1.n)
+    c1_ms = (time.perf_counter() - t0) * 1e3
+    c1_root = C.string_at(r, 32).hex() if r else ""
+    golden_path = REPO / "tests" / "golden" / "config_roots.json"
+    cases = json.loads(golden_path.read_text())["cases"] if golden_path.exists() else {}
+    gold = golden_roots(args.n)
+    keys = sum(b.n for b in batches)
+    m = statistics.median(times)
+    line = {"metric": "put+root-hash Mkeys/s", "value": round(keys / m / 1e6, 3), "unit": "Mkeys/s",
+            "impl": "reference-gpu", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(m * 1e3, 3), "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"ycsb-shaped load {args.n} + zipf(0.99) updates {args.n}; 23 B keys, 100 B "
+                                   "values; fresh trie per step", "keys_per_step": keys},
+            "path": "reference lib/libgmpt.cu insert_mpt_olc per batch (LockNU + hash_onepass_v2 + root), host "
+                    "arrays, wall clock",
+            "roots": roots[-1], "load_root_matches_oracle": bool(gold) and roots[-1][0] == gold[0],
+            "update_root_matches_oracle": bool(gold) and roots[-1][1] == gold[1],
+            "random_2pow20": {"ms": round(c1_ms, 3), "mkeys_s": round(c1.n / (c1_ms / 1e3) / 1e6, 3),
+                              "root": c1_root,
+                              "root_matches_oracle": c1_root == cases.get("c1_random_1m", {}).get("roots", [""])[0]}}
     print(json.dumps(line), flush=True)
 
 
@@ -1102,6 +1171,9 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.impl == "reference-gpu":
+        run_reference_gpu(args, world, rank)
         return
     run_ours(args, world, rank, local)
 
