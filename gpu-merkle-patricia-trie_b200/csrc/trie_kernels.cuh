@@ -901,6 +901,16 @@ __device__ __forceinline__ uint32_t full_class(const TrieView &tv, uint32_t idx)
   return min((20u + 32u * cnt) / 136u, kHashClasses - 1u);
 }
 
+// Finer classes for the order inside one hashing CTA (leaves with values of
+// up to kilobytes take 1 to 31 blocks): 1, 2, 3, 4, 5-6, 7-10, 11-18, 19+
+// blocks.
+constexpr uint32_t kCtaClasses = 8;
+
+__device__ __forceinline__ uint32_t blocks_class(uint32_t blocks_minus_1) {
+  const uint32_t b = blocks_minus_1;
+  return b < 4u ? b : (b < 6u ? 4u : (b < 10u ? 5u : (b < 18u ? 6u : 7u)));
+}
+
 __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   const uint32_t kind = ref_kind(r), idx = ref_idx(r);
   uint32_t bytes;
@@ -912,7 +922,7 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
     bytes = tv.short_klen[idx] / 2u + 8u;
     bytes += ref_kind(ch) == KIND_VALUE ? tv.rec_len[tv.value_vid[ref_idx(ch)]] : 33u;
   }
-  return min(bytes / 136u, kHashClasses - 1u);
+  return blocks_class(bytes / 136u);
 }
 
 // bin of a dirty node: (nibble depth, kind, hash class); the class is
@@ -1466,15 +1476,15 @@ constexpr int kHashLevelThreads = 128;  // k_hash_level's block size (the partit
 __global__ void __launch_bounds__(kHashLevelThreads, 6) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
   __shared__ uint32_t s_ref[kHashLevelThreads];
-  __shared__ uint32_t s_cnt[kHashClasses][kHashLevelThreads / 32];  // [class][warp]
+  __shared__ uint32_t s_cnt[kCtaClasses][kHashLevelThreads / 32];  // [class][warp]
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool valid = t < count;
   const uint32_t r = valid ? refs[t] : 0u;
-  const uint32_t c = valid ? hash_class(tv, r) : kHashClasses;
+  const uint32_t c = valid ? hash_class(tv, r) : kCtaClasses;
   uint32_t mine = 0;
 #pragma unroll
-  for (uint32_t v = 0; v < kHashClasses; ++v) {
+  for (uint32_t v = 0; v < kCtaClasses; ++v) {
     const unsigned b = __ballot_sync(0xffffffffu, c == v);
     if (lane == 0) s_cnt[v][warp] = (uint32_t)__popc(b);
     if (c == v) mine = (uint32_t)__popc(b & ((1u << lane) - 1u));
@@ -1482,7 +1492,7 @@ __global__ void __launch_bounds__(kHashLevelThreads, 6) k_hash_level(TrieView tv
   __syncthreads();
   if (valid) {
     uint32_t pos = mine;
-    for (uint32_t v = 0; v < kHashClasses; ++v)
+    for (uint32_t v = 0; v < kCtaClasses; ++v)
       for (int w = 0; w < kHashLevelThreads / 32; ++w)
         if (v < c || (v == c && w < warp)) pos += s_cnt[v][w];
     s_ref[pos] = r;
