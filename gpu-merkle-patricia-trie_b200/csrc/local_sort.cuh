@@ -18,14 +18,22 @@ constexpr int kSortLocalThreads = 256;
 constexpr int kSortLocalWarps = kSortLocalThreads / 32;
 constexpr int kSortLocalPerWarp = kSortLocalCap / kSortLocalWarps;  // 256 items, 8 rounds
 
+// groups no larger than this are ordered by direct counting instead of radix passes
+constexpr uint32_t kSortSmallGroup = 32;
+
 struct LocalSortSmem {
   uint64_t key[2][kSortLocalCap];
   uint32_t val[2][kSortLocalCap];
-  uint16_t cnt[kSortLocalWarps][256];  // per-warp digit counts, then offsets (<= kSortLocalCap)
+  union {
+    uint16_t cnt[kSortLocalWarps][256];  // radix pass: per-warp digit counts, then offsets (<= kSortLocalCap)
+    uint16_t gbeg[kSortLocalCap];        // small-group pass: first position of every tied group
+  };
   uint32_t warp_tmp[kSortLocalWarps + 1];
   unsigned long long mask;
   uint32_t maxlen;
+  uint32_t maxg;
 };
+static_assert(kSortLocalWarps * 256 == kSortLocalCap, "gbeg shares the radix counters' space");
 
 // block-wide exclusive scan of one value per thread
 __device__ __forceinline__ uint32_t cta_excl_scan(uint32_t v, uint32_t *tmp, uint32_t &total) {
@@ -151,14 +159,21 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     uint32_t rank = cta_excl_scan(starts, L.warp_tmp, ngroups);
     if (ngroups == (uint32_t)m) break;  // every key distinct
     // build (rank, chunk) keys in the current order
-    if (threadIdx.x == 0) L.mask = 0;
+    if (threadIdx.x == 0) {
+      L.mask = 0;
+      L.maxg = 0;
+    }
     __syncthreads();
     uint64_t acc = 0, k0 = 0;
+    uint16_t gid[ipt];
 #pragma unroll
     for (int r = 0; r < ipt; ++r) {
       int k = threadIdx.x * ipt + r;
+      gid[r] = 0;
       if (k >= m) continue;
       rank += st[r];
+      gid[r] = (uint16_t)(rank - 1);
+      if (c > c0 && st[r]) L.gbeg[rank - 1] = (uint16_t)k;
       uint32_t it = L.val[src][k];
       // an item already alone in its group keeps its place whatever its
       // chunk: skip the gather of its key bytes
@@ -167,7 +182,42 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
       uint64_t key = ((uint64_t)(rank - 1) << 32) | ch;
       L.key[src][k] = key;
     }
+    if (c > c0 && threadIdx.x == 0) L.gbeg[ngroups] = (uint16_t)m;  // ngroups < m <= kSortLocalCap
     __syncthreads();
+    if (c > c0) {
+      // Largest tied group: when every group is small (the usual tail, a
+      // few pairs among singletons), each item finds its place in its group
+      // by counting the members that order before it -- one pass instead
+      // of one radix pass per varying byte of (rank, chunk).
+      uint32_t gmax = 0;
+#pragma unroll
+      for (int r = 0; r < ipt; ++r) {
+        const int k = threadIdx.x * ipt + r;
+        if (k < m && st[r]) gmax = max(gmax, (uint32_t)(L.gbeg[gid[r] + 1] - L.gbeg[gid[r]]));
+      }
+      gmax = __reduce_max_sync(0xffffffffu, gmax);
+      if ((threadIdx.x & 31) == 0 && gmax) atomicMax(&L.maxg, gmax);
+      __syncthreads();
+      if (L.maxg <= kSortSmallGroup) {
+#pragma unroll
+        for (int r = 0; r < ipt; ++r) {
+          const int k = threadIdx.x * ipt + r;
+          if (k >= m) continue;
+          const uint64_t key = L.key[src][k];
+          const uint32_t b = L.gbeg[gid[r]], e = L.gbeg[gid[r] + 1];
+          uint32_t pos = b;
+          for (uint32_t j = b; j < e; ++j) {  // stable: equal chunks keep their order
+            const uint64_t kj = L.key[src][j];
+            pos += (kj < key || (kj == key && j < (uint32_t)k)) ? 1u : 0u;
+          }
+          L.key[src ^ 1][pos] = key;
+          L.val[src ^ 1][pos] = L.val[src][k];
+        }
+        src ^= 1;
+        __syncthreads();
+        continue;
+      }
+    }
     k0 = L.key[src][0];
     for (int k = threadIdx.x; k < m; k += kSortLocalThreads) acc |= L.key[src][k] ^ k0;
     for (int o = 16; o; o >>= 1) acc |= __shfl_xor_sync(0xffffffffu, acc, o);
