@@ -193,8 +193,7 @@ __global__ void __launch_bounds__(256) k_block_stage(TrieView tv, BlockBufs bb) 
                     (int64_t)bb.patch_off[i] + 32 > ve - vs + 1))
       bad |= BLOCK_BAD_PATCH;
     const uint64_t vid = vid_base + (uint64_t)i;
-    tv.rec_off[vid] = val_base + (uint64_t)vs;
-    tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
+    tv.rec[vid] = ValueRec{val_base + (uint64_t)vs, (uint32_t)(ve - vs + 1), 0u};
     tv.rec_hp[vid] = 0;
   }
   terms = __reduce_add_sync(0xffffffffu, terms);
@@ -259,7 +258,7 @@ __global__ void __launch_bounds__(256, 2) k_block(TrieView tv0, DirtyList dl, Bl
       for (int i = n0 + t; i < n; i += T) {
         const int pt = bb.patch_trie[i];
         if (pt < 0) continue;
-        uint8_t *dst = const_cast<uint8_t *>(tv.vals) + tv.rec_off[vid_base + (uint64_t)i] + bb.patch_off[i];
+        uint8_t *dst = const_cast<uint8_t *>(tv.vals) + tv.rec[vid_base + (uint64_t)i].off + bb.patch_off[i];
         const uint32_t r = __ldcg(tv.roots + pt);
         const uint32_t kind = ref_kind(r), idx = ref_idx(r);
         const uint8_t *h = kind == KIND_FULL ? tv.full_hash + (size_t)idx * 32

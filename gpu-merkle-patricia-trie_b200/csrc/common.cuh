@@ -57,6 +57,14 @@ struct Counters {
   uint32_t pad3;
 };
 
+// A value record: byte offset into the value arena and length, side by side
+// in 16 bytes so one sector holds both (a leaf's hash reads them together).
+struct __align__(16) ValueRec {
+  uint64_t off;
+  uint32_t len;
+  uint32_t pad;
+};
+
 // Everything a kernel needs to reach the trie; passed by value.
 struct TrieView {
   // branch (full) nodes
@@ -79,8 +87,7 @@ struct TrieView {
   uint32_t *short_pseudo; // pseudo item created by that claim
   // value nodes -> value records
   unsigned long long *value_vid;
-  uint64_t *rec_off;      // byte offset into the value arena
-  uint32_t *rec_len;
+  ValueRec *rec;          // value records (arena offset + length)
   uint64_t *rec_hp;       // caller's host pointer (echoed by gets)
   // arenas
   const uint8_t *keys;    // nibble arena (one byte per nibble, 16 = term.)
@@ -117,6 +124,13 @@ __device__ __forceinline__ uint32_t warp_alloc(uint32_t *counter, uint32_t n) {
   if ((int)lane == leader && total) base = atomicAdd(counter, total);
   base = __shfl_sync(mask, base, leader);
   return base + before;
+}
+
+// One value record in a single 16-byte load (records are written by the
+// staging launch and never change afterwards: the read-only path is safe).
+__device__ __forceinline__ ValueRec load_rec(const TrieView &tv, uint64_t vid) {
+  const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2 *>(tv.rec) + vid);
+  return ValueRec{v.x, (uint32_t)v.y, 0u};
 }
 
 // Unaligned 8-byte little-endian load from a byte array padded by >= 8 bytes.

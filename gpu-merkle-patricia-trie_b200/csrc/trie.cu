@@ -101,7 +101,7 @@ Trie::~Trie() {
   void *ptrs[] = {tv_.full_child, tv_.full_epoch, tv_.full_depth, tv_.full_hash, tv_.full_hlen, tv_.full_dead, fl_refs_,
                   tv_.short_key, tv_.short_klen, tv_.short_child, tv_.short_epoch, tv_.short_depth,
                   tv_.short_dead, tv_.short_hash, tv_.short_hlen, tv_.short_claim, tv_.short_pseudo,
-                  tv_.value_vid, tv_.rec_off, tv_.rec_len, tv_.rec_hp, (void *)tv_.keys, (void *)tv_.vals,
+                  tv_.value_vid, tv_.rec, tv_.rec_hp, (void *)tv_.keys, (void *)tv_.vals,
                   roots_, ctr_, dirty_ref_, dirty_depth_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -249,8 +249,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   uint64_t need_rec = n_rec_ + add_rec;
   if (need_rec > cap_rec_) {
     uint64_t nc = grow_to(need_rec, cap_rec_);
-    if (e == cudaSuccess) e = grow_array(tv_.rec_off, n_rec_, nc, st_, managed_, dev_);
-    if (e == cudaSuccess) e = grow_array(tv_.rec_len, n_rec_, nc, st_, managed_, dev_);
+    if (e == cudaSuccess) e = grow_array(tv_.rec, n_rec_, nc, st_, managed_, dev_);
     if (e == cudaSuccess) e = grow_array(tv_.rec_hp, n_rec_, nc, st_, managed_, dev_);
     if (e != cudaSuccess) return check_cuda(e, "grow value records");
     cap_rec_ = nc;
@@ -290,7 +289,7 @@ int Trie::ensure_capacity(uint64_t add_full, uint64_t add_short, uint64_t add_va
   tv_.cap_short = cap_short_;
   tv_.cap_value = cap_value_;
   stats_.device_bytes = (uint64_t)cap_full_ * (68 + 4 + 2 + 32 + 1 + 1) + (uint64_t)cap_short_ * (8 + 4 + 4 + 4 + 2 + 1 + 32 + 1 + 8) +
-                        (uint64_t)cap_value_ * 8 + cap_rec_ * 20 + cap_keys_ + cap_vals_ + cap_dirty_ * 6;
+                        (uint64_t)cap_value_ * 8 + cap_rec_ * 24 + cap_keys_ + cap_vals_ + cap_dirty_ * 6;
   return OK;
 }
 
@@ -1085,7 +1084,7 @@ int Trie::get_values(const uint8_t *keys_hexs, const int *keys_indexs, int n, st
   std::vector<uint64_t> roff(n, 0);
   for (int i = 0; i < n; ++i) {
     if (vid[i] < 0) continue;
-    e = cudaMemcpyAsync(&roff[i], tv_.rec_off + vid[i], 8, cudaMemcpyDeviceToHost, st_);
+    e = cudaMemcpyAsync(&roff[i], &tv_.rec[vid[i]].off, 8, cudaMemcpyDeviceToHost, st_);
     if (e != cudaSuccess) return check_cuda(e, "get_values rec");
   }
   cudaStreamSynchronize(st_);

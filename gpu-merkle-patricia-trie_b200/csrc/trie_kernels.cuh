@@ -145,8 +145,7 @@ __global__ void __launch_bounds__(256) k_stage(TrieView tv, const int *ki, const
       ve = -1;
     }
     uint64_t vid = vid_base + (uint64_t)i;
-    tv.rec_off[vid] = val_base + (uint64_t)vs;
-    tv.rec_len[vid] = (uint32_t)(ve - vs + 1);
+    tv.rec[vid] = ValueRec{val_base + (uint64_t)vs, (uint32_t)(ve - vs + 1), 0u};
     tv.rec_hp[vid] = hp ? hp[i] : 0ull;
   }
   __shared__ uint32_t red[3][8];
@@ -429,7 +428,7 @@ __global__ void k_rw_resolve(TrieView tv, const uint32_t *order, const uint8_t *
   }
   const unsigned long long r = rrank[i];
   out_hp[r] = vid < 0 ? 0ull : tv.rec_hp[vid];
-  out_len[r] = vid < 0 ? 0 : (int)tv.rec_len[vid];
+  out_len[r] = vid < 0 ? 0 : (int)tv.rec[vid].len;
 }
 
 // ---------------------------------------------------------------------------
@@ -920,7 +919,7 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
     if (tv.short_dead[idx]) return 0u;
     const uint32_t ch = tv.short_child[idx];
     bytes = tv.short_klen[idx] / 2u + 8u;
-    bytes += ref_kind(ch) == KIND_VALUE ? tv.rec_len[tv.value_vid[ref_idx(ch)]] : 33u;
+    bytes += ref_kind(ch) == KIND_VALUE ? load_rec(tv, tv.value_vid[ref_idx(ch)]).len : 33u;
   }
   return blocks_class(bytes / 136u);
 }
@@ -1059,8 +1058,9 @@ __device__ __forceinline__ EncItem child_item(const TrieView &tv, uint32_t r) {
   uint32_t hl;
   if (kind == KIND_VALUE) {
     unsigned long long vid = ldn<kCoh>(tv.value_vid + idx);
-    h = tv.vals + tv.rec_off[vid];
-    hl = tv.rec_len[vid];
+    const ValueRec rc = load_rec(tv, vid);
+    h = tv.vals + rc.off;
+    hl = rc.len;
   } else {
     if (kind == KIND_FULL) {
       h = tv.full_hash + (size_t)idx * 32;
@@ -1201,9 +1201,10 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
     prefetch_l1(kp);
     if (ref_kind(child) == KIND_VALUE) {
       unsigned long long vid = tv.value_vid[ref_idx(child)];
-      const uint8_t *vp = tv.vals + tv.rec_off[vid];
+      const ValueRec rc = load_rec(tv, vid);
+      const uint8_t *vp = tv.vals + rc.off;
       prefetch_l1(vp);
-      if (tv.rec_len[vid] > 120) prefetch_l1(vp + 128);
+      if (rc.len > 120) prefetch_l1(vp + 128);
     } else {
       prefetch_child(tv, child);
     }
@@ -1544,7 +1545,7 @@ __global__ void k_gets(TrieView tv, const uint8_t *keys, const int *idx, int n, 
     out_len[i] = 0;
   } else {
     out_hp[i] = tv.rec_hp[vid];
-    out_len[i] = (int)tv.rec_len[vid];
+    out_len[i] = (int)tv.rec[vid].len;
   }
 }
 
@@ -1568,8 +1569,9 @@ __global__ void k_roots(TrieView tv, const int *ids, int n, uint8_t *out) {
     len = tv.short_hlen[idx];
   } else if (kind == KIND_VALUE) {
     unsigned long long vid = tv.value_vid[idx];
-    h = tv.vals + tv.rec_off[vid];
-    len = min(32u, tv.rec_len[vid]);
+    const ValueRec rc = tv.rec[vid];
+    h = tv.vals + rc.off;
+    len = min(32u, rc.len);
   }
   out[t] = (h && (uint32_t)t < len) ? h[t] : 0;
   if (t == 0) out[32] = (uint8_t)len;
