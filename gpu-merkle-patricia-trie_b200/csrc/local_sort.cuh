@@ -223,7 +223,31 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     for (int o = 16; o; o >>= 1) acc |= __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc) atomicOr(&L.mask, (unsigned long long)acc);
     __syncthreads();
-    const uint64_t mask = L.mask;
+    uint64_t mask = L.mask;
+    {
+      // nibbles that vary move to the low end of every key when that saves
+      // digit passes (the order and the equalities between keys are kept;
+      // the keys are rebuilt from scratch for the next chunk)
+      uint64_t nmask = 0;
+      int nv = 0, bytes = 0;
+      for (int k = 0; k < 16; ++k)
+        if ((mask >> (4 * k)) & 0xFull) {
+          nmask |= 0xFull << (4 * k);
+          ++nv;
+        }
+      for (int b = 0; b < 8; ++b) bytes += ((mask >> (8 * b)) & 0xFFull) ? 1 : 0;
+      if ((4 * nv + 7) / 8 < bytes) {
+        for (int k = threadIdx.x; k < m; k += kSortLocalThreads) {
+          const uint64_t x = L.key[src][k];
+          uint64_t out = 0;
+          for (int q = 15; q >= 0; --q)
+            if ((nmask >> (4 * q)) & 0xFull) out = (out << 4) | ((x >> (4 * q)) & 0xFull);
+          L.key[src][k] = out;
+        }
+        mask = nv >= 16 ? ~0ull : ((1ull << (4 * nv)) - 1);
+        __syncthreads();
+      }
+    }
     for (int shift = 0; shift < 64; shift += 8) {
       if (((mask >> shift) & 0xFF) == 0) continue;
       cta_radix_pass(L, src, m, shift);

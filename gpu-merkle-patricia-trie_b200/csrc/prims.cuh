@@ -187,6 +187,35 @@ static __global__ void k_or_diff(const uint64_t *keys, int64_t n, unsigned long 
   if (threadIdx.x == 0 && s) atomicOr(mask, s);
 }
 
+// Nibble packing around the digit passes: the nibbles that vary across the
+// keys (nmask) move, in order, to the low end of each key, so a key whose
+// varying bits are spread over many bytes (one nibble in each of several
+// bytes, as in nibble-per-byte keys) sorts in fewer 8-bit passes.  Packing
+// keeps the order (it drops only nibbles that are equal in every key), and
+// unpacking puts them back next to the common nibbles of key k0.
+static __global__ void k_nibble_pack(uint64_t *keys, int64_t n, uint64_t nmask) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t x = keys[i];
+  uint64_t out = 0;
+  for (int k = 15; k >= 0; --k)
+    if ((nmask >> (4 * k)) & 0xFull) out = (out << 4) | ((x >> (4 * k)) & 0xFull);
+  keys[i] = out;
+}
+
+static __global__ void k_nibble_unpack(uint64_t *keys, int64_t n, uint64_t nmask, uint64_t k0) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t p = keys[i];
+  uint64_t x = k0 & ~nmask;
+  for (int k = 0; k < 16; ++k)
+    if ((nmask >> (4 * k)) & 0xFull) {
+      x |= (p & 0xFull) << (4 * k);
+      p >>= 4;
+    }
+  keys[i] = x;
+}
+
 static __global__ void k_radix_hist(const uint64_t *keys, int64_t n, int shift, uint32_t *counts, int tiles) {
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
@@ -260,7 +289,7 @@ struct RadixSorter {
   cudaError_t init() {
     cudaError_t e = mask.ensure(64);
     if (e != cudaSuccess) return e;
-    if (!h_mask) e = cudaMallocHost(&h_mask, sizeof(unsigned long long));
+    if (!h_mask) e = cudaMallocHost(&h_mask, 2 * sizeof(unsigned long long));
     return e;
   }
   void release() {
@@ -284,10 +313,26 @@ struct RadixSorter {
     int grid = (int)((n + 1023) / 1024);
     if (grid > 2048) grid = 2048;
     count_launch(), k_or_diff<<<grid, 256, 0, st>>>(keys, n, mask.as<unsigned long long>());
+    // the varying bits and the first key (its nibbles are every key's common ones)
     if ((e = cudaMemcpyAsync(h_mask, mask.p, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(h_mask + 1, keys, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    uint64_t m = *h_mask;
+    uint64_t m = h_mask[0];
+    const uint64_t k0 = h_mask[1];
     if (m == 0) return cudaSuccess;
+    uint64_t nmask = 0;
+    int nv = 0, bytes = 0;
+    for (int k = 0; k < 16; ++k)
+      if ((m >> (4 * k)) & 0xFull) {
+        nmask |= 0xFull << (4 * k);
+        ++nv;
+      }
+    for (int b = 0; b < 8; ++b) bytes += ((m >> (8 * b)) & 0xFFull) ? 1 : 0;
+    const bool pack = (4 * nv + 7) / 8 < bytes;
+    if (pack) {
+      count_launch(), k_nibble_pack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(keys, n, nmask);
+      m = nv >= 16 ? ~0ull : ((1ull << (4 * nv)) - 1);
+    }
     int tiles = (int)((n + kSortTile - 1) / kSortTile);
     if ((e = alt_keys.ensure((size_t)n * 8)) != cudaSuccess) return e;
     if ((e = alt_vals.ensure((size_t)n * 4)) != cudaSuccess) return e;
@@ -313,6 +358,7 @@ struct RadixSorter {
       if ((e = cudaMemcpyAsync(keys, kin, (size_t)n * 8, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
       if ((e = cudaMemcpyAsync(vals, vin, (size_t)n * 4, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
     }
+    if (pack) count_launch(), k_nibble_unpack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(keys, n, nmask, k0);
     return cudaGetLastError();
   }
 };
