@@ -301,7 +301,10 @@ def run_reference_gpu(args, world, rank):
             "random_2pow20": {"ms": round(c1_ms, 3), "mkeys_s": round(c1.n / (c1_ms / 1e3) / 1e6, 3),
                               "root": c1_root,
                               "root_matches_oracle": c1_root == cases.get("c1_random_1m", {}).get("roots", [""])[0]}}
-    print(json.dumps(line), flush=True)
+    # the reference prints its roots and timings through C stdio: flush them
+    # first so the JSON line stands on a line of its own
+    C.CDLL(None).fflush(None)
+    print("\n" + json.dumps(line), flush=True)
 
 
 def cpu_baseline(args, batches):
