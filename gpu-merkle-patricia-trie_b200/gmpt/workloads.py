@@ -251,20 +251,25 @@ def ycsb_load(n: int, value_bytes: int = 100, seed: int = 0x5EED0002) -> Batch:
     return Batch(kh, ki, vb, vi)
 
 
-def zipf_ranks(rng: Xoshiro256ss, n_items: int, n: int, theta: float) -> np.ndarray:
-    """Gray et al.'s zipfian generator (as in YCSB's ZipfianGenerator)."""
+def zipf_from_uniform(u: np.ndarray, n_items: int, theta: float) -> np.ndarray:
+    """Gray et al.'s zipfian generator (as in YCSB's ZipfianGenerator) on
+    given uniforms in [0, 1)."""
     if theta <= 0.0:
-        return (rng.uniform(n) * n_items).astype(np.int64).clip(0, n_items - 1)
+        return (u * n_items).astype(np.int64).clip(0, n_items - 1)
     i = np.arange(1, n_items + 1, dtype=np.float64)
     zetan = float(np.sum(i ** -theta))
     zeta2 = 1.0 + 0.5 ** theta
     alpha = 1.0 / (1.0 - theta) if theta != 1.0 else 1e9
     eta = (1.0 - (2.0 / n_items) ** (1.0 - theta)) / (1.0 - zeta2 / zetan)
-    u = rng.uniform(n)
     uz = u * zetan
     r = (n_items * np.power(np.maximum(eta * u - eta + 1.0, 0.0), alpha)).astype(np.int64)
     r = np.where(uz < 1.0, 0, np.where(uz < 1.0 + 0.5 ** theta, 1, r))
     return np.clip(r, 0, n_items - 1)
+
+
+def zipf_ranks(rng: Xoshiro256ss, n_items: int, n: int, theta: float) -> np.ndarray:
+    """n zipfian ranks over n_items (zipf_from_uniform of the next n draws)."""
+    return zipf_from_uniform(rng.uniform(n), n_items, theta)
 
 
 def ycsb_zipf_updates(n_loaded: int, n: int, theta: float = 0.99, value_bytes: int = 100,
@@ -292,12 +297,25 @@ def vocab_keys(n: int, seed: int = 0x5EED0004, vocab_size: int = 10000,
     letters = (rng.words(int(woff[-1])) % np.uint64(26)).astype(np.uint8) + ord("a")
     klen = np.clip(np.rint(np.exp(mu + sigma * rng.normal(n))), min_len, max_len).astype(np.int64)
     max_words = max_len // 2 + 1
-    words = zipf_ranks(rng, vocab_size, n * max_words, 0.8).reshape(n, max_words)
+    # word j of key i comes from uniform draw (i, j) of one block of n *
+    # max_words draws; ranks are computed only for the words a key uses
+    # (column by column while its length is not reached)
+    u = rng.uniform(n * max_words).reshape(n, max_words)
+    words = np.zeros((n, max_words), dtype=np.int64)
+    wlen = np.zeros((n, max_words), dtype=np.int64)
+    cum_all = np.zeros((n, max_words), dtype=np.int64)
+    cum = np.zeros(n, dtype=np.int64)
+    for j in range(max_words):
+        rows = np.nonzero(cum < klen)[0]
+        if len(rows) == 0:
+            break
+        words[rows, j] = zipf_from_uniform(u[rows, j], vocab_size, 0.8)
+        wlen[rows, j] = wl[words[rows, j]]
+        cum_all[rows, j] = cum[rows]
+        cum[rows] += wlen[rows, j]
     # concatenate words, truncate to klen
-    wlen = wl[words]                                         # [n, max_words]
-    cum = np.cumsum(wlen, axis=1) - wlen                     # start of each word in key
-    take = cum < klen[:, None]                               # words that contribute
-    piece = np.minimum(wlen, klen[:, None] - cum) * take     # bytes taken from each word
+    take = (cum_all < klen[:, None]) & (wlen > 0)            # words that contribute
+    piece = np.minimum(wlen, klen[:, None] - cum_all) * take  # bytes taken from each word
     flat_piece = piece.reshape(-1)
     flat_word = words.reshape(-1)
     total = int(flat_piece.sum())
