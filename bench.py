@@ -59,29 +59,31 @@ def parse():
     p.add_argument("--eth-blocks", type=int, default=512)
     p.add_argument("--eth-compare-blocks", type=int, default=32,
                    help="blocks also run through the per-trie and forest multi-launch paths")
-    p.add_argument("--req-tenants", default="0,1048576,4194304,16777216",
+    p.add_argument("--req-tenants", default="0,1048576,4194304,8388608",
                    help="pre-existing keys of each tenant trie of the request loop (empty = skip)")
     p.add_argument("--req-train", type=int, default=1200, help="requests of the selector's training streams")
     p.add_argument("--req-train-episode", type=int, default=300, help="requests per training episode")
     p.add_argument("--req-eval", type=int, default=300, help="requests of each evaluation stream")
     p.add_argument("--req-min", type=int, default=1000)
-    p.add_argument("--req-max", type=int, default=1 << 22)
+    p.add_argument("--req-max", type=int, default=1 << 21)
     p.add_argument("--req-util", type=float, default=0.85, help="load of the plain server (arrival rate)")
     p.add_argument("--req-load", type=float, default=0.25, help="share of puts that fill a new empty tenant trie")
-    p.add_argument("--req-configs", default="",
-                   help="schedules timed in the request loop's matrix (comma-separated names; empty = all)")
+    p.add_argument("--req-configs",
+                   default="phasenu,locknu-4,locknu-2,persistent-1cta,locknu-4-nodedup,phasenu-warp-hash",
+                   help="schedules timed in the request loop's matrix (comma-separated names; empty = all); "
+                        "every one holds a replica of the tenant forest")
     p.add_argument("--req-full", action="store_true",
-                   help="the request loop at its configured ranges: tenants up to 64M keys, batches 1K-16M, "
-                        "2000 requests per stream (a dedicated run of several minutes)")
+                   help="the request loop at the largest ranges that fit four replicas on one GPU: tenants "
+                        "up to 32M keys, batches 1K-8M, 2000 requests per stream (a dedicated run of minutes)")
     p.add_argument("--vocab-n", type=int, default=8 << 20,
                    help="keys of the variable-length vocabulary-key section (0 = skip)")
     p.add_argument("--no-gets", action="store_true")
     a = p.parse_args()
     if a.req_full:
-        a.req_tenants = "0,2097152,16777216,67108864"
-        a.req_min, a.req_max = 1000, 1 << 24
+        a.req_tenants = "0,4194304,16777216,33554432"
+        a.req_min, a.req_max = 1000, 1 << 23
         a.req_eval, a.req_train, a.req_train_episode = 2000, 1000, 500
-        a.req_configs = a.req_configs or "phasenu,locknu-4,locknu-2,persistent-1cta"
+        a.req_configs = "phasenu,locknu-4,locknu-2,persistent-1cta"
     return a
 
 
@@ -683,7 +685,7 @@ def run_eth(args, local, dev):
     }
 
 
-MERGE_KEYS = 1 << 23  # largest merged batch of the queue-draining server
+MERGE_KEYS = 1 << 22  # largest merged batch of the queue-draining server
 
 
 def run_requests(args, local, dev):
