@@ -686,6 +686,9 @@ def run_eth(args, local, dev):
 
 
 MERGE_KEYS = 1 << 22  # largest merged batch of the queue-draining server
+# largest window of the mixed read/write server: one mixed call answers every
+# request of its window at once, so a smaller window keeps the tail latency down
+MIXED_KEYS = 1 << 20
 
 
 def run_requests(args, local, dev):
@@ -769,12 +772,13 @@ def run_requests(args, local, dev):
 
         def live(name, policy, batching, mixed=False):
             rn.reset(tenants)
+            cap = MIXED_KEYS if mixed else MERGE_KEYS
             if batching:
-                rn.reserve_for(ev, merged_keys=MERGE_KEYS)
+                rn.reserve_for(ev, merged_keys=cap)
             fb0 = csel.counts()[1]
             gc.collect()
             gc.disable()  # service times are host wall clock: no collector pauses inside
-            r = S.serve(rn, ev, policy, batching, max_keys=MERGE_KEYS, mixed=mixed)
+            r = S.serve(rn, ev, policy, batching, max_keys=cap, mixed=mixed)
             gc.enable()
             assert rn.roots() == final, f"{name}: roots differ from the fixed-schedule replicas"
             res[name] = {"mkeys_s": round(r.keys / (r.busy_ms / 1e3) / 1e6, 3),
