@@ -62,29 +62,20 @@ def parse():
     p.add_argument("--req-tenants", default="0,1048576,4194304,8388608",
                    help="pre-existing keys of each tenant trie of the request loop (empty = skip)")
     p.add_argument("--req-train", type=int, default=1200, help="requests of the selector's training streams")
-    p.add_argument("--req-train-episode", type=int, default=300, help="requests per training episode")
+    p.add_argument("--req-train-episode", type=int, default=150, help="requests per training episode")
     p.add_argument("--req-eval", type=int, default=300, help="requests of each evaluation stream")
     p.add_argument("--req-min", type=int, default=1000)
-    p.add_argument("--req-max", type=int, default=1 << 21)
+    p.add_argument("--req-max", type=int, default=1 << 20)
     p.add_argument("--req-util", type=float, default=0.85, help="load of the plain server (arrival rate)")
     p.add_argument("--req-load", type=float, default=0.25, help="share of puts that fill a new empty tenant trie")
     p.add_argument("--req-configs",
                    default="phasenu,locknu-4,locknu-2,persistent-1cta,locknu-4-nodedup,phasenu-warp-hash",
                    help="schedules timed in the request loop's matrix (comma-separated names; empty = all); "
                         "every one holds a replica of the tenant forest")
-    p.add_argument("--req-full", action="store_true",
-                   help="the request loop at the largest ranges that fit four replicas on one GPU: tenants "
-                        "up to 32M keys, batches 1K-8M, 2000 requests per stream (a dedicated run of minutes)")
     p.add_argument("--vocab-n", type=int, default=8 << 20,
                    help="keys of the variable-length vocabulary-key section (0 = skip)")
     p.add_argument("--no-gets", action="store_true")
-    a = p.parse_args()
-    if a.req_full:
-        a.req_tenants = "0,4194304,16777216,33554432"
-        a.req_min, a.req_max = 1000, 1 << 23
-        a.req_eval, a.req_train, a.req_train_episode = 2000, 1000, 500
-        a.req_configs = "phasenu,locknu-4,locknu-2,persistent-1cta"
-    return a
+    return p.parse_args()
 
 
 # --------------------------------------------------------------------------
@@ -286,6 +277,21 @@ def run_reference_gpu(args, world, rank):
                          P(np.ascontiguousarray(c1.values_indexs, np.int64)), None, c1.n)
     c1_ms = (time.perf_counter() - t0) * 1e3
     c1_root = C.string_at(r, 32).hex() if r else ""
+    # the same batch through the reference's class under its other insert +
+    # hash pairings (which of its paths agrees with its CPU MPT)
+    variants = {}
+    if hasattr(L, "ref_gpu_variant_root"):
+        L.ref_gpu_variant_root.restype = C.c_int
+        L.ref_gpu_variant_root.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+        out = np.zeros(32, np.uint8)
+        for v, name in ((0, "puts_latching_with_valuehp+hash_onepass"),
+                        (1, "puts_latching_with_valuehp_v2+hash_onepass_v2"),
+                        (2, "puts_2phase_with_valuehp+hash_onepass_v2")):
+            out[:] = 0
+            sz = L.ref_gpu_variant_root(v, P(c1.keys_hexs), P(np.ascontiguousarray(c1.keys_indexs, np.int32)),
+                                        P(c1.values), P(np.ascontiguousarray(c1.values_indexs, np.int64)), c1.n,
+                                        P(out))
+            variants[name] = out.tobytes().hex() if sz == 32 else f"size {sz}"
     golden_path = REPO / "tests" / "golden" / "config_roots.json"
     cases = json.loads(golden_path.read_text())["cases"] if golden_path.exists() else {}
     gold = golden_roots(args.n)
@@ -302,7 +308,9 @@ def run_reference_gpu(args, world, rank):
             "update_root_matches_oracle": bool(gold) and roots[-1][1] == gold[1],
             "random_2pow20": {"ms": round(c1_ms, 3), "mkeys_s": round(c1.n / (c1_ms / 1e3) / 1e6, 3),
                               "root": c1_root,
-                              "root_matches_oracle": c1_root == cases.get("c1_random_1m", {}).get("roots", [""])[0]}}
+                              "root_matches_oracle": c1_root == cases.get("c1_random_1m", {}).get("roots", [""])[0],
+                              "oracle_root": cases.get("c1_random_1m", {}).get("roots", [""])[0],
+                              "reference_class_paths": variants}}
     # the reference prints its roots and timings through C stdio: flush them
     # first so the JSON line stands on a line of its own
     C.CDLL(None).fflush(None)
@@ -685,7 +693,7 @@ def run_eth(args, local, dev):
     }
 
 
-MERGE_KEYS = 1 << 22  # largest merged batch of the queue-draining server
+MERGE_KEYS = 1 << 21  # largest merged batch of the queue-draining server
 # largest window of the mixed read/write server: one mixed call answers every
 # request of its window at once, so a smaller window keeps the tail latency down
 MIXED_KEYS = 1 << 20
@@ -1156,15 +1164,28 @@ def run_ours(args, world, rank, local):
     if world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0):
         t.close()
         del dbat
+        gc.collect()
         torch.cuda.empty_cache()
+
+    def section(key, fn, *a):
+        # a secondary section that fails is reported in its own key; the
+        # headline line above stands on its own
+        try:
+            line[key] = fn(*a)
+        except Exception as e:  # noqa: BLE001
+            import traceback
+
+            traceback.print_exc()
+            line[key] = {"error": f"{type(e).__name__}: {e}"}
+        gc.collect()
+        torch.cuda.empty_cache()
+
     if world == 1 and args.vocab_n > 0:
-        line["vocab"] = run_vocab(args, local, dev, hbm_peak, kpeak)
-        torch.cuda.empty_cache()
+        section("vocab", run_vocab, args, local, dev, hbm_peak, kpeak)
     if world == 1 and args.eth_accounts > 0:
-        line["batched"] = run_eth(args, local, dev)
-        torch.cuda.empty_cache()
+        section("batched", run_eth, args, local, dev)
     if world == 1 and args.req_tenants:
-        line["learned"] = run_requests(args, local, dev)
+        section("learned", run_requests, args, local, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if not (world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0)):

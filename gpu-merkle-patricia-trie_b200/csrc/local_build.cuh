@@ -19,7 +19,7 @@ constexpr int kLocalIpt = kLocalCap / kLocalThreads;
 constexpr int kLocalSegs = kLocalCap / 2;  // a segment has >= 2 items
 // resident CTAs per SM the register allocation is bounded for
 #ifndef GMPT_LOCAL_BUILD_CTAS
-#define GMPT_LOCAL_BUILD_CTAS 2
+#define GMPT_LOCAL_BUILD_CTAS 4
 #endif
 
 struct LocalSegs {

@@ -18,3 +18,41 @@ void shim_keccak256(const byte *in, std::size_t len, byte *out32) {
   std::memcpy(out32, st, 32);
 }
 }  // namespace CryptoPP
+
+// The reference's GPU MPT through its C++ class on the same batch, under the
+// insert + hash pairings the reference uses (values_hps pointing at the
+// values, as test/trie.cu:1207-1210 makes them); the root goes to out32.
+//   variant 0: puts_latching_with_valuehp + hash_onepass (keys walk), the
+//              pair test/trie.cu:1282-1293 times and test/trie.cu:1446-1451
+//              checks against the CPU MPT
+//   variant 1: puts_latching_with_valuehp_v2 + hash_onepass_v2, the pair
+//              insert_mpt_olc runs (lib/libgmpt.cu:299-303)
+//   variant 2: puts_2phase_with_valuehp + hash_onepass_v2
+// Returns the root's size (32, or 0 for no root); -1 for an unknown variant.
+extern "C" int ref_gpu_variant_root(int variant, const uint8_t *keys_hexs, int *keys_indexs,
+                                    const uint8_t *values, int64_t *values_indexs, int n, uint8_t *out32) {
+  if (variant < 0 || variant > 2) return -1;
+  GPUHashMultiThread::load_constants();
+  const uint8_t **hps = new const uint8_t *[n];
+  for (int i = 0; i < n; ++i) hps[i] = util::element_start(values_indexs, i, values);
+  int size = 0;
+  {
+    GpuMPT::Compress::MPT mpt;
+    if (variant == 0) {
+      mpt.puts_latching_with_valuehp(keys_hexs, keys_indexs, values, values_indexs, hps, n);
+      mpt.hash_onepass(keys_hexs, keys_indexs, n);
+    } else if (variant == 1) {
+      auto [nodes, cnt] = mpt.puts_latching_with_valuehp_v2(keys_hexs, keys_indexs, values, values_indexs, hps, n);
+      mpt.hash_onepass_v2(nodes, cnt);
+    } else {
+      auto [nodes, cnt] = mpt.puts_2phase_with_valuehp(keys_hexs, keys_indexs, values, values_indexs, hps, n);
+      mpt.hash_onepass_v2(nodes, cnt);
+    }
+    const uint8_t *h = nullptr;
+    mpt.get_root_hash(h, size);
+    if (h && size > 0) std::memcpy(out32, h, size < 32 ? size : 32);
+    delete[] h;
+  }
+  delete[] hps;
+  return size;
+}
