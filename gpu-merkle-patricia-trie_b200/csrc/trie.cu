@@ -27,8 +27,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHashThreads = kHashLevelThreads;
-constexpr int kMaxDepthBins = 2 * (kMaxKeyNibbles + 2);          // (depth, kind)
-constexpr int kHashBins = kMaxDepthBins * (int)kHashClasses;       // (depth, kind, hash class)
+constexpr uint32_t kMaxDepths = kMaxKeyNibbles + 2;  // nibble depths a dirty node can have
 // LockNU batches of at least this many keys drop repeated keys first
 constexpr int kDedupMinKeys = 1 << 16;
 
@@ -362,7 +361,7 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (e == cudaSuccess && hp) e = cudaMemcpyAsync(hp, b.values_hps, sizeof(uint64_t) * (size_t)n, kind, st_);
   if (e == cudaSuccess && tid) e = cudaMemcpyAsync(tid, b.trie_ids, sizeof(int) * (size_t)n, kind, st_);
   if (e == cudaSuccess) e = cudaMemsetAsync(karena + key_base + kbytes, 0, 64, st_);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 4, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_max, 0, 8, st_);
   if (e != cudaSuccess) return check_cuda(e, "stage copy");
   if ((e = cudaMemsetAsync(&ctr_->stream_terms, 0, 24, st_)) != cudaSuccess) return check_cuda(e, "stage reset");
   count_launch(), k_stage<<<std::min<unsigned>(blocks_for(n), 148 * 8), kThreads, 0, st_>>>(tv_, ki, vi, hp, n, key_base, val_base, vid_base, kbytes, vbytes,
@@ -370,11 +369,13 @@ int Trie::stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64
   if (kbytes > 0 && !b.raw_keys)  // expanded raw keys are well formed by construction
     count_launch(), k_stage_stream<<<std::min<unsigned>(blocks_for(kbytes / 8 + 1), 148 * 8), kThreads, 0, st_>>>(
         tv_, karena + key_base, kbytes);
-  e = cudaMemcpyAsync(h_small_, d_max, 4, cudaMemcpyDeviceToHost, st_);
+  e = cudaMemcpyAsync(h_small_, d_max, 8, cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctr_, ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, st_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
   if (e != cudaSuccess) return check_cuda(e, "stage");
   *maxlen = (uint32_t)(h_small_[0] & 0xFFFFFFFFu);
+  max_key_nibbles_ = std::max(max_key_nibbles_, *maxlen);
+  max_value_len_ = std::max(max_value_len_, (uint32_t)(h_small_[0] >> 32));
   if (b.raw_keys) {
     // nothing to check beyond k_raw_lens (errors come back with the counters)
   } else if (h_ctr_->noncontig) {
@@ -843,31 +844,50 @@ int Trie::put_2phase(const BatchIn &b) {
 
 // Counting sort of the nd dirty nodes by (depth, kind, hash class) into
 // ws_.sorted_dirty; off[b] .. off[b + 1] is bin b (dirty_bin).
-int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off) {
+int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off, uint32_t *depths_out) {
   cudaError_t e = cudaSuccess;
-  uint32_t *bins = wsp<uint32_t>(ws_.bins, kHashBins + 1, e);
-  uint32_t *cursor = wsp<uint32_t>(ws_.cursor, kHashBins + 1, e);
   uint32_t *sorted = wsp<uint32_t>(ws_.sorted_dirty, nd, e);
   uint8_t *cls = wsp<uint8_t>(ws_.dirty_cls, nd, e);
-  if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * (kHashBins + 1), st_);
   if (e != cudaSuccess) return check_cuda(e, "hash alloc");
-  int grid = std::min<int>(blocks_for(nd), 148 * 4);
-  count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * kHashBins, st_>>>(tv_, dirty_ref_, dirty_depth_,
-                                                                                      (int)nd, bins, kHashBins, cls);
-  std::vector<uint32_t> hb(kHashBins);
-  off.assign(kHashBins + 1, 0);
-  if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * kHashBins, cudaMemcpyDeviceToHost, st_)) !=
-          cudaSuccess ||
-      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
-    return check_cuda(e, "hash bins");
-  off[0] = 0;
-  for (int b = 0; b < kHashBins; ++b) off[b + 1] = off[b] + hb[b];
-  if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * kHashBins, cudaMemcpyHostToDevice, st_)) !=
+  // a leaf can take two or more Keccak blocks: order leaves by block count
+  const int leaf_classes = (uint64_t)max_value_len_ + max_key_nibbles_ / 2 + 8 > 135 ? 1 : 0;
+  // depth range: every dirty node lies on the path of a staged key; nodes
+  // deeper than that (keys that reached the trie another way) make the
+  // histogram run again over every depth
+  uint32_t depths = std::min<uint32_t>(max_key_nibbles_ + 2, kMaxDepths);
+  std::vector<uint32_t> hb;
+  uint32_t *bins = nullptr, *cursor = nullptr;
+  uint32_t nbins = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    nbins = depths * kBinsPerDepth;
+    bins = wsp<uint32_t>(ws_.bins, (size_t)nbins + 1, e);
+    cursor = wsp<uint32_t>(ws_.cursor, (size_t)nbins + 1, e);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * ((size_t)nbins + 1), st_);
+    const size_t smem = sizeof(uint32_t) * ((size_t)nbins + 1);
+    if (e == cudaSuccess && smem > 48 * 1024)
+      e = cudaFuncSetAttribute(k_dirty_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "hash bins alloc");
+    int grid = std::min<int>(blocks_for(nd), 148 * 4);
+    count_launch(), k_dirty_hist<<<grid, kThreads, smem, st_>>>(tv_, dirty_ref_, dirty_depth_, (int)nd, bins,
+                                                                  (int)nbins, depths, leaf_classes, cls);
+    hb.resize((size_t)nbins + 1);
+    if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * ((size_t)nbins + 1), cudaMemcpyDeviceToHost,
+                             st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "hash bins");
+    if (hb[nbins] == 0) break;
+    if (depths == kMaxDepths) return fail(E_INTERNAL, "dirty node deeper than any key");
+    depths = kMaxDepths;
+  }
+  off.assign((size_t)nbins + 1, 0);
+  for (uint32_t b = 0; b < nbins; ++b) off[b + 1] = off[b] + hb[b];
+  if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * nbins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
   count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(
                       dirty_ref_, dirty_depth_, cls, (int)nd, cursor, sorted, ctr_);
   *sorted_out = sorted;
+  *depths_out = depths;
   return OK;
 }
 
@@ -884,7 +904,8 @@ int Trie::bucket_and_hash() {
   if (nd == 0) return OK;
   uint32_t *sorted = nullptr;
   std::vector<uint32_t> off;
-  int rc = bucket_dirty(nd, &sorted, off);
+  uint32_t depths = 0;
+  int rc = bucket_dirty(nd, &sorted, off, &depths);
   if (rc) return rc;
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;
@@ -899,9 +920,9 @@ int Trie::bucket_and_hash() {
   }
   const size_t smem_warp = smem + 4 * kWarpMsgBytes;
   tv_.account = timing_ ? 1 : 0;  // per-node accounting atomics only when measuring
-  for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
-    const uint32_t C = kHashClasses;
-    uint32_t a = off[2 * d * C], m = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];
+  for (int d = (int)depths - 1; d >= 0; --d) {
+    const uint32_t B = kBinsPerDepth;
+    uint32_t a = off[d * B], m = off[d * B + kLeafClasses], z = off[(d + 1) * B];
     if (z == a) continue;
     ++levels;
     if (z - m > 0 && z - m <= (uint32_t)opt_warp_full_max_) {
@@ -1117,6 +1138,7 @@ int Trie::reset() {
   if (e != cudaSuccess) return check_cuda(e, "reset");
   n_full_ = n_short_ = n_value_ = 0;
   n_rec_ = key_used_ = val_used_ = 0;
+  max_key_nibbles_ = max_value_len_ = 0;
   fl_n_ = 0;
   empty_ = true;
   ++gen_;
@@ -1789,6 +1811,10 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   stats_.n_value = n_value_;
   stats_.last_dirty = (uint64_t)h->dirty[0] + h->dirty[1];
   stats_.last_hash_levels = (uint64_t)h->levels[0] + h->levels[1];
+  // deepest node the block touched (maxbin = 2 depth + kind + 1): keeps the
+  // hash bins' depth range of later single-trie passes above it
+  for (int s = 0; s < 2; ++s)
+    if (h->maxbin[s]) max_key_nibbles_ = std::max(max_key_nibbles_, (h->maxbin[s] - 1) / 2 + 1);
   if (b.n_out > 0) {
     std::vector<uint8_t> o(33 * (size_t)b.n_out);
     if ((e = cudaMemcpyAsync(o.data(), blk_.out.p, o.size(), cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
@@ -2060,10 +2086,11 @@ int Trie::del(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool devi
   if (nd == 0) return OK;
   uint32_t *sorted = nullptr;
   std::vector<uint32_t> off;
-  if ((rc = bucket_dirty(nd, &sorted, off))) return rc;
-  const uint32_t C = kHashClasses;
-  for (int d = kMaxDepthBins / 2 - 1; d >= 0; --d) {
-    const uint32_t a = off[(2 * d + 1) * C], z = off[(2 * d + 2) * C];  // branches at depth d
+  uint32_t depths = 0;
+  if ((rc = bucket_dirty(nd, &sorted, off, &depths))) return rc;
+  const uint32_t B = kBinsPerDepth;
+  for (int d = (int)depths - 1; d >= 0; --d) {
+    const uint32_t a = off[d * B + kLeafClasses], z = off[(d + 1) * B];  // branches at depth d
     if (z == a) continue;
     const int cnt = (int)(z - a);
     // room for this level's new keys and short nodes, then collapse

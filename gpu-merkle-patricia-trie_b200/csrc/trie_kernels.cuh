@@ -101,14 +101,14 @@ __device__ __forceinline__ uint32_t new_short(const TrieView &tv, DirtyList d, u
 // staging
 
 // Per-key records of a staged batch.  Grid-stride, with the stream counters
-// (terminated keys, index-pair gaps, longest key) reduced per CTA: one
-// atomic per CTA and counter instead of one per warp, which serialised on
-// the three counter addresses at 16M keys.
+// (terminated keys, index-pair gaps; maxlen[0] = longest key, maxlen[1] =
+// longest value) reduced per CTA: one atomic per CTA and counter instead of
+// one per warp, which serialised on the counter addresses at 16M keys.
 __global__ void __launch_bounds__(256) k_stage(TrieView tv, const int *ki, const int64_t *vi, const uint64_t *hp,
                                                int n, uint64_t key_base, uint64_t val_base, uint64_t vid_base,
                                                int64_t kbytes, int64_t vbytes, uint64_t *koff, uint32_t *klen,
                                                uint32_t *maxlen, const int *tid) {
-  uint32_t terms = 0, gaps = 0, lmax = 0;
+  uint32_t terms = 0, gaps = 0, lmax = 0, vmax = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (tid && (uint32_t)tid[i] >= tv.n_tries) set_error(tv.ctr, ERR_BAD_TRIE);
     int ks = ki[2 * i], ke = ki[2 * i + 1];
@@ -145,30 +145,35 @@ __global__ void __launch_bounds__(256) k_stage(TrieView tv, const int *ki, const
       ve = -1;
     }
     uint64_t vid = vid_base + (uint64_t)i;
+    vmax = max(vmax, (uint32_t)(ve - vs + 1));
     tv.rec[vid] = ValueRec{val_base + (uint64_t)vs, (uint32_t)(ve - vs + 1), 0u};
     tv.rec_hp[vid] = hp ? hp[i] : 0ull;
   }
-  __shared__ uint32_t red[3][8];
+  __shared__ uint32_t red[4][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   terms = __reduce_add_sync(0xffffffffu, terms);
   gaps = __reduce_or_sync(0xffffffffu, gaps);
   lmax = __reduce_max_sync(0xffffffffu, lmax);
+  vmax = __reduce_max_sync(0xffffffffu, vmax);
   if (lane == 0) {
     red[0][warp] = terms;
     red[1][warp] = gaps;
     red[2][warp] = lmax;
+    red[3][warp] = vmax;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint32_t t = 0, g = 0, m = 0;
+    uint32_t t = 0, g = 0, m = 0, v = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       t += red[0][w];
       g |= red[1][w];
       m = max(m, red[2][w]);
+      v = max(v, red[3][w]);
     }
     if (t) atomicAdd(&tv.ctr->key_terms, t);
     if (g) atomicOr(&tv.ctr->noncontig, 1u);
     if (m) atomicMax(maxlen, m);
+    if (v) atomicMax(maxlen + 1, v);  // longest value of the batch
   }
 }
 
@@ -924,26 +929,53 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   return blocks_class(bytes / 136u);
 }
 
-// bin of a dirty node: (nibble depth, kind, hash class); the class is
-// counted for branches only (one read of the child slots), leaves are
-// ordered inside each hashing CTA
-__device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
-  return (2u * depth + (ref_kind(r) == KIND_FULL ? 1u : 0u)) * kHashClasses + cls;
+// Exact Keccak block count of a leaf (short node over a value), minus one,
+// capped at kLeafClasses - 1.  With values of up to kilobytes (1 to 31
+// blocks) a level's leaves are ordered by it over the whole level, so a
+// warp's 32 leaves need the same number of permutations; ordering inside one
+// 128-node CTA alone left about half of the lanes idle.
+constexpr uint32_t kLeafClasses = 32;
+// bins per nibble depth: leaves/extensions by leaf class, then branches by
+// hash class; a level is one contiguous range of the sorted dirty list
+constexpr uint32_t kBinsPerDepth = kLeafClasses + kHashClasses;
+
+__device__ __forceinline__ uint32_t leaf_class(const TrieView &tv, uint32_t idx) {
+  if (tv.short_dead[idx]) return 0u;
+  const uint32_t ch = tv.short_child[idx];
+  if (ref_kind(ch) != KIND_VALUE) return 0u;
+  const uint32_t bytes = tv.short_klen[idx] / 2u + 8u + load_rec(tv, tv.value_vid[ref_idx(ch)]).len;
+  return min(bytes / 136u, kLeafClasses - 1u);
 }
 
+// bin of a dirty node: (nibble depth, kind, class)
+__device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
+  return depth * kBinsPerDepth + (ref_kind(r) == KIND_FULL ? kLeafClasses + cls : cls);
+}
+
+// Histogram of the dirty list over (depth, kind, class) for depths below
+// `depths` (nbins = depths * kBinsPerDepth; bins[nbins] counts nodes deeper
+// than that, which makes the host redo the histogram over every depth).
+// Leaves are classed only when `leaf_classes` is set (a batch held values
+// long enough for a leaf to take two or more Keccak blocks).
 __global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *depth, int n, uint32_t *bins,
-                             int nbins, uint8_t *cls) {
+                             int nbins, uint32_t depths, int leaf_classes, uint8_t *cls) {
   extern __shared__ uint32_t h[];
-  for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0;
+  for (int b = threadIdx.x; b <= nbins; b += blockDim.x) h[b] = 0;
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t r = ref[i];
-    const uint32_t c = ref_kind(r) == KIND_FULL ? full_class(tv, ref_idx(r)) : 0u;
+    const uint32_t r = ref[i], d = depth[i];
+    if (d >= depths) {
+      cls[i] = 0;
+      atomicAdd(&h[nbins], 1u);
+      continue;
+    }
+    const uint32_t c = ref_kind(r) == KIND_FULL ? full_class(tv, ref_idx(r))
+                                                : (leaf_classes ? leaf_class(tv, ref_idx(r)) : 0u);
     cls[i] = (uint8_t)c;
-    atomicAdd(&h[dirty_bin(depth[i], r, c)], 1u);
+    atomicAdd(&h[dirty_bin(d, r, c)], 1u);
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+  for (int b = threadIdx.x; b <= nbins; b += blockDim.x)
     if (h[b]) atomicAdd(&bins[b], h[b]);
 }
 
