@@ -844,50 +844,33 @@ int Trie::put_2phase(const BatchIn &b) {
 
 // Counting sort of the nd dirty nodes by (depth, kind, hash class) into
 // ws_.sorted_dirty; off[b] .. off[b + 1] is bin b (dirty_bin).
-int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off, uint32_t *depths_out) {
+int Trie::bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off) {
   cudaError_t e = cudaSuccess;
+  const uint32_t nbins = level_bin(kMaxDepths);
+  uint32_t *bins = wsp<uint32_t>(ws_.bins, nbins, e);
+  uint32_t *cursor = wsp<uint32_t>(ws_.cursor, nbins, e);
   uint32_t *sorted = wsp<uint32_t>(ws_.sorted_dirty, nd, e);
   uint8_t *cls = wsp<uint8_t>(ws_.dirty_cls, nd, e);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * nbins, st_);
   if (e != cudaSuccess) return check_cuda(e, "hash alloc");
   // a leaf can take two or more Keccak blocks: order leaves by block count
   const int leaf_classes = (uint64_t)max_value_len_ + max_key_nibbles_ / 2 + 8 > 135 ? 1 : 0;
-  // depth range: every dirty node lies on the path of a staged key; nodes
-  // deeper than that (keys that reached the trie another way) make the
-  // histogram run again over every depth
-  uint32_t depths = std::min<uint32_t>(max_key_nibbles_ + 2, kMaxDepths);
-  std::vector<uint32_t> hb;
-  uint32_t *bins = nullptr, *cursor = nullptr;
-  uint32_t nbins = 0;
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    nbins = depths * kBinsPerDepth;
-    bins = wsp<uint32_t>(ws_.bins, (size_t)nbins + 1, e);
-    cursor = wsp<uint32_t>(ws_.cursor, (size_t)nbins + 1, e);
-    if (e == cudaSuccess) e = cudaMemsetAsync(bins, 0, sizeof(uint32_t) * ((size_t)nbins + 1), st_);
-    const size_t smem = sizeof(uint32_t) * ((size_t)nbins + 1);
-    if (e == cudaSuccess && smem > 48 * 1024)
-      e = cudaFuncSetAttribute(k_dirty_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "hash bins alloc");
-    int grid = std::min<int>(blocks_for(nd), 148 * 4);
-    count_launch(), k_dirty_hist<<<grid, kThreads, smem, st_>>>(tv_, dirty_ref_, dirty_depth_, (int)nd, bins,
-                                                                  (int)nbins, depths, leaf_classes, cls);
-    hb.resize((size_t)nbins + 1);
-    if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * ((size_t)nbins + 1), cudaMemcpyDeviceToHost,
-                             st_)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
-      return check_cuda(e, "hash bins");
-    if (hb[nbins] == 0) break;
-    if (depths == kMaxDepths) return fail(E_INTERNAL, "dirty node deeper than any key");
-    depths = kMaxDepths;
-  }
+  int grid = std::min<int>(blocks_for(nd), 148 * 4);
+  count_launch(), k_dirty_hist<<<grid, kThreads, sizeof(uint32_t) * nbins, st_>>>(
+                      tv_, dirty_ref_, dirty_depth_, (int)nd, bins, (int)nbins, leaf_classes, cls);
+  std::vector<uint32_t> hb(nbins);
   off.assign((size_t)nbins + 1, 0);
-  for (uint32_t b = 0; b < nbins; ++b) off[b + 1] = off[b] + hb[b];
+  if ((e = cudaMemcpyAsync(hb.data(), bins, sizeof(uint32_t) * nbins, cudaMemcpyDeviceToHost, st_)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "hash bins");
+  for (uint32_t i = 0; i < nbins; ++i) off[i + 1] = off[i] + hb[i];
   if ((e = cudaMemcpyAsync(cursor, off.data(), sizeof(uint32_t) * nbins, cudaMemcpyHostToDevice, st_)) !=
       cudaSuccess)
     return check_cuda(e, "hash cursor");
   count_launch(), k_dirty_scatter<<<std::min<unsigned>(blocks_for(nd), 148 * 8), kThreads, 0, st_>>>(
                       dirty_ref_, dirty_depth_, cls, (int)nd, cursor, sorted, ctr_);
   *sorted_out = sorted;
-  *depths_out = depths;
   return OK;
 }
 
@@ -904,8 +887,7 @@ int Trie::bucket_and_hash() {
   if (nd == 0) return OK;
   uint32_t *sorted = nullptr;
   std::vector<uint32_t> off;
-  uint32_t depths = 0;
-  int rc = bucket_dirty(nd, &sorted, off, &depths);
+  int rc = bucket_dirty(nd, &sorted, off);
   if (rc) return rc;
   size_t smem = sizeof(uint64_t) * 17 * kHashThreads;
   int levels = 0;
@@ -920,9 +902,14 @@ int Trie::bucket_and_hash() {
   }
   const size_t smem_warp = smem + 4 * kWarpMsgBytes;
   tv_.account = timing_ ? 1 : 0;  // per-node accounting atomics only when measuring
-  for (int d = (int)depths - 1; d >= 0; --d) {
-    const uint32_t B = kBinsPerDepth;
-    uint32_t a = off[d * B], m = off[d * B + kLeafClasses], z = off[(d + 1) * B];
+  // every leaf first (one launch), then the levels deepest first
+  if (off[kLeafClasses] > 0) {
+    ++levels;
+    count_launch(), k_hash_level<<<blocks_for(off[kLeafClasses], kHashThreads), kHashThreads, smem, st_>>>(
+                        tv_, sorted, (int)off[kLeafClasses]);
+  }
+  for (int d = (int)kMaxDepths - 1; d >= 0; --d) {
+    uint32_t a = off[level_bin(d)], m = off[level_bin(d) + 1], z = off[level_bin(d + 1)];
     if (z == a) continue;
     ++levels;
     if (z - m > 0 && z - m <= (uint32_t)opt_warp_full_max_) {
@@ -1811,10 +1798,6 @@ int Trie::block_update(const BlockIn &b, uint8_t *out32, int *sizes) {
   stats_.n_value = n_value_;
   stats_.last_dirty = (uint64_t)h->dirty[0] + h->dirty[1];
   stats_.last_hash_levels = (uint64_t)h->levels[0] + h->levels[1];
-  // deepest node the block touched (maxbin = 2 depth + kind + 1): keeps the
-  // hash bins' depth range of later single-trie passes above it
-  for (int s = 0; s < 2; ++s)
-    if (h->maxbin[s]) max_key_nibbles_ = std::max(max_key_nibbles_, (h->maxbin[s] - 1) / 2 + 1);
   if (b.n_out > 0) {
     std::vector<uint8_t> o(33 * (size_t)b.n_out);
     if ((e = cudaMemcpyAsync(o.data(), blk_.out.p, o.size(), cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
@@ -2086,11 +2069,9 @@ int Trie::del(const uint8_t *keys_hexs, const int *keys_indexs, int n, bool devi
   if (nd == 0) return OK;
   uint32_t *sorted = nullptr;
   std::vector<uint32_t> off;
-  uint32_t depths = 0;
-  if ((rc = bucket_dirty(nd, &sorted, off, &depths))) return rc;
-  const uint32_t B = kBinsPerDepth;
-  for (int d = (int)depths - 1; d >= 0; --d) {
-    const uint32_t a = off[d * B + kLeafClasses], z = off[(d + 1) * B];  // branches at depth d
+  if ((rc = bucket_dirty(nd, &sorted, off))) return rc;
+  for (int d = (int)kMaxDepths - 1; d >= 0; --d) {
+    const uint32_t a = off[level_bin(d) + 1], z = off[level_bin(d + 1)];  // branches at depth d
     if (z == a) continue;
     const int cnt = (int)(z - a);
     // room for this level's new keys and short nodes, then collapse

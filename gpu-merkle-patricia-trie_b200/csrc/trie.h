@@ -196,8 +196,7 @@ class Trie {
   uint32_t n_full_ = 0, n_short_ = 0, n_value_ = 0;
   uint64_t n_rec_ = 0, key_used_ = 0, val_used_ = 0;
   // longest key (nibbles) and value (bytes) staged since the last reset:
-  // bound the depth range of the hash bins and decide whether leaves are
-  // ordered by Keccak block count
+  // whether the hash pass orders leaves by Keccak block count
   uint32_t max_key_nibbles_ = 0, max_value_len_ = 0;
   uint32_t *roots_ = nullptr;  // [n_tries_] root words
   uint32_t n_tries_ = 1;
@@ -288,7 +287,7 @@ class Trie {
                       uint64_t add_key_bytes, uint64_t add_val_bytes, bool exact = false);
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
-  int bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off, uint32_t *depths_out);
+  int bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off);
   int sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                  uint32_t **order_out, uint8_t **eqprev_out);
   int sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid, uint32_t **uord_out,

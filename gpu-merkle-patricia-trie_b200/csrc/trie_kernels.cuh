@@ -888,7 +888,8 @@ __global__ void k_level_scatter(const uint32_t *act, const uint32_t *aseg, const
 }
 
 // ---------------------------------------------------------------------------
-// PhaseHC: dirty nodes bucketed by (nibble depth, kind), deepest first
+// PhaseHC: dirty leaves first, then the other nodes bucketed by (nibble
+// depth, kind), deepest first
 
 // Keccak blocks a dirty node's encoding is expected to take, minus one,
 // capped at 3: a branch's children counted as 33-byte references, a leaf's
@@ -929,53 +930,60 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   return blocks_class(bytes / 136u);
 }
 
-// Exact Keccak block count of a leaf (short node over a value), minus one,
-// capped at kLeafClasses - 1.  With values of up to kilobytes (1 to 31
-// blocks) a level's leaves are ordered by it over the whole level, so a
-// warp's 32 leaves need the same number of permutations; ordering inside one
-// 128-node CTA alone left about half of the lanes idle.
+// Leaves (short nodes over a value) depend on nothing below them, so every
+// dirty leaf is hashed in one launch ahead of the levels, whatever its
+// depth; the levels then hold only branches and extensions.  Leaves are
+// ordered by their exact Keccak block count (minus one, capped at
+// kLeafClasses - 1) over the whole batch, so a warp's 32 leaves need the
+// same number of permutations.  Ordering inside one 128-node CTA alone left
+// about half of the lanes idle with values of up to kilobytes (1 to 31
+// blocks), and hashing leaves level by level made deep tries a chain of
+// small launches, each as long as its slowest leaf.
 constexpr uint32_t kLeafClasses = 32;
-// bins per nibble depth: leaves/extensions by leaf class, then branches by
-// hash class; a level is one contiguous range of the sorted dirty list
-constexpr uint32_t kBinsPerDepth = kLeafClasses + kHashClasses;
+// bins: the kLeafClasses leaf bins, then per nibble depth one bin of
+// extensions and kHashClasses bins of branches; a level is one contiguous
+// range of the sorted dirty list
+constexpr uint32_t kBinsPerDepth = 1 + kHashClasses;
+constexpr uint32_t kLeafBit = 0x80;  // class byte of a leaf
 
-__device__ __forceinline__ uint32_t leaf_class(const TrieView &tv, uint32_t idx) {
+__host__ __device__ __forceinline__ uint32_t level_bin(uint32_t depth) { return kLeafClasses + depth * kBinsPerDepth; }
+
+// class byte of a dirty node: kLeafBit | block class for a leaf, the hash
+// class for a branch, 0 for an extension (or a dead short node)
+__device__ __forceinline__ uint32_t dirty_class(const TrieView &tv, uint32_t r, bool leaf_classes) {
+  const uint32_t idx = ref_idx(r);
+  if (ref_kind(r) == KIND_FULL) return full_class(tv, idx);
   if (tv.short_dead[idx]) return 0u;
   const uint32_t ch = tv.short_child[idx];
   if (ref_kind(ch) != KIND_VALUE) return 0u;
+  if (!leaf_classes) return kLeafBit;
   const uint32_t bytes = tv.short_klen[idx] / 2u + 8u + load_rec(tv, tv.value_vid[ref_idx(ch)]).len;
-  return min(bytes / 136u, kLeafClasses - 1u);
+  return kLeafBit | min(bytes / 136u, kLeafClasses - 1u);
 }
 
-// bin of a dirty node: (nibble depth, kind, class)
+// bin of a dirty node from its depth, kind and class byte
 __device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
-  return depth * kBinsPerDepth + (ref_kind(r) == KIND_FULL ? kLeafClasses + cls : cls);
+  if (cls & kLeafBit) return cls & ~kLeafBit;
+  return level_bin(depth) + (ref_kind(r) == KIND_FULL ? 1u + cls : 0u);
 }
 
-// Histogram of the dirty list over (depth, kind, class) for depths below
-// `depths` (nbins = depths * kBinsPerDepth; bins[nbins] counts nodes deeper
-// than that, which makes the host redo the histogram over every depth).
-// Leaves are classed only when `leaf_classes` is set (a batch held values
-// long enough for a leaf to take two or more Keccak blocks).
+// Histogram of the dirty list over the bins (nbins of them, covering every
+// depth a node can have).  Leaves are classed by block count only when
+// `leaf_classes` is set (a batch held values long enough for a leaf to take
+// two or more Keccak blocks).
 __global__ void k_dirty_hist(TrieView tv, const uint32_t *ref, const uint16_t *depth, int n, uint32_t *bins,
-                             int nbins, uint32_t depths, int leaf_classes, uint8_t *cls) {
+                             int nbins, int leaf_classes, uint8_t *cls) {
   extern __shared__ uint32_t h[];
-  for (int b = threadIdx.x; b <= nbins; b += blockDim.x) h[b] = 0;
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0;
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t r = ref[i], d = depth[i];
-    if (d >= depths) {
-      cls[i] = 0;
-      atomicAdd(&h[nbins], 1u);
-      continue;
-    }
-    const uint32_t c = ref_kind(r) == KIND_FULL ? full_class(tv, ref_idx(r))
-                                                : (leaf_classes ? leaf_class(tv, ref_idx(r)) : 0u);
+    const uint32_t r = ref[i];
+    const uint32_t c = dirty_class(tv, r, leaf_classes != 0);
     cls[i] = (uint8_t)c;
-    atomicAdd(&h[dirty_bin(d, r, c)], 1u);
+    atomicAdd(&h[dirty_bin(depth[i], r, c)], 1u);
   }
   __syncthreads();
-  for (int b = threadIdx.x; b <= nbins; b += blockDim.x)
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
     if (h[b]) atomicAdd(&bins[b], h[b]);
 }
 

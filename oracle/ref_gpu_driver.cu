@@ -56,3 +56,16 @@ extern "C" int ref_gpu_variant_root(int variant, const uint8_t *keys_hexs, int *
   delete[] hps;
   return size;
 }
+
+// The reference's warp-cooperative GPU Keccak-256 (hash/gpu_hash_kernel.cuh
+// call_keccak_basic_kernel over hash/batch_mode_hash.cuh
+// batch_keccak_device: one state spread over 25 lanes in shared memory) on
+// one message; the digest goes to out32.  Messages whose length is a
+// multiple of 8 bytes only: the helper zeroes just the first bytes of its
+// last word (gpu_hash_kernel.cuh:198).
+extern "C" int ref_gpu_keccak(const uint8_t *in, uint32_t len, uint8_t *out32) {
+  if (len == 0 || (len & 7u)) return -1;
+  GPUHashMultiThread::load_constants();
+  GPUHashMultiThread::call_keccak_basic_kernel(in, len, out32);
+  return 0;
+}
