@@ -175,6 +175,23 @@ def regret(times_ms: np.ndarray, choice) -> float:
     return float(np.nansum(got) / np.nansum(best) - 1.0)
 
 
+def candidates(times_ms: np.ndarray, near: float = 1.05, share: float = 0.02) -> list:
+    """Configurations the network may pick: those within `near` of the
+    per-batch best on at least `share` of the measured batches (and at
+    least one).  A configuration that never came close in training has only
+    extrapolated predictions, and one low guess for it (a PhaseNU rebuild of
+    a large trie, say) costs several times the batch; leaving it out bounds
+    what a wrong pick can cost."""
+    t = np.asarray(times_ms, dtype=np.float64)
+    best = np.nanmin(t, 1, keepdims=True)
+    close = np.where(np.isnan(t), False, t <= near * best)
+    need = max(1, int(np.ceil(share * len(t))))
+    cols = [k for k in range(t.shape[1]) if close[:, k].sum() >= need]
+    if not cols:  # every configuration measured somewhere is a candidate
+        cols = [k for k in range(t.shape[1]) if np.any(~np.isnan(t[:, k]))]
+    return cols
+
+
 @dataclass
 class Selector:
     """MLP schedule selector with the autotuned rule as fallback and yardstick:
@@ -202,7 +219,7 @@ class Selector:
         self.lo, self.hi = x.min(0), x.max(0)
         z = ((x - self.mean) / self.std).astype(np.float32)
         t = np.asarray(times_ms, dtype=np.float64)
-        self.cols = [k for k in range(t.shape[1]) if np.any(~np.isnan(t[:, k]))]
+        self.cols = candidates(t)
         tgt, m = self._targets(t)
         return self.net.train(z, tgt, m, epochs=epochs, batch=batch, lr=lr, seed=seed)
 
