@@ -292,6 +292,21 @@ def run_reference_gpu(args, world, rank):
                                         P(c1.values), P(np.ascontiguousarray(c1.values_indexs, np.int64)), c1.n,
                                         P(out))
             variants[name] = out.tobytes().hex() if sz == 32 else f"size {sz}"
+    # the reference's GPU Keccak-256 alone on seeded messages, against the
+    # oracle's Keccak-256 (its digests decide every root it returns)
+    keccak_kat = []
+    if hasattr(L, "ref_gpu_keccak"):
+        sys.path.insert(0, str(REPO / "oracle"))
+        from oracle import keccak256
+
+        L.ref_gpu_keccak.restype = C.c_int
+        L.ref_gpu_keccak.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        rng = np.random.default_rng(0x5EED)
+        for ln in (8, 136, 512):
+            msg = rng.integers(0, 256, ln, dtype=np.uint8)
+            out = np.zeros(32, np.uint8)
+            L.ref_gpu_keccak(P(msg), ln, P(out))
+            keccak_kat.append({"bytes": ln, "agrees_with_keccak256": out.tobytes() == keccak256(msg.tobytes())})
     golden_path = REPO / "tests" / "golden" / "config_roots.json"
     cases = json.loads(golden_path.read_text())["cases"] if golden_path.exists() else {}
     gold = golden_roots(args.n)
@@ -310,7 +325,8 @@ def run_reference_gpu(args, world, rank):
                               "root": c1_root,
                               "root_matches_oracle": c1_root == cases.get("c1_random_1m", {}).get("roots", [""])[0],
                               "oracle_root": cases.get("c1_random_1m", {}).get("roots", [""])[0],
-                              "reference_class_paths": variants}}
+                              "reference_class_paths": variants},
+            "reference_gpu_keccak": keccak_kat}
     # the reference prints its roots and timings through C stdio: flush them
     # first so the JSON line stands on a line of its own
     C.CDLL(None).fflush(None)
