@@ -34,9 +34,10 @@ sys.path.insert(0, str(REPO / "gpu-merkle-patricia-trie_b200"))
 from gmpt import workloads as W  # noqa: E402
 
 PEAKS_FILE = REPO / "MEASURED_PEAKS.json"
-# DRAM bytes per hashed node of k_hash_level, from one ncu capture of the
-# largest level of a 1M-key YCSB load (276.7 MB over 701K nodes)
-HASH_TRAFFIC_B_PER_NODE = 394.7
+# DRAM bytes per hashed node of k_hash_level: ncu dram__bytes_read.sum +
+# dram__bytes_write.sum over every k_hash_level launch of one 1M-key YCSB
+# load + update step (786.9 MB) over the 2,519,879 nodes it hashed
+HASH_TRAFFIC_B_PER_NODE = 312.3
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -1148,8 +1149,8 @@ def run_ours(args, world, rank, local):
                      "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4),
                      "traffic": int(HASH_TRAFFIC_B_PER_NODE * nodes_per_launch),
-                     "traffic_source": "ncu dram__bytes_read+write per hashed node of the largest level of a "
-                                       "1M-key YCSB load, scaled by the hashed nodes per level of this run",
+                     "traffic_source": "ncu dram__bytes_read+write of every k_hash_level launch of a 1M-key "
+                                       "YCSB step per hashed node, times the hashed nodes per launch of this run",
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": int(alg_bytes_per_launch),
                      "avg_launch_us": round(avg_launch_s * 1e6, 2),

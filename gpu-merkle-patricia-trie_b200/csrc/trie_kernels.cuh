@@ -891,19 +891,27 @@ __global__ void k_level_scatter(const uint32_t *act, const uint32_t *aseg, const
 // PhaseHC: dirty leaves first, then the other nodes bucketed by (nibble
 // depth, kind), deepest first
 
-// Keccak blocks a dirty node's encoding is expected to take, minus one,
-// capped at 3: a branch's children counted as 33-byte references, a leaf's
-// value length read from its record.  k_hash_level orders each CTA's nodes by
-// it, so the lanes of a warp need the same number of permutations and none
-// idles through another's extra ones.
-constexpr uint32_t kHashClasses = 4;
+// Keccak blocks a dirty branch's encoding is expected to take, minus one,
+// capped at kHashClasses - 1: children counted as 33-byte references, and a
+// value in slot 16 (a key that ends at the branch) by its length, which can
+// be kilobytes.  Branches of a level are binned by it, and k_hash_level
+// orders each CTA's nodes by block class, so the lanes of a warp need the
+// same number of permutations and none idles through another's extra ones.
+constexpr uint32_t kHashClasses = 8;
 
-__device__ __forceinline__ uint32_t full_class(const TrieView &tv, uint32_t idx) {
+__device__ __forceinline__ uint32_t full_bytes(const TrieView &tv, uint32_t idx) {
   const uint32_t *c = tv.full_child + (size_t)idx * 17;
   uint32_t cnt = 0;
 #pragma unroll
-  for (int k = 0; k < 17; ++k) cnt += c[k] != 0u ? 1u : 0u;
-  return min((20u + 32u * cnt) / 136u, kHashClasses - 1u);
+  for (int k = 0; k < 16; ++k) cnt += c[k] != 0u ? 1u : 0u;
+  uint32_t bytes = 20u + 32u * cnt;
+  const uint32_t v = c[16];
+  if (ref_kind(v) == KIND_VALUE) bytes += 3u + load_rec(tv, tv.value_vid[ref_idx(v)]).len;
+  return bytes;
+}
+
+__device__ __forceinline__ uint32_t full_class(const TrieView &tv, uint32_t idx) {
+  return min(full_bytes(tv, idx) / 136u, kHashClasses - 1u);
 }
 
 // Finer classes for the order inside one hashing CTA (leaves with values of
@@ -920,7 +928,7 @@ __device__ __forceinline__ uint32_t hash_class(const TrieView &tv, uint32_t r) {
   const uint32_t kind = ref_kind(r), idx = ref_idx(r);
   uint32_t bytes;
   if (kind == KIND_FULL) {
-    return full_class(tv, idx);
+    return blocks_class(full_bytes(tv, idx) / 136u);
   } else {
     if (tv.short_dead[idx]) return 0u;
     const uint32_t ch = tv.short_child[idx];
