@@ -504,7 +504,9 @@ def run_vocab(args, local, dev, hbm_peak, perm_peak):
                       "hash_kernels_ms": round(info["t_hash_kernels_ms"], 3),
                       "keccak_int_frac": round(info["last_keccak_blocks"] / (info["t_hash_kernels_ms"] / 1e3) /
                                                perm_peak, 4),
-                      "permutations": int(info["last_keccak_blocks"]), "hashed_nodes": int(info["last_hashed"])}
+                      "permutations": int(info["last_keccak_blocks"]), "hashed_nodes": int(info["last_hashed"]),
+                      "phases_ms": {k: round(info[k], 3) for k in ("t_stage_ms", "t_sort_ms", "t_walk_ms", "t_build_ms",
+                                                                   "t_hash_ms")}}
     t.set_timing(False)
     t.close()
     golden = None
