@@ -1381,6 +1381,14 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
       pre_pending = true;
     }
     if (raw) break;
+    // a long body (a value of up to kilobytes) streams through many blocks:
+    // start the loads of the next two lines of it before the permutation,
+    // so they arrive while it runs (addresses stay inside the body)
+    if (cur.body && !cur.nib && off < cur.blen) {
+      const uint32_t rest = cur.blen - off - 1;
+      prefetch_l1(cur.body + off + min(128u, rest));
+      prefetch_l1(cur.body + off + min(256u, rest));
+    }
     sp.absorb();
     if (last) break;
   }
