@@ -1267,18 +1267,10 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
   bool raw = total < 32 && !force;
   Sponge sp;
   sp.reset(stage, stride);
-  // Three encoders fill the staged 136-byte block: (0) a short node of one
-  // block, (1) a regular branch, generated word by word, (2) any other
-  // node, streamed item by item.  They share one permutation site below,
-  // so the lanes of a warp that take different encoders still permute
-  // together (a warp would otherwise run each encoder's permutations in
-  // turn).
-  const int mode = (!full && total <= 135) ? 0 : (regular ? 1 : 2);
-  bool pending = false, done = false;
-  if (mode == 0) {
-    // place each segment's 8-byte chunks into the zeroed block with
-    // shared-memory OR, then pad (every leaf with a value up to ~100 bytes,
-    // every extension)
+  if (!full && total <= 135) {
+    // One-block short node (every leaf with a value up to ~100 bytes, every
+    // extension): place each segment's 8-byte chunks into the zeroed block
+    // with shared-memory OR, pad, and permute once.
     uint64_t *st = sp.stage;
     const uint32_t S = sp.stride;
 #pragma unroll
@@ -1303,25 +1295,20 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
     if (!raw) {
       or_bytes(st, S, 0x01, 1, p);
       st[16 * S] |= 0x8000000000000000ull;
-      sp.w = 17;
-      pending = true;
+#pragma unroll
+      for (int w = 0; w < 17; ++w) sp.a[w] = st[w * S];
+      keccak_f1600(sp.a);
     }
-    done = true;
-  }
+  } else if (regular) {
   // regular branch: pending message bytes (little-endian), next slot, words
   // left of the current child's hash
   uint64_t buf = hdr;
   uint32_t nb = hn, slot = 0, hj = 8;
   const uint32_t *hw = nullptr;
-  // streamed node: current item, offset in its body
-  int item = 0;
-  EncItem cur{hdr, hn, 0, nullptr, 0};
-  uint32_t off = 0;
-  bool pre_pending = true;
+  bool last = false;
   while (true) {
-    if (mode == 1 && !done) {
-      // one block: 0x80 per empty slot, 0xa0 + 32 hash bytes per child,
-      // then the Keccak padding (rlp.cuh:132-155, node.cuh:46-112)
+    {  // one block: 0x80 per empty slot, 0xa0 + 32 hash bytes per child, then
+       // the Keccak padding (rlp.cuh:132-155, node.cuh:46-112)
       uint64_t *st = sp.stage;
       const uint32_t S = sp.stride;
       for (int w = 0; w < 17; ++w) {
@@ -1345,10 +1332,10 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
               }
               nb += 1;
               ++slot;
-            } else if (slot == 17) {
+            } else if (!last) {
               buf |= 0x01ull << (8 * nb);  // Keccak padding starts here
               nb += 1;
-              ++slot;
+              last = true;
             } else {
               nb = 4;  // zeros to the end of the block
             }
@@ -1359,53 +1346,52 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
         }
         st[w * S] = word;
       }
-      // the padding byte leaves buf in the half-word it joins, so the block
-      // that received it is the last one
-      const bool last = slot == 18;
       if (last) st[16 * S] |= 0x8000000000000000ull;
-      sp.w = 17;
-      pending = true;
-      done = last;
-    } else if (mode == 2 && !done) {
-      bool last = false;
-      while (!sp.full()) {
-        if (pre_pending) {
-          pre_pending = false;
-          if (cur.pren) sp.push(cur.pre, cur.pren);
-          continue;
-        }
-        if (off < cur.blen) {
-          uint32_t n8 = min(8u, cur.blen - off);
-          uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : ld8<kCoh>(cur.body + off);
-          sp.push(v & low_bytes_mask(n8), n8);
-          off += n8;
-          continue;
-        }
-        if (++item == nitems) {
-          sp.pad();
-          last = true;
-          break;
-        }
-        cur = node_item<kCoh>(tv, full, idx, item, payload);
-        off = 0;
-        pre_pending = true;
-      }
-      done = last || raw;
-      pending = !raw;
-      // a long body (a value of up to kilobytes) streams through many
-      // blocks: start the loads of the next two lines of it before the
-      // permutation, so they arrive while it runs (addresses stay inside)
-      if (!done && cur.body && !cur.nib && off < cur.blen) {
-        const uint32_t rest = cur.blen - off - 1;
-        prefetch_l1(cur.body + off + min(128u, rest));
-        prefetch_l1(cur.body + off + min(256u, rest));
-      }
     }
-    if (pending) {  // the one permutation site
-      sp.absorb();
-      pending = false;
+    sp.absorb();
+    if (last) break;
+  }
+  } else {
+  // pass 2: stream
+  int item = 0;
+  EncItem cur{hdr, hn, 0, nullptr, 0};
+  uint32_t off = 0;
+  bool pre_pending = true, last = false;
+  while (true) {
+    while (!sp.full()) {
+      if (pre_pending) {
+        pre_pending = false;
+        if (cur.pren) sp.push(cur.pre, cur.pren);
+        continue;
+      }
+      if (off < cur.blen) {
+        uint32_t nb = min(8u, cur.blen - off);
+        uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : ld8<kCoh>(cur.body + off);
+        sp.push(v & low_bytes_mask(nb), nb);
+        off += nb;
+        continue;
+      }
+      if (++item == nitems) {
+        sp.pad();
+        last = true;
+        break;
+      }
+      cur = node_item<kCoh>(tv, full, idx, item, payload);
+      off = 0;
+      pre_pending = true;
     }
-    if (done) break;
+    if (raw) break;
+    // a long body (a value of up to kilobytes) streams through many blocks:
+    // start the loads of the next two lines of it before the permutation,
+    // so they arrive while it runs (addresses stay inside the body)
+    if (cur.body && !cur.nib && off < cur.blen) {
+      const uint32_t rest = cur.blen - off - 1;
+      prefetch_l1(cur.body + off + min(128u, rest));
+      prefetch_l1(cur.body + off + min(256u, rest));
+    }
+    sp.absorb();
+    if (last) break;
+  }
   }
   if (tv.account) {  // accounting (timing mode): encoding bytes and absorbed blocks of this pass
     unsigned am = __activemask();
