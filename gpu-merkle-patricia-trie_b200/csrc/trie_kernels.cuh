@@ -1238,6 +1238,10 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
       EncItem it = child_item<kCoh>(tv, ch[k]);
       payload += it.pren + it.blen;
       const uint32_t kd = ref_kind(ch[k]);
+      if (kd == KIND_VALUE) {  // a key ending here: its value (up to kilobytes) closes the encoding
+        prefetch_l1(it.body);
+        if (it.blen > 120) prefetch_l1(it.body + 128);
+      }
       if (kd != KIND_NULL) {
         present |= 1u << k;
         regular = regular && k < 16 && kd != KIND_VALUE && it.blen == 32 && it.pren == 1;
