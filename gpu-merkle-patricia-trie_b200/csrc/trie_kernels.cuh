@@ -1369,6 +1369,26 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
         continue;
       }
       if (off < cur.blen) {
+        const uint32_t room = 17u - sp.w;  // whole words left in this block
+        if (!cur.nib && cur.blen - off >= 8u * room) {
+          // the item (a long value) covers the rest of the block: whole
+          // words straight from memory, the loads independent of each other
+          // (the partial word carried in acc keeps its length)
+          const uint8_t *src = cur.body + off;
+          const uint32_t ca = 8u * sp.accn;
+#pragma unroll 4
+          for (uint32_t i = 0; i < room; ++i) {
+            const uint64_t x = ld8<kCoh>(src + 8u * i);
+            if (ca == 0) {
+              sp.emit(x);
+            } else {
+              sp.emit(sp.acc | (x << ca));
+              sp.acc = x >> (64u - ca);
+            }
+          }
+          off += 8u * room;
+          continue;
+        }
         uint32_t nb = min(8u, cur.blen - off);
         uint64_t v = cur.nib ? pack_pairs8(cur.body + 2 * off) : ld8<kCoh>(cur.body + off);
         sp.push(v & low_bytes_mask(nb), nb);
