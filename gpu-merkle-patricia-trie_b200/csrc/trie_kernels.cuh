@@ -969,10 +969,12 @@ __device__ __forceinline__ uint32_t dirty_class(const TrieView &tv, uint32_t r, 
   return kLeafBit | min(bytes / 136u, kLeafClasses - 1u);
 }
 
-// bin of a dirty node from its depth, kind and class byte
+// bin of a dirty node from its depth, kind and class byte; inside a launch
+// the classes run longest first, so the CTAs of the slowest nodes start in
+// the first wave instead of forming the last one
 __device__ __forceinline__ uint32_t dirty_bin(uint32_t depth, uint32_t r, uint32_t cls) {
-  if (cls & kLeafBit) return cls & ~kLeafBit;
-  return level_bin(depth) + (ref_kind(r) == KIND_FULL ? 1u + cls : 0u);
+  if (cls & kLeafBit) return kLeafClasses - 1u - (cls & ~kLeafBit);
+  return level_bin(depth) + (ref_kind(r) == KIND_FULL ? kHashClasses - cls : 0u);
 }
 
 // Histogram of the dirty list over the bins (nbins of them, covering every
