@@ -115,7 +115,7 @@ __device__ __forceinline__ void cta_radix_pass(LocalSortSmem &L, int src, int m,
 __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, const uint32_t *seg_start,
                                                                   const uint32_t *seg_end, int c0, uint32_t *order,
                                                                   uint8_t *eqprev, const uint64_t *koff,
-                                                                  const uint32_t *klen) {
+                                                                  const uint32_t *klen, const uint32_t *term_len) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   LocalSortSmem &L = *reinterpret_cast<LocalSortSmem *>(smem_raw);
   const uint32_t a = seg_start[blockIdx.x];
@@ -158,6 +158,17 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     uint32_t ngroups;
     uint32_t rank = cta_excl_scan(starts, L.warp_tmp, ngroups);
     if (ngroups == (uint32_t)m) break;  // every key distinct
+    if (c > c0 && term_len) {
+      // every item still tied is a terminated key with no nibble left
+      // (k_term_len): the ties are repeats of one key, final as they stand
+      int live = 0;
+#pragma unroll
+      for (int r = 0; r < ipt; ++r) {
+        const int k = threadIdx.x * ipt + r;
+        if (k < m && (tp[r] || tp[r + 1]) && term_len[L.val[src][k]] > 8u * (uint32_t)c) live = 1;
+      }
+      if (!__syncthreads_or(live)) break;
+    }
     // build (rank, chunk) keys in the current order
     if (threadIdx.x == 0) {
       L.mask = 0;

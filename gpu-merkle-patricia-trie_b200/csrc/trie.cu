@@ -410,13 +410,19 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
   unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
   if (e != cudaSuccess) return check_cuda(e, "sort alloc");
+  uint32_t *term_len = wsp<uint32_t>(ws_.term_len, (size_t)n, e);
+  if (e != cudaSuccess) return check_cuda(e, "sort alloc");
   count_launch(), k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
+  count_launch(), k_term_len<<<blocks_for(n), kThreads, 0, st_>>>(tv_.keys, koff, klen, n, term_len);
   int nchunks = (int)((maxlen + 7) / 8);
   stats_.sort_passes = 0;
   // forest batches: a first pass orders by trie id
   for (int c = tid ? -1 : 0; c <= nchunks; ++c) {
     int cc = (c == nchunks) ? -1 : (c < 0 ? -2 : c);  // final pass: key length
-    count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
+    // from chunk 1 on, runs of one terminated key repeated drop out (their
+    // order is final); the length pass sees only keys without a terminator
+    count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, order, c > 0 ? term_len : nullptr,
+                                                                       8u * (uint32_t)(c > 0 ? c : 0), n, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
@@ -443,7 +449,8 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
         if ((e = cudaFuncSetAttribute(k_local_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
           return check_cuda(e, "local sort attr");
-        count_launch(), k_local_sort<<<S, kSortLocalThreads, smem, st_>>>(tv_, rs, re, c, order, eqprev, koff, klen);
+        count_launch(), k_local_sort<<<S, kSortLocalThreads, smem, st_>>>(tv_, rs, re, c, order, eqprev, koff, klen,
+                                                                            term_len);
         if ((e = cudaGetLastError()) != cudaSuccess) return check_cuda(e, "local sort");
         break;
       }
