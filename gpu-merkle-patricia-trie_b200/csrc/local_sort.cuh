@@ -158,14 +158,18 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     uint32_t ngroups;
     uint32_t rank = cta_excl_scan(starts, L.warp_tmp, ngroups);
     if (ngroups == (uint32_t)m) break;  // every key distinct
-    if (c > c0 && term_len) {
-      // every item still tied is a terminated key with no nibble left
-      // (k_term_len): the ties are repeats of one key, final as they stand
+    if (c > c0) {
+      // every tie left is between repeats of one key (k_term_len: both
+      // terminated, ended before this chunk, same length): the order is
+      // final, and the remaining chunks would only compare zeros
       int live = 0;
 #pragma unroll
       for (int r = 0; r < ipt; ++r) {
         const int k = threadIdx.x * ipt + r;
-        if (k < m && (tp[r] || tp[r + 1]) && term_len[L.val[src][k]] > 8u * (uint32_t)c) live = 1;
+        if (k < m && tp[r]) {
+          const uint32_t a = term_len[L.val[src][k - 1]], b = term_len[L.val[src][k]];
+          if (!(b == a && b <= 8u * (uint32_t)c)) live = 1;
+        }
       }
       if (!__syncthreads_or(live)) break;
     }

@@ -419,10 +419,7 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
   // forest batches: a first pass orders by trie id
   for (int c = tid ? -1 : 0; c <= nchunks; ++c) {
     int cc = (c == nchunks) ? -1 : (c < 0 ? -2 : c);  // final pass: key length
-    // from chunk 1 on, runs of one terminated key repeated drop out (their
-    // order is final); the length pass sees only keys without a terminator
-    count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, order, c > 0 ? term_len : nullptr,
-                                                                       8u * (uint32_t)(c > 0 ? c : 0), n, flags);
+    count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_small_, d_tot, 8, cudaMemcpyDeviceToHost, st_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st_);

@@ -268,9 +268,11 @@ __device__ __forceinline__ uint32_t key_chunk(const uint8_t *keys, uint64_t off,
 }
 
 // Nibbles of a terminated key (last nibble 16), else 0xFFFFFFFF.  Staging
-// admits the terminator only as a key's last nibble, so a terminated key
-// that is still tied with others after every nibble it has is tied with
-// repeats of itself: no later chunk pass can reorder its run.
+// admits the terminator only as a key's last nibble, and chunks compare
+// nibbles 0..15 exactly, so two chunk-equal neighbours that are terminated
+// keys of the same length, both ended, are the same key (a terminator packs
+// like nibble 0, so keys of different lengths can still tie on every chunk
+// and are told apart by the length pass).
 __global__ void k_term_len(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, int n,
                            uint32_t *term_len) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -279,16 +281,12 @@ __global__ void k_term_len(const uint8_t *keys, const uint64_t *koff, const uint
   term_len[i] = (len > 0 && keys[koff[i] + len - 1] == 16) ? len : 0xFFFFFFFFu;
 }
 
-// active = tied with a neighbour (and, when term_len is given, not a
-// terminated key of at most `ended` nibbles: its run is one key repeated);
-// packed: low = active, high = segment start
-__global__ void k_sort_flags(const uint8_t *eqprev, const uint32_t *order, const uint32_t *term_len,
-                             uint32_t ended, int n, unsigned long long *flags) {
+// active = tied with a neighbour; packed: low = active, high = segment start
+__global__ void k_sort_flags(const uint8_t *eqprev, int n, unsigned long long *flags) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   uint32_t tl = eqprev[p], tr = eqprev[p + 1];
   uint32_t active = (tl | tr) ? 1u : 0u;
-  if (active && term_len && term_len[order[p]] <= ended) active = 0;
   uint32_t start = (active && !tl) ? 1u : 0u;
   flags[p] = (unsigned long long)active | ((unsigned long long)start << 32);
 }
