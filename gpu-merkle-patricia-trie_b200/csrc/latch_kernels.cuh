@@ -463,6 +463,28 @@ __global__ void k_rw_slots(TrieView tv, const uint64_t *koff, const uint32_t *kl
   sval[i] = (uint32_t)i;
 }
 
+// Repeated keys in an evenly spaced sample of a batch (key hashes in a small
+// open-addressing table of tmask + 1 slots): PhaseNU drops a batch's repeats
+// before sorting when the sample shows many (runs of one key repeated
+// thousands of times otherwise keep the chunked sort going to the last
+// chunk).
+__global__ void k_dup_sample(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, const int *tid,
+                             int samples, int stride, unsigned long long *table, uint32_t tmask, uint32_t *dups) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= samples) return;
+  const int i = j * stride;
+  const unsigned long long h = dedup_hash(keys + koff[i], klen[i], tid ? (uint32_t)tid[i] : 0u, ~0ull);
+  uint32_t s = (uint32_t)(h ^ (h >> 32)) & tmask;
+  for (uint32_t probe = 0; probe <= tmask; ++probe, s = (s + 1) & tmask) {
+    const unsigned long long old = atomicCAS(&table[s], kDedupEmpty, h);
+    if (old == kDedupEmpty) return;
+    if (old == h) {
+      atomicAdd(dups, 1u);
+      return;
+    }
+  }
+}
+
 __global__ void k_dedup_compact(const unsigned long long *keep, const unsigned long long *pos, int n, uint32_t *sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && keep[i]) sel[pos[i]] = (uint32_t)i;

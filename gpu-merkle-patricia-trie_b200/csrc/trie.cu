@@ -470,6 +470,11 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
 int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                       uint32_t **uord_out, int *m_out) {
   if (rw_) return sort_rw(n, koff, klen, maxlen, tid, uord_out, m_out);
+  if (opt_sort_dedup_ && n >= kDedupMinKeys) {
+    bool done = false;
+    int rc = sort_unique_dedup(n, koff, klen, maxlen, tid, uord_out, m_out, &done);
+    if (rc || done) return rc;
+  }
   uint32_t *order;
   uint8_t *eqprev;
   int rc = sort_batch(n, koff, klen, maxlen, tid, &order, &eqprev);
@@ -491,6 +496,76 @@ int Trie::sort_unique(int n, const uint64_t *koff, const uint32_t *klen, uint32_
   return OK;
 }
 
+
+// PhaseNU with repeated keys: keep each key's last occurrence (the LockNU
+// repeat table, k_dedup_*), then sort only the distinct keys.  Runs of one
+// key repeated never untie in the chunked sort, so a batch with many
+// repeats would run it to the last chunk of its longest key; distinct keys
+// leave it after a few chunks.  Taken when an evenly spaced sample of 2^16
+// keys holds more than 1 % repeats (or always, sort_dedup = 2); *done stays
+// false (the caller sorts the whole batch) when it is not taken or when two
+// different keys share a 64-bit hash.
+int Trie::sort_unique_dedup(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                            uint32_t **uord_out, int *m_out, bool *done) {
+  cudaError_t e = cudaSuccess;
+  *done = false;
+  if (opt_sort_dedup_ == 1) {
+    const int samples = std::min(n, 1 << 16);
+    const uint32_t tsize = 1u << 17;
+    unsigned long long *table = wsp<unsigned long long>(ws_.dd_hash, tsize, e);
+    uint32_t *dups = reinterpret_cast<uint32_t *>(wsp<unsigned long long>(ws_.misc, 16, e) + 2);
+    if (e == cudaSuccess) e = cudaMemsetAsync(table, 0, sizeof(unsigned long long) * tsize, st_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dups, 0, 4, st_);
+    if (e != cudaSuccess) return check_cuda(e, "repeat sample alloc");
+    count_launch(), k_dup_sample<<<blocks_for(samples), kThreads, 0, st_>>>(tv_.keys, koff, klen, tid, samples,
+                                                                              n / samples, table, tsize - 1, dups);
+    if ((e = cudaMemcpyAsync(h_small_, dups, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+      return check_cuda(e, "repeat sample");
+    if ((uint64_t)(h_small_[0] & 0xFFFFFFFFu) * 100 <= (uint64_t)samples) return OK;
+  }
+  uint64_t size = 1024;
+  while (size < 2ull * (uint64_t)n) size <<= 1;
+  unsigned long long *table = wsp<unsigned long long>(ws_.dd_hash, 2 * size, e);
+  uint32_t *sel = wsp<uint32_t>(ws_.dd_sel, (size_t)n, e);
+  unsigned long long *keep = wsp<unsigned long long>(ws_.flags, (size_t)n, e);
+  unsigned long long *rank = wsp<unsigned long long>(ws_.pos, (size_t)n, e);
+  unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
+  uint32_t *collision = reinterpret_cast<uint32_t *>(d_tot + 1);
+  uint32_t *slot_of = wsp<uint32_t>(ws_.dd_slot, (size_t)n, e);
+  if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
+  if (e == cudaSuccess) e = cudaMemsetAsync(table, 0, 2 * sizeof(unsigned long long) * size, st_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(collision, 0, 4, st_);
+  if (e != cudaSuccess) return check_cuda(e, "repeat table alloc");
+  const uint64_t hmask = opt_dedup_bits_ >= 64 ? ~0ull : ((1ull << opt_dedup_bits_) - 1);
+  DedupTable tab{table, size - 1, hmask};
+  count_launch(), k_dedup_insert<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, slot_of);
+  count_launch(), k_dedup_mark<<<blocks_for(n), kThreads, 0, st_>>>(tv_, koff, klen, tid, n, tab, slot_of, keep,
+                                                                    collision);
+  if ((e = exclusive_scan<unsigned long long>(keep, rank, n, d_tot, scan_ws_, st_)) != cudaSuccess)
+    return check_cuda(e, "repeat scan");
+  count_launch(), k_dedup_compact<<<blocks_for(n), kThreads, 0, st_>>>(keep, rank, n, sel);
+  if ((e = cudaMemcpyAsync(h_small_, d_tot, 16, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+    return check_cuda(e, "repeat count");
+  if (h_small_[1] & 0xFFFFFFFFu) return OK;  // a hash shared by two keys: sort the whole batch
+  const int m = (int)(h_small_[0] & 0xFFFFFFFFu);
+  uint64_t *koff2 = wsp<uint64_t>(ws_.rw_koff, (size_t)m, e);
+  uint32_t *klen2 = wsp<uint32_t>(ws_.rw_klen, (size_t)m, e);
+  int *tid2 = tid ? wsp<int>(ws_.rw_tid, (size_t)m, e) : nullptr;
+  uint32_t *uord = wsp<uint32_t>(ws_.uord, (size_t)m, e);
+  if (e != cudaSuccess) return check_cuda(e, "repeat gather alloc");
+  count_launch(), k_rw_gather<<<blocks_for(m), kThreads, 0, st_>>>(sel, m, koff, klen, tid, koff2, klen2, tid2);
+  uint32_t *order2;
+  uint8_t *eqprev2;
+  int rc = sort_batch(m, koff2, klen2, maxlen, tid2, &order2, &eqprev2);
+  if (rc) return rc;
+  count_launch(), k_rw_map<<<blocks_for(m), kThreads, 0, st_>>>(order2, sel, m, uord);
+  *uord_out = uord;
+  *m_out = m;
+  *done = true;
+  return OK;
+}
 
 // Mixed read/write batch: group equal keys in batch order (hash-table slots
 // + a stable radix sort of the slots; full-key sort if two keys share a
@@ -1525,6 +1600,11 @@ int Trie::set_option(const std::string &name, int64_t value) {
   if (name == "latch_dedup") {
     if (value < 0 || value > 2) return fail(E_ARG, "latch_dedup must be 0, 1 or 2");
     opt_latch_dedup_ = (int)value;
+    return OK;
+  }
+  if (name == "sort_dedup") {
+    if (value < 0 || value > 2) return fail(E_ARG, "sort_dedup must be 0, 1 or 2");
+    opt_sort_dedup_ = (int)value;
     return OK;
   }
   if (name == "latch_dedup_bits") {

@@ -180,6 +180,7 @@ class Trie {
   bool opt_local_sort_ = true;   // finish small tied sort runs in one CTA each
   int opt_latch_ways_ = 4;       // LockNU keys per thread (1, 2, 4)
   int opt_latch_dedup_ = 1;      // 0 off, 1 batches >= kDedupMinKeys, 2 always
+  int opt_sort_dedup_ = 1;       // PhaseNU drops repeats first: 0 never, 1 when a sample shows them, 2 always
   int opt_dedup_bits_ = 64;      // hash bits the dedup keeps (fewer only to test collisions)
   int opt_warp_full_max_ = 4096; // hash levels with at most this many branches: a warp per branch
   int opt_local_build_cap_ = 0;  // largest segment finished in one CTA (0 = the kernel's capacity)
@@ -289,6 +290,8 @@ class Trie {
   int stage(const BatchIn &b, uint64_t &key_base, uint64_t &vid_base, uint64_t **koff, uint32_t **klen,
             uint32_t *maxlen, const int **tid);
   int bucket_dirty(uint32_t nd, uint32_t **sorted_out, std::vector<uint32_t> &off);
+  int sort_unique_dedup(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
+                        uint32_t **uord_out, int *m_out, bool *done);
   int sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid,
                  uint32_t **order_out, uint8_t **eqprev_out);
   int sort_rw(int n, const uint64_t *koff, const uint32_t *klen, uint32_t maxlen, const int *tid, uint32_t **uord_out,

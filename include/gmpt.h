@@ -360,6 +360,10 @@ int gmpt_flush_dirty(gmpt_trie *t, const uint8_t **hashs, const uint8_t **encs,
  *                      more loads in flight; 1: more threads for small batches);
  *   "latch_dedup" 0/1/2: LockNU drops repeated keys of a batch before the
  *                      walk: never / batches of >= 64K keys (default) / always;
+ *   "sort_dedup"  0/1/2: PhaseNU drops repeated keys of a batch (keeping the
+ *                      last) before sorting: never / batches of >= 64K keys
+ *                      whose 64K-key sample holds more than 1 % repeats
+ *                      (default) / always;
  *   "warp_full_max" N: PhaseHC hashes a level's branches one warp each when
  *                      the level has at most N branches (default 4096);
  *   "block_grid"  N:   CTAs of the persistent block kernel (0 = one per SM,

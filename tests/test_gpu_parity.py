@@ -346,3 +346,38 @@ def test_pipelined_host_batches(gpu_lib, strategies):
     h, sizes = t.gets_parallel(last.keys_hexs, last.keys_indexs)
     # a key's echoed pointer is the one given with the last batch position that wrote it
     assert np.all(sizes > 0) and np.all(h >= 1000)
+
+
+@pytest.mark.parametrize("mode,bits", [(0, 64), (1, 64), (2, 64), (2, 3)])
+def test_phasenu_repeat_filter_does_not_change_results(gpu_lib, mode, bits):
+    # PhaseNU batches heavy with repeated keys (70000 zipf updates of 20000
+    # keys: the 1 % sample trigger fires), with the repeat filter off,
+    # sampled, forced, and forced with a 3-bit hash (different keys share
+    # hashes: the sort must fall back to the whole batch); then a forest
+    load = W.ycsb_load(20000, seed=91)
+    upd = [W.ycsb_zipf_updates(20000, 70000, theta=1.1, seed=92 + k) for k in range(2)]
+    roots, o = oracle_root([load] + upd)
+    t = gpu_lib.MPT()
+    t.set_option("sort_dedup", mode)
+    t.set_option("latch_dedup_bits", bits)
+    for b, r in zip([load] + upd, roots):
+        t.puts_2phase_with_valuehp(b.keys_hexs, b.keys_indexs, b.values, b.values_indexs)
+        t.hash_onepass_v2()
+        assert t.get_root_hash() == r
+    u = upd[-1]
+    assert t.get_values(u.keys_hexs, u.keys_indexs) == o.gets(u.keys_hexs, u.keys_indexs)
+    f = gpu_lib.MPT(max_tries=2)
+    f.set_option("sort_dedup", mode)
+    f.set_option("latch_dedup_bits", bits)
+    b = upd[0]
+    tids = (np.arange(b.n) % 2).astype(np.int32)
+    f.puts_forest(True, b.keys_hexs, b.keys_indexs, b.values, b.values_indexs, tids)
+    f.hash_onepass_v2()
+    want = []
+    for tr in (0, 1):
+        ot = O.OracleTrie()
+        sub = b.subset(np.nonzero(tids == tr)[0])
+        ot.puts(sub.keys_hexs, sub.keys_indexs, sub.values, sub.values_indexs)
+        ot.hash()
+        want.append(ot.root())
+    assert f.get_roots(n=2) == want
