@@ -27,6 +27,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHashThreads = kHashLevelThreads;
+// k_hash_level_wide (132 registers: three CTAs per SM) for launches that
+// cannot place more than three CTAs on each of B200's 148 SMs anyway
+constexpr unsigned kWideGrid = 3 * 148;
 constexpr uint32_t kMaxDepths = kMaxKeyNibbles + 2;  // nibble depths a dirty node can have
 // LockNU batches of at least this many keys drop repeated keys first
 constexpr int kDedupMinKeys = 1 << 16;
@@ -981,11 +984,20 @@ int Trie::bucket_and_hash() {
   }
   const size_t smem_warp = smem + 4 * kWarpMsgBytes;
   tv_.account = timing_ ? 1 : 0;  // per-node accounting atomics only when measuring
+  // a launch of at most kWideGrid CTAs cannot fill the SMs at the
+  // throughput form's occupancy: it runs the wide form (more registers per
+  // thread, no spills, shorter serial chains)
+  auto level = [&](const uint32_t *refs, uint32_t cnt) {
+    const unsigned grid = blocks_for(cnt, kHashThreads);
+    if (grid <= kWideGrid)
+      count_launch(), k_hash_level_wide<<<grid, kHashThreads, smem, st_>>>(tv_, refs, (int)cnt);
+    else
+      count_launch(), k_hash_level<<<grid, kHashThreads, smem, st_>>>(tv_, refs, (int)cnt);
+  };
   // every leaf first (one launch), then the levels deepest first
   if (off[kLeafClasses] > 0) {
     ++levels;
-    count_launch(), k_hash_level<<<blocks_for(off[kLeafClasses], kHashThreads), kHashThreads, smem, st_>>>(
-                        tv_, sorted, (int)off[kLeafClasses]);
+    level(sorted, off[kLeafClasses]);
   }
   for (int d = (int)kMaxDepths - 1; d >= 0; --d) {
     uint32_t a = off[level_bin(d)], m = off[level_bin(d) + 1], z = off[level_bin(d + 1)];
@@ -993,13 +1005,10 @@ int Trie::bucket_and_hash() {
     ++levels;
     if (z - m > 0 && z - m <= (uint32_t)opt_warp_full_max_) {
       // few branches: short nodes thread-wise, branches one warp each
-      if (m > a)
-        count_launch(), k_hash_level<<<blocks_for(m - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a,
-                                                                                                  (int)(m - a));
+      if (m > a) level(sorted + a, m - a);
       count_launch(), k_hash_full_warp<<<(z - m + 3) / 4, 128, smem_warp, st_>>>(tv_, sorted + m, (int)(z - m));
     } else {
-      count_launch(), k_hash_level<<<blocks_for(z - a, kHashThreads), kHashThreads, smem, st_>>>(tv_, sorted + a,
-                                                                                                (int)(z - a));
+      level(sorted + a, z - a);
     }
   }
   if (timing_) {

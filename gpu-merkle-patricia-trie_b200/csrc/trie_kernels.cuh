@@ -1573,7 +1573,7 @@ constexpr int kHashLevelThreads = 128;  // k_hash_level's block size (the partit
 #ifndef GMPT_HASH_CTAS
 #define GMPT_HASH_CTAS 6
 #endif
-__global__ void __launch_bounds__(kHashLevelThreads, GMPT_HASH_CTAS) k_hash_level(TrieView tv, const uint32_t *refs, int count) {
+__device__ __forceinline__ void hash_level_cta(const TrieView &tv, const uint32_t *refs, int count) {
   extern __shared__ uint64_t stage_all[];
   __shared__ uint32_t s_ref[kHashLevelThreads];
   __shared__ uint32_t s_cnt[kCtaClasses][kHashLevelThreads / 32];  // [class][warp]
@@ -1600,6 +1600,20 @@ __global__ void __launch_bounds__(kHashLevelThreads, GMPT_HASH_CTAS) k_hash_leve
   __syncthreads();
   if (!valid) return;  // the valid nodes fill s_ref[0 .. valid count)
   hash_node<false>(tv, s_ref[threadIdx.x], stage_all + threadIdx.x, blockDim.x);
+}
+
+// The level kernel at the register budget of six resident CTAs per SM (the
+// throughput form), and with the whole register file open to one CTA per
+// SM: a level too small to fill the SMs is as long as the serial Keccak
+// chain of its longest node, which the wider form schedules with more
+// permutation state in flight.
+__global__ void __launch_bounds__(kHashLevelThreads, GMPT_HASH_CTAS) k_hash_level(TrieView tv, const uint32_t *refs,
+                                                                                 int count) {
+  hash_level_cta(tv, refs, count);
+}
+
+__global__ void __launch_bounds__(kHashLevelThreads, 1) k_hash_level_wide(TrieView tv, const uint32_t *refs, int count) {
+  hash_level_cta(tv, refs, count);
 }
 
 // ---------------------------------------------------------------------------
