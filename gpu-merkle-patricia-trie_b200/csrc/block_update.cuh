@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(256, 2) k_block(TrieView tv0, DirtyList dl, Bl
     if (!grid_barrier(D, tv.ctr)) return;
     if (t == 0) atomicExch(&tv.ctr->n_dirty, 0u);  // the list is consumed
     // hash, deepest level first
+    const CoopLanes coop = coop_lanes(lane);
     const uint32_t top = __ldcg(&D->maxbin[s]);
     uint32_t levels = 0;
     for (int d = (int)(top + 1) / 2 - 1; d >= 0; --d) {
@@ -361,9 +362,7 @@ __global__ void __launch_bounds__(256, 2) k_block(TrieView tv0, DirtyList dl, Bl
       if (z - m <= (uint32_t)(kWarpFullPerWarp * W)) {
         // few branches: a warp per node (latency)
         for (uint32_t j = (uint32_t)(W - 1 - gw); j < z - m; j += (uint32_t)W) {
-          const uint32_t r = __ldcg(bb.sorted + m + j);
-          if (!hash_full_warp<true>(tv, ref_idx(r), wmsg, smem + threadIdx.x, blockDim.x) && lane == 0)
-            hash_node<true>(tv, r, smem + threadIdx.x, blockDim.x);
+          hash_full_warp<true>(tv, ref_idx(__ldcg(bb.sorted + m + j)), wmsg, coop);
           __syncwarp();
         }
       } else {

@@ -109,6 +109,73 @@ __device__ __forceinline__ void keccak_f1600(uint64_t (&a)[25]) {
   for (int r = 0; r < 24; ++r) keccak_round(a, kKeccakRC[r]);
 }
 
+// Keccak-f[1600] spread over a warp: lane t < 25 holds lane t = x + 5y of
+// the state, the other lanes carry copies that nothing reads.  A round is
+// ten 64-bit shuffles (theta's column sums, the two neighbour columns,
+// pi's lane permutation, chi's two row neighbours) around a handful of
+// integer ops per lane, so one permutation's latency is a few shuffle
+// round trips per round instead of one thread's whole serial chain: the
+// form for nodes whose many blocks would otherwise set a level's time.
+struct CoopLanes {
+  uint32_t col[5];   // theta: the lanes of this lane's column
+  uint32_t cm1, cp1; // lanes holding column x - 1 and x + 1
+  uint32_t rot;      // rho offset of this lane
+  uint32_t src;      // pi: the lane whose rotated word lands here
+  uint32_t chi1, chi2;
+};
+
+__device__ __forceinline__ CoopLanes coop_lanes(int lane) {
+  // rho offsets r[x][y] (FIPS 202), indexed x + 5y
+  constexpr uint8_t kRho[25] = {0,  1,  62, 28, 27, 36, 44, 6,  55, 20, 3,  10, 43,
+                                25, 39, 41, 45, 15, 21, 8,  18, 2,  61, 56, 14};
+  const uint32_t t = (uint32_t)lane < 25u ? (uint32_t)lane : (uint32_t)lane - 25u;
+  const uint32_t x = t % 5u, y = t / 5u;
+  CoopLanes c;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) c.col[k] = x + 5u * (uint32_t)k;
+  c.cm1 = (x + 4u) % 5u;
+  c.cp1 = (x + 1u) % 5u;
+  c.rot = kRho[t];
+  // pi: B[x'][y'] = A[x][y] with x' = y, y' = (2x + 3y) mod 5; here (x', y')
+  // = (x, y), so the source has y_s = x and x_s = 3 (y - 3x) mod 5
+  const uint32_t xs = (3u * (y + 15u - 3u * x)) % 5u, ys = x;
+  c.src = xs + 5u * ys;
+  c.chi1 = (x + 1u) % 5u + 5u * y;
+  c.chi2 = (x + 2u) % 5u + 5u * y;
+  return c;
+}
+
+__device__ __forceinline__ uint64_t rotl64_var(uint64_t v, uint32_t r) {
+  uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+  if (r & 32u) {
+    const uint32_t t = lo;
+    lo = hi;
+    hi = t;
+  }
+  const uint32_t s = r & 31u;
+  const uint32_t nh = __funnelshift_l(lo, hi, s), nl = __funnelshift_l(hi, lo, s);
+  return ((uint64_t)nh << 32) | nl;
+}
+
+// All 32 lanes call it together; returns this lane's state word after the
+// permutation.
+__device__ __forceinline__ uint64_t keccak_f1600_warp(uint64_t a, const CoopLanes &c, int lane) {
+  constexpr unsigned kAll = 0xffffffffu;
+#pragma unroll 1
+  for (int r = 0; r < 24; ++r) {
+    const uint64_t cs = __shfl_sync(kAll, a, c.col[0]) ^ __shfl_sync(kAll, a, c.col[1]) ^
+                        __shfl_sync(kAll, a, c.col[2]) ^ __shfl_sync(kAll, a, c.col[3]) ^
+                        __shfl_sync(kAll, a, c.col[4]);
+    const uint64_t dm = __shfl_sync(kAll, cs, c.cm1), dp = __shfl_sync(kAll, cs, c.cp1);
+    a ^= dm ^ rotl64(dp, 1);
+    const uint64_t b = __shfl_sync(kAll, rotl64_var(a, c.rot), c.src);
+    const uint64_t b1 = __shfl_sync(kAll, b, c.chi1), b2 = __shfl_sync(kAll, b, c.chi2);
+    a = b ^ (~b1 & b2);
+    if (lane == 0) a ^= kKeccakRC[r];
+  }
+  return a;
+}
+
 // Streaming sponge.  Message bytes are pushed in little-endian runs of <= 8
 // bytes; whole 64-bit words go to this thread's 17-word staging block in
 // shared memory (word w at stage[w * stride]), which absorb() folds into the

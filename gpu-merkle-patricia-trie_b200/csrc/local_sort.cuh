@@ -115,7 +115,7 @@ __device__ __forceinline__ void cta_radix_pass(LocalSortSmem &L, int src, int m,
 __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, const uint32_t *seg_start,
                                                                   const uint32_t *seg_end, int c0, uint32_t *order,
                                                                   uint8_t *eqprev, const uint64_t *koff,
-                                                                  const uint32_t *klen, const uint32_t *term_len) {
+                                                                  const uint32_t *klen) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   LocalSortSmem &L = *reinterpret_cast<LocalSortSmem *>(smem_raw);
   const uint32_t a = seg_start[blockIdx.x];
@@ -158,21 +158,6 @@ __global__ void __launch_bounds__(kSortLocalThreads) k_local_sort(TrieView tv, c
     uint32_t ngroups;
     uint32_t rank = cta_excl_scan(starts, L.warp_tmp, ngroups);
     if (ngroups == (uint32_t)m) break;  // every key distinct
-    if (c > c0) {
-      // every tie left is between repeats of one key (k_term_len: both
-      // terminated, ended before this chunk, same length): the order is
-      // final, and the remaining chunks would only compare zeros
-      int live = 0;
-#pragma unroll
-      for (int r = 0; r < ipt; ++r) {
-        const int k = threadIdx.x * ipt + r;
-        if (k < m && tp[r]) {
-          const uint32_t a = term_len[L.val[src][k - 1]], b = term_len[L.val[src][k]];
-          if (!(b == a && b <= 8u * (uint32_t)c)) live = 1;
-        }
-      }
-      if (!__syncthreads_or(live)) break;
-    }
     // build (rank, chunk) keys in the current order
     if (threadIdx.x == 0) {
       L.mask = 0;

@@ -30,6 +30,8 @@ constexpr int kHashThreads = kHashLevelThreads;
 // k_hash_level_wide (132 registers: three CTAs per SM) for launches that
 // cannot place more than three CTAs on each of B200's 148 SMs anyway
 constexpr unsigned kWideGrid = 3 * 148;
+// branch hash class (blocks - 1) from which a branch is hashed by a warp
+constexpr uint32_t kWarpMinClass = 4;
 constexpr uint32_t kMaxDepths = kMaxKeyNibbles + 2;  // nibble depths a dirty node can have
 // LockNU batches of at least this many keys drop repeated keys first
 constexpr int kDedupMinKeys = 1 << 16;
@@ -413,10 +415,7 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
   unsigned long long *d_tot = wsp<unsigned long long>(ws_.misc, 16, e) + 2;
   if (e == cudaSuccess) e = scan_ws_.ensure(scan_ws_bytes<unsigned long long>(n));
   if (e != cudaSuccess) return check_cuda(e, "sort alloc");
-  uint32_t *term_len = wsp<uint32_t>(ws_.term_len, (size_t)n, e);
-  if (e != cudaSuccess) return check_cuda(e, "sort alloc");
   count_launch(), k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
-  count_launch(), k_term_len<<<blocks_for(n), kThreads, 0, st_>>>(tv_.keys, koff, klen, n, term_len);
   int nchunks = (int)((maxlen + 7) / 8);
   stats_.sort_passes = 0;
   // forest batches: a first pass orders by trie id
@@ -449,8 +448,7 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
         if ((e = cudaFuncSetAttribute(k_local_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
           return check_cuda(e, "local sort attr");
-        count_launch(), k_local_sort<<<S, kSortLocalThreads, smem, st_>>>(tv_, rs, re, c, order, eqprev, koff, klen,
-                                                                            term_len);
+        count_launch(), k_local_sort<<<S, kSortLocalThreads, smem, st_>>>(tv_, rs, re, c, order, eqprev, koff, klen);
         if ((e = cudaGetLastError()) != cudaSuccess) return check_cuda(e, "local sort");
         break;
       }
@@ -982,7 +980,7 @@ int Trie::bucket_and_hash() {
     cudaEventCreate(&kz);
     cudaEventRecord(ka, st_);
   }
-  const size_t smem_warp = smem + 4 * kWarpMsgBytes;
+  const size_t smem_warp = 4 * kWarpMsgBytes;
   tv_.account = timing_ ? 1 : 0;  // per-node accounting atomics only when measuring
   // a launch of at most kWideGrid CTAs cannot fill the SMs at the
   // throughput form's occupancy: it runs the wide form (more registers per
@@ -1003,10 +1001,20 @@ int Trie::bucket_and_hash() {
     uint32_t a = off[level_bin(d)], m = off[level_bin(d) + 1], z = off[level_bin(d + 1)];
     if (z == a) continue;
     ++levels;
+    // branches of kWarpMinClass + 1 blocks or more: the level's first branch
+    // bins (longest first)
+    const uint32_t ml = off[level_bin(d) + 1 + (kHashClasses - kWarpMinClass)];
     if (z - m > 0 && z - m <= (uint32_t)opt_warp_full_max_) {
       // few branches: short nodes thread-wise, branches one warp each
       if (m > a) level(sorted + a, m - a);
       count_launch(), k_hash_full_warp<<<(z - m + 3) / 4, 128, smem_warp, st_>>>(tv_, sorted + m, (int)(z - m));
+    } else if (ml > m && ml - m <= (uint32_t)opt_warp_full_max_) {
+      // a few branches of many blocks (a key ending at a branch puts its
+      // value, up to kilobytes, in slot 16) would set the level's time as
+      // one thread's serial chain: one warp each, the rest thread-wise
+      count_launch(), k_hash_full_warp<<<(ml - m + 3) / 4, 128, smem_warp, st_>>>(tv_, sorted + m, (int)(ml - m));
+      if (m > a) level(sorted + a, m - a);
+      level(sorted + ml, z - ml);
     } else {
       level(sorted + a, z - a);
     }

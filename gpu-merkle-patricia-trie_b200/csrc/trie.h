@@ -259,7 +259,6 @@ class Trie {
     DevBlock dd_hash, dd_pos, dd_sel, dd_slot;                  // LockNU batch dedup
     DevBlock raw;                                               // raw key bytes of the batch
     DevBlock dirty_cls;                                         // hash class of each dirty node
-    DevBlock term_len;                                          // sort: length of each terminated key
     DevBlock rw_flags, rw_a, rw_b, rw_c, rw_d, rw_e, rw_wpos;   // mixed read/write resolution
     DevBlock rw_hp, rw_len, rw_tot, rw_kept, rw_koff, rw_klen, rw_tid;
     DevBlock del_hslot, del_hext, del_stamp;                    // deletes: how each path branch is linked

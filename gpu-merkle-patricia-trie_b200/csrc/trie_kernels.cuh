@@ -267,20 +267,6 @@ __device__ __forceinline__ uint32_t key_chunk(const uint8_t *keys, uint64_t off,
   return pack_nibbles8(x);
 }
 
-// Nibbles of a terminated key (last nibble 16), else 0xFFFFFFFF.  Staging
-// admits the terminator only as a key's last nibble, and chunks compare
-// nibbles 0..15 exactly, so two chunk-equal neighbours that are terminated
-// keys of the same length, both ended, are the same key (a terminator packs
-// like nibble 0, so keys of different lengths can still tie on every chunk
-// and are told apart by the length pass).
-__global__ void k_term_len(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, int n,
-                           uint32_t *term_len) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t len = klen[i];
-  term_len[i] = (len > 0 && keys[koff[i] + len - 1] == 16) ? len : 0xFFFFFFFFu;
-}
-
 // active = tied with a neighbour; packed: low = active, high = segment start
 __global__ void k_sort_flags(const uint8_t *eqprev, int n, unsigned long long *flags) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1467,98 +1453,98 @@ __device__ __forceinline__ void hash_node(const TrieView &tv, uint32_t ref, uint
 constexpr int kWarpMsgBytes = 8 * 136;
 
 // Warp-cooperative encode + hash of branch node idx, for levels with few
-// nodes where one thread's serial encoding is the latency: lane k < 17 places
-// child k's item into the warp's message at its scanned offset, then lane 0
-// pads and permutes.  All 32 lanes call it with the same idx; returns false
-// (nothing written) when the encoding does not fit kWarpMsgBytes, and the
-// caller hashes the node with hash_node instead.
+// nodes or for branches of many blocks, where one thread's serial chain is
+// the latency: the message is built window by window (kWarpMsgBytes, 8
+// blocks) in the warp's shared buffer, every lane copying a share of each
+// item's bytes (lane k < 17 holds child k's item, the header goes first),
+// and absorbed with the warp-spread permutation.  All 32 lanes call it with
+// the same idx.
 template <bool kCoh>
-__device__ __forceinline__ bool hash_full_warp(const TrieView &tv, uint32_t idx, uint8_t *msg, uint64_t *stage,
-                                               uint32_t stride) {
+__device__ __forceinline__ void hash_full_warp(const TrieView &tv, uint32_t idx, uint8_t *msg, const CoopLanes &cl) {
+  constexpr unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  if (ldn<kCoh>(tv.full_dead + idx)) return true;  // unlinked by a delete: nothing to hash
+  if (ldn<kCoh>(tv.full_dead + idx)) return;  // unlinked by a delete: nothing to hash
   EncItem it{0, 0, 0, nullptr, 0};
   if (lane < 17) it = child_item<kCoh>(tv, ldn<kCoh>(tv.full_child + (size_t)idx * 17 + lane));
   const uint32_t sz = lane < 17 ? it.pren + it.blen : 0u;
   uint32_t incl = sz;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    const uint32_t v = __shfl_up_sync(kAll, incl, o);
     if (lane >= o) incl += v;
   }
-  const uint32_t payload = __shfl_sync(0xffffffffu, incl, 31);
+  const uint32_t payload = __shfl_sync(kAll, incl, 31);
   uint64_t hdr;
   uint32_t hn;
   rlp_head(payload, 0xc0, 0xf7, hdr, hn);
   const uint32_t total = payload + hn;
-  if (total + 1 > (uint32_t)kWarpMsgBytes) return false;
   const bool force = tv.geth_mode && ldn<kCoh>(tv.full_depth + idx) == 0;
   const bool raw = total < 32 && !force;
   const uint32_t nblk = raw ? 1u : (total + 1 + 135) / 136;
   const uint32_t padded = nblk * 136;
-  // zero the blocks, then place the header and the items
+  const uint32_t my_off = hn + incl - sz;  // message offset of this lane's item
   uint64_t *m64 = reinterpret_cast<uint64_t *>(msg);
-  for (uint32_t w = lane; w < padded / 8; w += 32) m64[w] = 0;
-  __syncwarp();
-  if (lane == 0)
-    for (uint32_t b = 0; b < hn; ++b) msg[b] = (uint8_t)(hdr >> (8 * b));
-  if (lane < 17) {
-    uint32_t p = hn + incl - sz;
-    for (uint32_t b = 0; b < it.pren; ++b) msg[p + b] = (uint8_t)(it.pre >> (8 * b));
-    p += it.pren;
-    for (uint32_t o = 0; o < it.blen; o += 8) {
-      const uint64_t v = ld8<kCoh>(it.body + o);
-      const uint32_t nb = min(8u, it.blen - o);
-      for (uint32_t b = 0; b < nb; ++b) msg[p + o + b] = (uint8_t)(v >> (8 * b));
+  uint64_t a = 0;  // this lane's word of the state
+  for (uint32_t b0 = 0; b0 < nblk; b0 += kWarpMsgBytes / 136) {
+    const uint32_t wb = min((uint32_t)(kWarpMsgBytes / 136), nblk - b0);
+    const uint32_t lo = b0 * 136, hi = lo + wb * 136;
+    for (uint32_t w = lane; w < wb * 17; w += 32) m64[w] = 0;
+    __syncwarp();
+    if (lane == 0)
+      for (uint32_t q = 0; q < hn; ++q)
+        if (q >= lo && q < hi) msg[q - lo] = (uint8_t)(hdr >> (8 * q));
+    // items in order; the lanes share each item's bytes that fall in the window
+    for (int k = 0; k < 17; ++k) {
+      const uint32_t p = __shfl_sync(kAll, my_off, k);
+      const uint32_t pren = __shfl_sync(kAll, it.pren, k);
+      const uint32_t blen = __shfl_sync(kAll, it.blen, k);
+      const uint64_t pre = __shfl_sync(kAll, it.pre, k);
+      const uint8_t *body = reinterpret_cast<const uint8_t *>(
+          __shfl_sync(kAll, reinterpret_cast<unsigned long long>(it.body), k));
+      const uint32_t n = pren + blen;
+      if (p >= hi || p + n <= lo) continue;
+      const uint32_t j0 = lo > p ? lo - p : 0u, j1 = min(n, hi - p);
+      for (uint32_t j = j0 + (uint32_t)lane; j < j1; j += 32)
+        msg[p + j - lo] = j < pren ? (uint8_t)(pre >> (8 * j)) : ldn<kCoh>(body + (j - pren));
     }
+    __syncwarp();
+    if (raw) break;  // under 32 bytes: the window holds the whole encoding
+    if (lane == 0) {  // Keccak padding (pad byte 0x01 ... last byte |= 0x80)
+      if (total >= lo && total < hi) msg[total - lo] ^= 0x01;
+      if (padded - 1 >= lo && padded - 1 < hi) msg[padded - 1 - lo] ^= 0x80;
+    }
+    __syncwarp();
+    for (uint32_t bb = 0; bb < wb; ++bb) {
+      if (lane < 17) a ^= m64[bb * 17 + lane];
+      a = keccak_f1600_warp(a, cl, lane);
+    }
+    __syncwarp();  // the next window reuses the buffer
+  }
+  uint64_t *o = reinterpret_cast<uint64_t *>(tv.full_hash + (size_t)idx * 32);
+  if (raw) {
+    if (lane < 4) o[lane] = m64[lane];  // zero beyond total
+    if (lane == 0) tv.full_hlen[idx] = (uint8_t)total;
+  } else {
+    if (lane < 4) o[lane] = a;
+    if (lane == 0) tv.full_hlen[idx] = 32;
+  }
+  if (lane == 0 && tv.account) {
+    atomicAdd(&tv.ctr->enc_bytes, (unsigned long long)total);
+    atomicAdd(&tv.ctr->keccak_blocks, (unsigned long long)(raw ? 0u : nblk));
+    atomicAdd(&tv.ctr->hashed, 1u);
   }
   __syncwarp();
-  if (lane == 0) {
-    uint8_t *hout = tv.full_hash + (size_t)idx * 32;
-    uint64_t *o = reinterpret_cast<uint64_t *>(hout);
-    if (raw) {
-#pragma unroll
-      for (int w = 0; w < 4; ++w) o[w] = m64[w];  // zero beyond total
-      tv.full_hlen[idx] = (uint8_t)total;
-    } else {
-      msg[total] ^= 0x01;
-      msg[padded - 1] ^= 0x80;
-      uint64_t a[25];
-#pragma unroll
-      for (int w = 0; w < 25; ++w) a[w] = 0;
-      for (uint32_t b = 0; b < nblk; ++b) {
-#pragma unroll
-        for (int w = 0; w < 17; ++w) a[w] ^= m64[b * 17 + w];
-        keccak_f1600(a);
-      }
-      o[0] = a[0];
-      o[1] = a[1];
-      o[2] = a[2];
-      o[3] = a[3];
-      tv.full_hlen[idx] = 32;
-    }
-    if (tv.account) {
-      atomicAdd(&tv.ctr->enc_bytes, (unsigned long long)total);
-      atomicAdd(&tv.ctr->keccak_blocks, (unsigned long long)(raw ? 0u : nblk));
-      atomicAdd(&tv.ctr->hashed, 1u);
-    }
-  }
-  __syncwarp();
-  (void)stage;
-  (void)stride;
-  return true;
 }
 
-// A level's branch nodes, one warp each (levels with few branches, where a
-// node's serial encoding is the latency): 4 warps per CTA.
+// Branch nodes one warp each (a level's branches when it has few, or its
+// branches of many blocks): 4 warps per CTA.
 __global__ void __launch_bounds__(128) k_hash_full_warp(TrieView tv, const uint32_t *refs, int count) {
-  extern __shared__ uint64_t stage_all[];  // 17 words per thread, then 4 messages
+  extern __shared__ uint64_t msg_all[];  // one message window per warp
   const int j = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (j >= count) return;  // whole warps leave together
-  uint8_t *msg = reinterpret_cast<uint8_t *>(stage_all + 17 * blockDim.x) + (threadIdx.x >> 5) * kWarpMsgBytes;
-  const uint32_t r = refs[j];
-  if (!hash_full_warp<false>(tv, ref_idx(r), msg, stage_all + threadIdx.x, blockDim.x) && (threadIdx.x & 31) == 0)
-    hash_node<false>(tv, r, stage_all + threadIdx.x, blockDim.x);
+  uint8_t *msg = reinterpret_cast<uint8_t *>(msg_all) + (threadIdx.x >> 5) * kWarpMsgBytes;
+  const CoopLanes cl = coop_lanes(threadIdx.x & 31);
+  hash_full_warp<false>(tv, ref_idx(refs[j]), msg, cl);
 }
 
 // Six 128-thread CTAs per SM (at most 85 registers): the permutation keeps
