@@ -283,16 +283,19 @@ def run_reference_gpu(args, world, rank):
     variants = {}
     if hasattr(L, "ref_gpu_variant_root"):
         L.ref_gpu_variant_root.restype = C.c_int
-        L.ref_gpu_variant_root.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+        L.ref_gpu_variant_root.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p, C.c_void_p]
         out = np.zeros(32, np.uint8)
         for v, name in ((0, "puts_latching_with_valuehp+hash_onepass"),
                         (1, "puts_latching_with_valuehp_v2+hash_onepass_v2"),
                         (2, "puts_2phase_with_valuehp+hash_onepass_v2")):
             out[:] = 0
+            t_ms = C.c_double(0.0)
             sz = L.ref_gpu_variant_root(v, P(c1.keys_hexs), P(np.ascontiguousarray(c1.keys_indexs, np.int32)),
                                         P(c1.values), P(np.ascontiguousarray(c1.values_indexs, np.int64)), c1.n,
-                                        P(out))
-            variants[name] = out.tobytes().hex() if sz == 32 else f"size {sz}"
+                                        P(out), C.byref(t_ms))
+            variants[name] = {"root": out.tobytes().hex() if sz == 32 else f"size {sz}",
+                              "insert_hash_ms": round(t_ms.value, 3),
+                              "mkeys_s": round(c1.n / (t_ms.value / 1e3) / 1e6, 3) if t_ms.value > 0 else None}
     # the reference's GPU Keccak-256 alone on seeded messages, against the
     # oracle's Keccak-256 (its digests decide every root it returns)
     keccak_kat = []
@@ -433,6 +436,46 @@ def phase_roofline(batches, stats_all, hbm_peak, perm_peak):
                         "frac": round(bound_ms / tot_ms, 4),
                         "bound": "int (Keccak-f)" if tot_perm / perm_peak > tot_alg / (hbm_peak * 1e9) else "hbm"}
     return out
+
+
+def run_c1(local, dev):
+    """The small configuration (2^20 random 32 B keys, 64 B values, empty
+    trie, PhaseNU + PhaseHC + root), device-resident inputs; its root against
+    the oracle's (tests/golden/config_roots.json)."""
+    import torch
+
+    import gmpt
+
+    b = W.random_keys(1 << 20)
+    d = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (b.keys_hexs, b.keys_indexs, b.values,
+                                                                     b.values_indexs)]
+    t = gmpt.MPT(device=local)
+    t.reserve(b.n, b.key_bytes(), b.value_bytes())
+    stream = torch.cuda.ExternalStream(t.stream_ptr(), device=dev)
+    ms, roots = [], set()
+    for it in range(8):
+        t.reset()
+        torch.cuda.synchronize(dev)
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        t.puts_device(True, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), b.n, b.key_bytes(),
+                      b.value_bytes())
+        t.hash_onepass_v2()
+        roots.add(t.get_root_hash())
+        z.record(stream)
+        z.synchronize()
+        if it >= 3:
+            ms.append(a.elapsed_time(z))
+    t.close()
+    path = REPO / "tests" / "golden" / "config_roots.json"
+    gold = json.loads(path.read_text())["cases"]["c1_random_1m"]["roots"][0] if path.exists() else None
+    assert len(roots) == 1
+    root = roots.pop().hex()
+    m = statistics.median(ms)
+    return {"workload": "2^20 random 32 B keys, 64 B values, empty trie; PhaseNU + PhaseHC + root, device-resident",
+            "ms": round(m, 3), "mkeys_s": round(b.n / (m / 1e3) / 1e6, 2), "root": root,
+            "root_matches_oracle": gold is not None and root == gold}
 
 
 def run_gets(t, d, n, dev, stream, hbm_peak):
@@ -1180,7 +1223,7 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, batches)
-    if world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0):
+    if world == 1:
         t.close()
         del dbat
         gc.collect()
@@ -1199,6 +1242,8 @@ def run_ours(args, world, rank, local):
         gc.collect()
         torch.cuda.empty_cache()
 
+    if world == 1:
+        section("c1_random_2pow20", run_c1, local, dev)
     if world == 1 and args.vocab_n > 0:
         section("vocab", run_vocab, args, local, dev, hbm_peak, kpeak)
     if world == 1 and args.eth_accounts > 0:
@@ -1207,7 +1252,7 @@ def run_ours(args, world, rank, local):
         section("learned", run_requests, args, local, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if not (world == 1 and (args.eth_accounts > 0 or args.req_tenants or args.vocab_n > 0)):
+    if world != 1:
         t.close()
     if world > 1:
         import torch.distributed as dist

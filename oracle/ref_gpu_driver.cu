@@ -9,6 +9,8 @@
 // tree: the Crypto++ Keccak_256 that cpu_mpt.cuh's hashing names (the shim
 // header in ref_shim/ forwards to shim_keccak256, defined here on the
 // reference's own CPUHash::keccak1600, rate 136, Keccak padding).
+#include <chrono>
+
 #include "libgmpt.cu"
 
 namespace CryptoPP {
@@ -29,8 +31,11 @@ void shim_keccak256(const byte *in, std::size_t len, byte *out32) {
 //              insert_mpt_olc runs (lib/libgmpt.cu:299-303)
 //   variant 2: puts_2phase_with_valuehp + hash_onepass_v2
 // Returns the root's size (32, or 0 for no root); -1 for an unknown variant.
+// ms_out (optional): wall time of the insert + hash alone (the trie is built
+// before the clock starts), with a device synchronisation on both sides.
 extern "C" int ref_gpu_variant_root(int variant, const uint8_t *keys_hexs, int *keys_indexs,
-                                    const uint8_t *values, int64_t *values_indexs, int n, uint8_t *out32) {
+                                    const uint8_t *values, int64_t *values_indexs, int n, uint8_t *out32,
+                                    double *ms_out) {
   if (variant < 0 || variant > 2) return -1;
   GPUHashMultiThread::load_constants();
   const uint8_t **hps = new const uint8_t *[n];
@@ -38,6 +43,8 @@ extern "C" int ref_gpu_variant_root(int variant, const uint8_t *keys_hexs, int *
   int size = 0;
   {
     GpuMPT::Compress::MPT mpt;
+    cudaDeviceSynchronize();
+    const auto t0 = std::chrono::steady_clock::now();
     if (variant == 0) {
       mpt.puts_latching_with_valuehp(keys_hexs, keys_indexs, values, values_indexs, hps, n);
       mpt.hash_onepass(keys_hexs, keys_indexs, n);
@@ -48,6 +55,9 @@ extern "C" int ref_gpu_variant_root(int variant, const uint8_t *keys_hexs, int *
       auto [nodes, cnt] = mpt.puts_2phase_with_valuehp(keys_hexs, keys_indexs, values, values_indexs, hps, n);
       mpt.hash_onepass_v2(nodes, cnt);
     }
+    cudaDeviceSynchronize();
+    if (ms_out)
+      *ms_out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const uint8_t *h = nullptr;
     mpt.get_root_hash(h, size);
     if (h && size > 0) std::memcpy(out32, h, size < 32 ? size : 32);
