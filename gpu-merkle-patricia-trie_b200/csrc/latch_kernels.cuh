@@ -392,8 +392,14 @@ constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 // full), so the passes after it need not hash and probe again
 __global__ void k_dedup_insert(TrieView tv, const uint64_t *koff, const uint32_t *klen, const int *tid, int n,
                                DedupTable t, uint32_t *slot_of) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  // batch positions from the last one down: CTAs start roughly in order, so
+  // a zipf-hot key's latest occurrences claim its slot first and the earlier
+  // ones find a larger position there and skip the atomic (front to back,
+  // every occurrence of a key repeated a million times would raise the slot
+  // in turn, one atomic after another on the same address)
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const int i = n - 1 - u;
   const unsigned long long h = dedup_hash(tv.keys + koff[i], klen[i], tid ? (uint32_t)tid[i] : 0u, t.hmask);
   uint64_t s = dedup_home(h, t.mask);
   for (uint64_t probe = 0; probe <= t.mask; ++probe, s = (s + 1) & t.mask) {
