@@ -54,3 +54,21 @@ def test_selector_file_errors_are_reported(tmp_path):
         raise AssertionError("expected an error")
     except gmpt.GmptError as e:
         assert "schedules" in str(e)
+
+
+def test_network_candidates_are_the_near_best_configurations():
+    # configuration 0 is best everywhere, 1 within 5 % on a quarter of the
+    # batches, 2 close on a single batch (under the 2 % share), 3 never
+    # close, 4 never measured
+    rng = np.random.default_rng(3)
+    t = np.full((200, 5), np.nan)
+    t[:, 0] = rng.uniform(1.0, 2.0, 200)
+    t[:, 1] = t[:, 0] * 1.5
+    t[:50, 1] = t[:50, 0] * 1.03
+    t[:, 2] = t[:, 0] * 3.0
+    t[0, 2] = t[0, 0]
+    t[:, 3] = t[:, 0] * 10.0
+    assert TU.candidates(t) == [0, 1]
+    assert TU.candidates(t, share=0.0) == [0, 1, 2]
+    # nothing near the best anywhere but the best itself
+    assert TU.candidates(t[:, [3, 4]]) == [0]
