@@ -383,7 +383,7 @@ def cpu_baseline(args, batches):
 
 def phase_roofline(batches, stats_all, hbm_peak, perm_peak):
     """Per-phase HBM rooflines of the timed steps and the put + hash
-    composite (algorithmic bytes and ops as defined in DESIGN.md section 5):
+    composite, with these algorithmic bytes and ops:
       stage   2 (|k| + |v|) + 56 B per key (read the streams and index
               pairs, write the arenas, value records and key records)
       sort    |k| + 4 B per key (read every key once, write its rank)
