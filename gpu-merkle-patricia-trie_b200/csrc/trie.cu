@@ -418,8 +418,21 @@ int Trie::sort_batch(int n, const uint64_t *koff, const uint32_t *klen, uint32_t
   count_launch(), k_init_order<<<blocks_for(n + 1), kThreads, 0, st_>>>(order, eqprev, n);
   int nchunks = (int)((maxlen + 7) / 8);
   stats_.sort_passes = 0;
+  // leading chunks that every key shares sort nothing: skip their passes
+  int c_first = tid ? -1 : 0;
+  if (!tid && n > 1) {
+    uint32_t *differs = reinterpret_cast<uint32_t *>(d_tot + 1);
+    for (; c_first < nchunks; ++c_first) {
+      if ((e = cudaMemsetAsync(differs, 0, 4, st_)) != cudaSuccess) return check_cuda(e, "sort prefix");
+      count_launch(), k_chunk_shared<<<blocks_for(n), kThreads, 0, st_>>>(tv_.keys, koff, klen, n, c_first, differs);
+      if ((e = cudaMemcpyAsync(h_small_, differs, 4, cudaMemcpyDeviceToHost, st_)) != cudaSuccess ||
+          (e = cudaStreamSynchronize(st_)) != cudaSuccess)
+        return check_cuda(e, "sort prefix");
+      if (h_small_[0] & 0xFFFFFFFFu) break;
+    }
+  }
   // forest batches: a first pass orders by trie id
-  for (int c = tid ? -1 : 0; c <= nchunks; ++c) {
+  for (int c = c_first; c <= nchunks; ++c) {
     int cc = (c == nchunks) ? -1 : (c < 0 ? -2 : c);  // final pass: key length
     count_launch(), k_sort_flags<<<blocks_for(n), kThreads, 0, st_>>>(eqprev, n, flags);
     e = exclusive_scan<unsigned long long>(flags, pos, n, d_tot, scan_ws_, st_);

@@ -267,6 +267,15 @@ __device__ __forceinline__ uint32_t key_chunk(const uint8_t *keys, uint64_t off,
   return pack_nibbles8(x);
 }
 
+// *differs = 1 when some key's chunk c is not key 0's (a chunk every key of
+// the batch shares needs no sort pass: YCSB keys all begin with "user")
+__global__ void k_chunk_shared(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, int n, int c,
+                               uint32_t *differs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool d = i < n && key_chunk(keys, koff[i], klen[i], c) != key_chunk(keys, koff[0], klen[0], c);
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicOr(differs, 1u);
+}
+
 // active = tied with a neighbour; packed: low = active, high = segment start
 __global__ void k_sort_flags(const uint8_t *eqprev, int n, unsigned long long *flags) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
