@@ -1044,32 +1044,37 @@ def run_ours(args, world, rank, local):
     if not args.no_deletes:
         b0, d0 = batches[0], dbat[0]
         t.set_timing(False)
-        t.reset()
-        t.puts_device(True, d0["k"].data_ptr(), d0["ki"].data_ptr(), d0["v"].data_ptr(), d0["vi"].data_ptr(), d0["n"],
-                      d0["kb"], d0["vb"])
-        t.hash_onepass_v2()
-        root0 = t.get_root_hash()
-        assert root0 == roots_s[0], "load root differs from the timed step's"
         sub = b0.subset(np.arange(0, b0.n, 16))
         ds = dict(k=torch.from_numpy(sub.keys_hexs).to(dev), ki=torch.from_numpy(sub.keys_indexs).to(dev),
                   v=torch.from_numpy(sub.values).to(dev), vi=torch.from_numpy(sub.values_indexs).to(dev))
-        torch.cuda.synchronize(dev)
-        a = torch.cuda.Event(enable_timing=True)
-        z = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        t.deletes_device(ds["k"].data_ptr(), ds["ki"].data_ptr(), sub.n, sub.key_bytes())
-        t.hash_onepass_v2()
-        root_del = t.get_root_hash()
-        z.record(stream)
-        z.synchronize()
-        del_ms = a.elapsed_time(z)
-        t.puts_device(False, ds["k"].data_ptr(), ds["ki"].data_ptr(), ds["v"].data_ptr(), ds["vi"].data_ptr(), sub.n,
-                      sub.key_bytes(), sub.value_bytes())
-        t.hash_onepass_v2()
-        assert t.get_root_hash() == root0, "delete + re-insert did not restore the root"
-        assert root_del != root0
-        deletes = {"keys": int(sub.n), "from_trie_keys": int(b0.n), "ms": round(del_ms, 3),
-                   "mkeys_s": round(sub.n / (del_ms / 1e3) / 1e6, 3), "path": "gmpt_deletes_device + PhaseHC + root",
+        del_ms = []
+        for it in range(4):  # the first pass grows the delete workspaces and pools: not timed
+            t.reset()
+            t.puts_device(True, d0["k"].data_ptr(), d0["ki"].data_ptr(), d0["v"].data_ptr(), d0["vi"].data_ptr(),
+                          d0["n"], d0["kb"], d0["vb"])
+            t.hash_onepass_v2()
+            root0 = t.get_root_hash()
+            assert root0 == roots_s[0], "load root differs from the timed step's"
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            z = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            t.deletes_device(ds["k"].data_ptr(), ds["ki"].data_ptr(), sub.n, sub.key_bytes())
+            t.hash_onepass_v2()
+            root_del = t.get_root_hash()
+            z.record(stream)
+            z.synchronize()
+            if it > 0:
+                del_ms.append(a.elapsed_time(z))
+            t.puts_device(False, ds["k"].data_ptr(), ds["ki"].data_ptr(), ds["v"].data_ptr(), ds["vi"].data_ptr(),
+                          sub.n, sub.key_bytes(), sub.value_bytes())
+            t.hash_onepass_v2()
+            assert t.get_root_hash() == root0, "delete + re-insert did not restore the root"
+            assert root_del != root0
+        m = statistics.median(del_ms)
+        deletes = {"keys": int(sub.n), "from_trie_keys": int(b0.n), "ms": round(m, 3),
+                   "mkeys_s": round(sub.n / (m / 1e3) / 1e6, 3), "passes_ms": [round(x, 3) for x in del_ms],
+                   "path": "gmpt_deletes_device + PhaseHC + root (median of 3 passes after one untimed)",
                    "roundtrip_root_exact": True}
         del ds
 
