@@ -271,9 +271,12 @@ __device__ __forceinline__ uint32_t key_chunk(const uint8_t *keys, uint64_t off,
 // the batch shares needs no sort pass: YCSB keys all begin with "user")
 __global__ void k_chunk_shared(const uint8_t *keys, const uint64_t *koff, const uint32_t *klen, int n, int c,
                                uint32_t *differs) {
+  // once one warp has found a difference the rest have nothing to add: they
+  // read the flag and leave instead of queueing atomics on one address
+  if (__any_sync(0xffffffffu, __ldcg(differs) != 0u)) return;  // the whole warp leaves
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool d = i < n && key_chunk(keys, koff[i], klen[i], c) != key_chunk(keys, koff[0], klen[0], c);
-  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicOr(differs, 1u);
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0 && !__ldcg(differs)) atomicOr(differs, 1u);
 }
 
 // active = tied with a neighbour; packed: low = active, high = segment start
