@@ -969,11 +969,13 @@ constexpr uint32_t kLeafBit = 0x80;  // class byte of a leaf
 __host__ __device__ __forceinline__ uint32_t level_bin(uint32_t depth) { return kLeafClasses + depth * kBinsPerDepth; }
 
 // class byte of a dirty node: kLeafBit | block class for a leaf, the hash
-// class for a branch, 0 for an extension (a dead short node lands in either
-// and is skipped by the hash)
+// class for a branch, 0 for an extension or a dead short node (LockNU's
+// splits leave many: among the leaves they would idle lanes of the warps
+// that hash live leaves of the same block count)
 __device__ __forceinline__ uint32_t dirty_class(const TrieView &tv, uint32_t r, bool leaf_classes) {
   const uint32_t idx = ref_idx(r);
   if (ref_kind(r) == KIND_FULL) return full_class(tv, idx);
+  if (tv.short_dead[idx]) return 0u;
   const uint32_t ch = tv.short_child[idx];
   if (ref_kind(ch) != KIND_VALUE) return 0u;
   if (!leaf_classes) return kLeafBit;
